@@ -1,0 +1,179 @@
+"""ctypes mirror of include/nbg_b200.h and the loader of the native library.
+
+The product path is the in-tree shared library ``gpupdal_b200/_lib/libnbg_b200.so``
+(hand-written sm_100a CUDA behind a C ABI).  Loading fails loudly when it is
+missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "_lib")
+LIB_PATH = os.path.join(LIB_DIR, "libnbg_b200.so")
+
+NBG_OK = 0
+NBG_ERR_INVALID = 1
+NBG_ERR_OOM = 2
+NBG_ERR_BUDGET = 3
+NBG_ERR_CUDA = 4
+NBG_ERR_TIMEOUT = 5
+NBG_ERR_UNSUPPORTED = 6
+NBG_ERR_NO_DEVICE = 7
+NBG_ERR_EXCEPTIONS = 8
+
+STAGE_NORMAL = 1
+STAGE_EIGENVALUES = 2
+STAGE_COVARIANCEFEATURES = 3
+
+# covariance feature bits, reference order of feature_set "all"
+FEATURES = [
+    "Linearity",
+    "Planarity",
+    "Scattering",
+    "Verticality",
+    "Omnivariance",
+    "Anisotropy",
+    "Eigenentropy",
+    "EigenvalueSum",
+    "SurfaceVariation",
+    "DemantkeVerticality",
+    "Density",
+]
+FEAT_BIT = {name: 1 << i for i, name in enumerate(FEATURES)}
+FEAT_DIMENSIONALITY = 0x0F
+FEAT_ALL = 0x7FF
+
+MODE_RAW = 0
+MODE_SQRT = 1
+MODE_NORMALIZED = 2
+
+ROW_TOO_FEW = 1
+ROW_ZERO_COV = 2
+ROW_EIGEN_FAIL = 3
+ROW_ZERO_LAMBDA = 4
+
+MAX_DIMS = 16
+
+NORMAL_DIMS = ["NormalX", "NormalY", "NormalZ", "Curvature"]
+EIGENVALUE_DIMS = ["Eigenvalue0", "Eigenvalue1", "Eigenvalue2"]
+
+
+class StageOpts(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("knn", ctypes.c_int32),
+        ("always_up", ctypes.c_int32),
+        ("has_viewpoint", ctypes.c_int32),
+        ("viewpoint", ctypes.c_double * 3),
+        ("refine", ctypes.c_int32),
+        ("normalize", ctypes.c_int32),
+        ("feature_mask", ctypes.c_uint32),
+        ("mode", ctypes.c_int32),
+        ("stride", ctypes.c_int32),
+        ("optimized", ctypes.c_int32),
+    ]
+
+
+class Columns(ctypes.Structure):
+    _fields_ = [
+        ("base", ctypes.c_void_p),
+        ("point_stride", ctypes.c_int64),
+        ("ndims", ctypes.c_int32),
+        ("on_device", ctypes.c_int32),
+        ("offset", ctypes.c_int64 * MAX_DIMS),
+    ]
+
+
+class RowException(ctypes.Structure):
+    _fields_ = [
+        ("point_id", ctypes.c_uint32),
+        ("stage", ctypes.c_uint8),
+        ("code", ctypes.c_uint8),
+        ("reserved", ctypes.c_uint16),
+    ]
+
+
+class RunStats(ctypes.Structure):
+    _fields_ = [
+        ("points", ctypes.c_uint64),
+        ("tie_rows", ctypes.c_uint64),
+        ("deferred_rows", ctypes.c_uint64),
+        ("resolved_rows", ctypes.c_uint64),
+        ("grid_ms", ctypes.c_double),
+        ("query_ms", ctypes.c_double),
+        ("tree_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+    ]
+
+
+def stage_dims(opts: StageOpts) -> list:
+    """Output dimension names of one stage, in the library's order."""
+    if opts.kind == STAGE_NORMAL:
+        return list(NORMAL_DIMS)
+    if opts.kind == STAGE_EIGENVALUES:
+        return list(EIGENVALUE_DIMS)
+    return [f for i, f in enumerate(FEATURES) if opts.feature_mask & (1 << i)]
+
+
+def make_opts(kind, knn=8, always_up=True, viewpoint=None, refine=False,
+              normalize=False, feature_mask=FEAT_DIMENSIONALITY, mode=MODE_SQRT,
+              stride=1, optimized=False) -> StageOpts:
+    o = StageOpts()
+    o.kind = int(kind)
+    o.knn = int(knn)
+    o.always_up = int(bool(always_up))
+    o.has_viewpoint = int(viewpoint is not None)
+    if viewpoint is not None:
+        for i in range(3):
+            o.viewpoint[i] = float(viewpoint[i])
+    o.refine = int(bool(refine))
+    o.normalize = int(bool(normalize))
+    o.feature_mask = int(feature_mask)
+    o.mode = int(mode)
+    o.stride = int(stride)
+    o.optimized = int(bool(optimized))
+    return o
+
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the native library; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"native library {path} is missing; build it with "
+            "`python -m gpupdal_b200.build` (there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    u64 = ctypes.c_uint64
+    i32 = ctypes.c_int32
+    lib.nbg_version.restype = ctypes.c_char_p
+    lib.nbg_device_count.restype = ctypes.c_int
+    lib.nbg_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, u64]
+    lib.nbg_create.restype = ctypes.c_int
+    lib.nbg_destroy.argtypes = [vp]
+    lib.nbg_destroy.restype = ctypes.c_int
+    lib.nbg_last_error.argtypes = [vp]
+    lib.nbg_last_error.restype = ctypes.c_char_p
+    lib.nbg_tile_upload.argtypes = [vp, vp, vp, vp, u64, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double), i32, vp,
+                                    ctypes.POINTER(vp)]
+    lib.nbg_tile_upload.restype = ctypes.c_int
+    lib.nbg_tile_free.argtypes = [vp, vp]
+    lib.nbg_tile_free.restype = ctypes.c_int
+    lib.nbg_tile_size.argtypes = [vp]
+    lib.nbg_tile_size.restype = u64
+    lib.nbg_run.argtypes = [vp, vp, ctypes.POINTER(StageOpts), i32, ctypes.POINTER(Columns),
+                            vp, vp, i32, ctypes.POINTER(RowException), ctypes.c_uint32,
+                            ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(RunStats), vp]
+    lib.nbg_run.restype = ctypes.c_int
+    lib.nbg_neighbor_sets.argtypes = [vp, vp, i32, vp, i32, ctypes.POINTER(RunStats), vp]
+    lib.nbg_neighbor_sets.restype = ctypes.c_int
+    _LIB = lib
+    return lib

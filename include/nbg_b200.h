@@ -1,0 +1,185 @@
+/*
+ * nbg_b200.h — C ABI of the B200 neighbourhood-geometry library.
+ *
+ * The library computes, for every point of a tile, its k nearest neighbours,
+ * their 3x3 covariance and its symmetric eigendecomposition, and projects the
+ * result into the output dimensions of PDAL's filters.normal,
+ * filters.eigenvalues and filters.covariancefeatures.  Everything runs on one
+ * sm_100a GPU; there is no CPU fallback.
+ *
+ * Reference interfaces replaced (paths inside the PDAL fork):
+ *   - filters/NormalFilter.cpp:85-182          (options, compute loop)
+ *   - filters/EigenvaluesFilter.cpp:77-172     (options, filter loop)
+ *   - filters/CovarianceFeaturesFilter.cpp:102-367 (options, setDimensionality)
+ *   - pdal/private/KDImpl.hpp:351-381          (KD3ImplT::neighbors)
+ *   - pdal/private/MathUtils.cpp:139-196,572-611 (computeCovariance, findNormal)
+ *   - src/pdal/PdgNeighborhood.hpp:210-219,289-292 (fork's tryCuda*Columns seam)
+ *
+ * Conventions
+ *   - Return codes are int: NBG_OK (0) or one of NBG_ERR_*.  The text of the
+ *     last error of a context is available from nbg_last_error().
+ *   - Coordinates enter as LAS-style raw int32 triples plus scale and offset;
+ *     the value the reference sees is raw*scale+offset evaluated in double
+ *     (pdal/pdal_types.hpp:192-193, io/private/las/Utils.cpp:527-529).
+ *   - Neighbour counts include the query point (NormalFilter.cpp:135,
+ *     EigenvaluesFilter.cpp:139, CovarianceFeaturesFilter.cpp:228).
+ *   - Output dimensions are written as double into caller memory described
+ *     by nbg_columns (base + id*point_stride + offset[d]); rows the reference
+ *     skips are left untouched and reported in the row-exception list.
+ */
+#ifndef NBG_B200_H
+#define NBG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ---------------------------------------------------- */
+#define NBG_OK 0
+#define NBG_ERR_INVALID 1     /* invalid argument or stage option          */
+#define NBG_ERR_OOM 2         /* device allocation failed                  */
+#define NBG_ERR_BUDGET 3      /* request exceeds the context's HBM budget  */
+#define NBG_ERR_CUDA 4        /* CUDA runtime error                        */
+#define NBG_ERR_TIMEOUT 5     /* a bounded device-side wait expired        */
+#define NBG_ERR_UNSUPPORTED 6 /* input outside the supported domain        */
+#define NBG_ERR_NO_DEVICE 7   /* no sm_100 device available                */
+#define NBG_ERR_EXCEPTIONS 8  /* row-exception list overflowed             */
+
+/* ---- stage kinds ----------------------------------------------------- */
+#define NBG_STAGE_NORMAL 1             /* NormalX, NormalY, NormalZ, Curvature */
+#define NBG_STAGE_EIGENVALUES 2        /* Eigenvalue0, Eigenvalue1, Eigenvalue2 */
+#define NBG_STAGE_COVARIANCEFEATURES 3 /* selected features, bit order below */
+
+/* covariance feature bits, in the order of feature_set "all"
+ * (CovarianceFeaturesFilter.cpp:127-133) */
+#define NBG_FEAT_LINEARITY (1u << 0)
+#define NBG_FEAT_PLANARITY (1u << 1)
+#define NBG_FEAT_SCATTERING (1u << 2)
+#define NBG_FEAT_VERTICALITY (1u << 3)
+#define NBG_FEAT_OMNIVARIANCE (1u << 4)
+#define NBG_FEAT_ANISOTROPY (1u << 5)
+#define NBG_FEAT_EIGENENTROPY (1u << 6)
+#define NBG_FEAT_EIGENVALUESUM (1u << 7)
+#define NBG_FEAT_SURFACEVARIATION (1u << 8)
+#define NBG_FEAT_DEMANTKEVERTICALITY (1u << 9)
+#define NBG_FEAT_DENSITY (1u << 10)
+#define NBG_FEAT_DIMENSIONALITY 0x0Fu
+#define NBG_FEAT_ALL 0x7FFu
+#define NBG_NUM_FEATURES 11
+
+/* eigenvalue modes (CovarianceFeaturesFilter.cpp:71-86) */
+#define NBG_MODE_RAW 0
+#define NBG_MODE_SQRT 1
+#define NBG_MODE_NORMALIZED 2
+
+/* per-row exception codes; the stage shim turns them into the reference's
+ * log lines or exceptions */
+#define NBG_ROW_TOO_FEW 1       /* findNormal: fewer than 3 neighbours        */
+#define NBG_ROW_ZERO_COV 2      /* covariance isZero() (|b_ij| <= 1e-12)      */
+#define NBG_ROW_EIGEN_FAIL 3    /* eigensolver reported failure               */
+#define NBG_ROW_ZERO_LAMBDA 4   /* covariancefeatures: largest eigenvalue 0   */
+
+#define NBG_MAX_DIMS 16
+
+/* Options of one stage, same names and meaning as the reference's
+ * ProgramArgs (NormalFilter.cpp:85-97, EigenvaluesFilter.cpp:77-87,
+ * CovarianceFeaturesFilter.cpp:102-113).  `knn` is the user's value; the
+ * library adds the query point itself. */
+typedef struct nbg_stage_opts {
+    int32_t kind;          /* NBG_STAGE_*                                    */
+    int32_t knn;           /* k nearest neighbours, excluding the point      */
+    int32_t always_up;     /* normal: flip so that NormalZ >= 0              */
+    int32_t has_viewpoint; /* normal: orient towards viewpoint[]             */
+    double viewpoint[3];
+    int32_t refine;        /* normal: accepted, output-neutral (see DESIGN)  */
+    int32_t normalize;     /* eigenvalues: divide by their sum               */
+    uint32_t feature_mask; /* covariancefeatures: NBG_FEAT_* bits            */
+    int32_t mode;          /* covariancefeatures: NBG_MODE_*                 */
+    int32_t stride;        /* keep every stride-th of knn*stride neighbours  */
+    int32_t optimized;     /* covariancefeatures: per-point k = OptimalKNN   */
+} nbg_stage_opts;
+
+/* Output placement: dimension d of point id is the double at
+ *   (char*)base + id*point_stride + offset[d].
+ * A PDAL row layout is point_stride = record size; a column layout is
+ * point_stride = 8 and offset[d] = d*n*8. */
+typedef struct nbg_columns {
+    void* base;
+    int64_t point_stride;
+    int32_t ndims;
+    int32_t on_device;     /* 1: base is device memory; 0: host memory      */
+    int64_t offset[NBG_MAX_DIMS];
+} nbg_columns;
+
+/* One row the reference would skip or reject. */
+typedef struct nbg_row_exception {
+    uint32_t point_id;
+    uint8_t stage;         /* index into the stage array of the call         */
+    uint8_t code;          /* NBG_ROW_*                                      */
+    uint16_t reserved;
+} nbg_row_exception;
+
+/* Per-call counters (filled by nbg_run when non-null). */
+typedef struct nbg_run_stats {
+    uint64_t points;          /* queries answered                               */
+    uint64_t tie_rows;        /* rows whose k-th boundary tied (exact KD path)  */
+    uint64_t deferred_rows;   /* rows answered by the wide ring search          */
+    uint64_t resolved_rows;   /* rows re-solved in FP64                         */
+    double grid_ms;           /* device time of the grid build                  */
+    double query_ms;          /* device time of the fused query kernel(s)       */
+    double tree_ms;           /* device time of the KD replica build + DFS      */
+    double total_ms;          /* device time of the whole call                  */
+} nbg_run_stats;
+
+typedef struct nbg_context nbg_context;
+typedef struct nbg_tile nbg_tile;
+
+/* Library and device ------------------------------------------------------ */
+const char* nbg_version(void);
+int nbg_device_count(void);
+
+/* Context: owns device scratch, resident tiles and the HBM budget.
+ * Replaces the fork's resident neighbourhood lifetime
+ * (src/pdal/PdgNeighborhood.cpp:1383-1550). */
+int nbg_create(nbg_context** ctx, int device, uint64_t hbm_budget_bytes);
+int nbg_destroy(nbg_context* ctx);
+const char* nbg_last_error(const nbg_context* ctx);
+
+/* Tile: a point set with its uniform grid, resident on the device.
+ * x/y/z are raw int32 coordinates (host or device memory, `on_device`).
+ * Replaces PointView::build3dIndex (pdal/PointView.cpp:264-290) and the
+ * fork's SpatialIndex::build (src/index/SpatialIndexKernels.cu:1772-1906). */
+int nbg_tile_upload(nbg_context* ctx, const int32_t* x, const int32_t* y,
+                    const int32_t* z, uint64_t n, const double scale[3],
+                    const double offset[3], int32_t on_device, void* stream,
+                    nbg_tile** tile);
+int nbg_tile_free(nbg_context* ctx, nbg_tile* tile);
+uint64_t nbg_tile_size(const nbg_tile* tile);
+
+/* Run stages over a resident tile.  Stages sharing knn share one fused
+ * kNN + covariance + eigen pass.  `optimal_knn`/`optimal_radius` are the
+ * per-point OptimalKNN / OptimalRadius input columns (double, indexed by
+ * point id, host or device per `aux_on_device`), needed only for the
+ * Density feature and for `optimized`.  Replaces the per-point loops at
+ * NormalFilter.cpp:140-182, EigenvaluesFilter.cpp:115-172 and
+ * CovarianceFeaturesFilter.cpp:175-367. */
+int nbg_run(nbg_context* ctx, nbg_tile* tile, const nbg_stage_opts* stages,
+            int32_t n_stages, const nbg_columns* outputs,
+            const double* optimal_knn, const double* optimal_radius,
+            int32_t aux_on_device, nbg_row_exception* exceptions,
+            uint32_t exception_capacity, uint32_t* n_exceptions,
+            nbg_run_stats* stats, void* stream);
+
+/* Neighbour ids of every point (sorted ascending per row, `rows` x `k1`
+ * uint32, k1 = min(knn+1, n)), for parity checks against KD3Index. */
+int nbg_neighbor_sets(nbg_context* ctx, nbg_tile* tile, int32_t knn,
+                      uint32_t* ids_out, int32_t ids_on_device,
+                      nbg_run_stats* stats, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBG_B200_H */
