@@ -175,5 +175,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_run.restype = ctypes.c_int
     lib.nbg_neighbor_sets.argtypes = [vp, vp, i32, vp, i32, ctypes.POINTER(RunStats), vp]
     lib.nbg_neighbor_sets.restype = ctypes.c_int
+    lib.nbg_debug_kd_export.argtypes = [vp, vp] + [vp] * 9 + [ctypes.c_uint32]
+    lib.nbg_debug_kd_export.restype = ctypes.c_int
     _LIB = lib
     return lib

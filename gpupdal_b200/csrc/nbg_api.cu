@@ -1,0 +1,565 @@
+// nbg_api.cu — the C ABI declared in include/nbg_b200.h.
+//
+// Orchestrates one call the way the reference's stage loop does
+// (filters/NormalFilter.cpp:288-299 filter(), EigenvaluesFilter.cpp:115,
+// CovarianceFeaturesFilter.cpp:175): index the view, then answer every point;
+// stages sharing a neighbour count share one fused pass, as later PDAL
+// stages reuse the view's KD3 index (pdal/PointView.cpp:276-290).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "nbg_internal.h"
+
+struct nbg_context {
+    nbg::Context c;
+};
+struct nbg_tile {
+    nbg::Tile t;
+};
+
+namespace nbg {
+
+static int fail(Context* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+static int cuda_fail(Context* c, cudaError_t e, const char* what) {
+    return fail(c, NBG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define NBG_TRY(call, what)                               \
+    do {                                                  \
+        cudaError_t e__ = (call);                         \
+        if (e__ != cudaSuccess) return cuda_fail(ctx, e__, what); \
+    } while (0)
+
+static int dev_alloc(Context* ctx, void** p, size_t bytes, uint64_t* account) {
+    if (bytes == 0) bytes = 16;
+    if (ctx->budget && ctx->used + bytes > ctx->budget)
+        return fail(ctx, NBG_ERR_BUDGET, "HBM budget exceeded");
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(ctx, NBG_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    ctx->used += bytes;
+    if (account) *account += bytes;
+    return NBG_OK;
+}
+
+static void dev_free(Context* ctx, void* p, size_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    if (bytes == 0) bytes = 16;
+    ctx->used = ctx->used >= bytes ? ctx->used - bytes : 0;
+}
+
+static int ensure_scratch(Context* ctx, uint64_t n, uint64_t ex_cap) {
+    if (ctx->exact_cap < n) {
+        if (ctx->exact_rows) dev_free(ctx, ctx->exact_rows, ctx->exact_cap * 4);
+        ctx->exact_rows = nullptr;
+        ctx->exact_cap = 0;
+        int rc = dev_alloc(ctx, (void**)&ctx->exact_rows, std::max<uint64_t>(n, 1024) * 4, nullptr);
+        if (rc) return rc;
+        ctx->exact_cap = std::max<uint64_t>(n, 1024);
+    }
+    if (ctx->ex_cap < ex_cap) {
+        if (ctx->ex_rows) dev_free(ctx, ctx->ex_rows, ctx->ex_cap * sizeof(nbg_row_exception));
+        ctx->ex_rows = nullptr;
+        ctx->ex_cap = 0;
+        int rc = dev_alloc(ctx, (void**)&ctx->ex_rows, ex_cap * sizeof(nbg_row_exception), nullptr);
+        if (rc) return rc;
+        ctx->ex_cap = ex_cap;
+    }
+    return NBG_OK;
+}
+
+static void tile_release(Context* ctx, Tile* t) {
+    kd_free(ctx, t);
+    dev_free(ctx, t->x, t->n * 4);
+    dev_free(ctx, t->y, t->n * 4);
+    dev_free(ctx, t->z, t->n * 4);
+    dev_free(ctx, t->bbox, 64);
+    dev_free(ctx, t->gp, sizeof(GridParams));
+    dev_free(ctx, t->keys, t->n * 4);
+    dev_free(ctx, t->cell_start, (t->ncells_cap + 1) * 4);
+    dev_free(ctx, t->cursor, (t->ncells_cap + 1) * 4);
+    dev_free(ctx, t->sorted, t->n * 16);
+    dev_free(ctx, t->scan_tmp, t->scan_tmp_bytes);
+    t->x = t->y = t->z = nullptr;
+}
+
+static int ndims_of(const nbg_stage_opts& o) {
+    if (o.kind == NBG_STAGE_NORMAL) return 4;
+    if (o.kind == NBG_STAGE_EIGENVALUES) return 3;
+    return __builtin_popcount(o.feature_mask & NBG_FEAT_ALL);
+}
+
+}  // namespace nbg
+
+using namespace nbg;
+
+extern "C" {
+
+const char* nbg_version(void) { return "nbg-b200 0.1 sm_100a"; }
+
+int nbg_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int good = 0;
+    for (int d = 0; d < n; ++d) {
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10) ++good;
+    }
+    return good;
+}
+
+int nbg_create(nbg_context** out, int device, uint64_t hbm_budget_bytes) {
+    if (!out) return NBG_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return NBG_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, device) != cudaSuccess || p.major != 10) return NBG_ERR_NO_DEVICE;
+    nbg_context* h = new (std::nothrow) nbg_context();
+    if (!h) return NBG_ERR_OOM;
+    Context* ctx = &h->c;
+    ctx->device = device;
+    ctx->sm_count = p.multiProcessorCount;
+    ctx->budget = hbm_budget_bytes;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete h;
+        return NBG_ERR_CUDA;
+    }
+    for (int i = 0; i < 8; ++i) cudaEventCreate(&ctx->ev[i]);
+    ctx->events = true;
+    if (dev_alloc(ctx, (void**)&ctx->counters, 64 * sizeof(uint32_t), nullptr)) {
+        delete h;
+        return NBG_ERR_OOM;
+    }
+    *out = h;
+    return NBG_OK;
+}
+
+int nbg_destroy(nbg_context* h) {
+    if (!h) return NBG_ERR_INVALID;
+    Context* ctx = &h->c;
+    cudaSetDevice(ctx->device);
+    dev_free(ctx, ctx->exact_rows, ctx->exact_cap * 4);
+    dev_free(ctx, ctx->ex_rows, ctx->ex_cap * sizeof(nbg_row_exception));
+    dev_free(ctx, ctx->counters, 64 * sizeof(uint32_t));
+    if (ctx->events)
+        for (int i = 0; i < 8; ++i) cudaEventDestroy(ctx->ev[i]);
+    delete h;
+    return NBG_OK;
+}
+
+const char* nbg_last_error(const nbg_context* h) { return h ? h->c.err.c_str() : "no context"; }
+
+uint64_t nbg_tile_size(const nbg_tile* t) { return t ? t->t.n : 0; }
+
+int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const int32_t* z,
+                    uint64_t n, const double scale[3], const double offset[3], int32_t on_device,
+                    void* stream_v, nbg_tile** out) {
+    if (!h || !out) return NBG_ERR_INVALID;
+    Context* ctx = &h->c;
+    *out = nullptr;
+    if (n > 0 && (!x || !y || !z)) return fail(ctx, NBG_ERR_INVALID, "null coordinate array");
+    if (n >= 0x7FFFFFF0ull) return fail(ctx, NBG_ERR_UNSUPPORTED, "tile larger than 2^31 points");
+    if (!scale || !offset) return fail(ctx, NBG_ERR_INVALID, "null scale/offset");
+    for (int d = 0; d < 3; ++d)
+        if (!(scale[d] > 0.0) || !std::isfinite(scale[d]) || !std::isfinite(offset[d]))
+            return fail(ctx, NBG_ERR_INVALID, "scale must be positive and finite");
+    if (scale[0] != scale[1] || scale[0] != scale[2])
+        return fail(ctx, NBG_ERR_UNSUPPORTED,
+                    "the integer distance order needs one scale for x, y and z");
+    cudaSetDevice(ctx->device);
+    cudaStream_t stream = (cudaStream_t)stream_v;
+    nbg_tile* th = new (std::nothrow) nbg_tile();
+    if (!th) return NBG_ERR_OOM;
+    Tile* t = &th->t;
+    t->n = n;
+    for (int d = 0; d < 3; ++d) {
+        t->tf.scale[d] = scale[d];
+        t->tf.offset[d] = offset[d];
+    }
+    t->ncells_cap = 2 * n + 1024;
+    int rc = NBG_OK;
+#define ALLOC(PTR_, NBYTES_) \
+    if (!rc) rc = dev_alloc(ctx, (void**)&(PTR_), (NBYTES_), &t->bytes);
+    ALLOC(t->x, n * 4);
+    ALLOC(t->y, n * 4);
+    ALLOC(t->z, n * 4);
+    ALLOC(t->bbox, 64);
+    ALLOC(t->gp, sizeof(GridParams));
+    ALLOC(t->keys, n * 4);
+    ALLOC(t->cell_start, (t->ncells_cap + 1) * 4);
+    ALLOC(t->cursor, (t->ncells_cap + 1) * 4);
+    ALLOC(t->sorted, n * 16);
+    t->scan_tmp_bytes = scan_temp_bytes(t->ncells_cap + 1);
+    ALLOC(t->scan_tmp, t->scan_tmp_bytes);
+#undef ALLOC
+    if (rc) {
+        tile_release(ctx, t);
+        delete th;
+        return rc;
+    }
+    if (n) {
+        cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        cudaError_t e = cudaMemcpyAsync(t->x, x, n * 4, kind, stream);
+        if (!e) e = cudaMemcpyAsync(t->y, y, n * 4, kind, stream);
+        if (!e) e = cudaMemcpyAsync(t->z, z, n * 4, kind, stream);
+        if (e) {
+            tile_release(ctx, t);
+            delete th;
+            return cuda_fail(ctx, e, "coordinate upload");
+        }
+    }
+    *out = th;
+    return NBG_OK;
+}
+
+int nbg_tile_free(nbg_context* h, nbg_tile* th) {
+    if (!h || !th) return NBG_ERR_INVALID;
+    cudaSetDevice(h->c.device);
+    tile_release(&h->c, &th->t);
+    delete th;
+    return NBG_OK;
+}
+
+}  // extern "C"
+
+namespace nbg {
+
+// Grid for neighbour count k1 (rebuilt when k1 moves far from the build's).
+static int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
+    if (t->grid_valid && k1 <= 2 * t->grid_k1 && 2 * k1 >= t->grid_k1) return NBG_OK;
+    int rc = build_grid(ctx, t, k1, stream);
+    if (rc) return fail(ctx, rc, "grid build failed");
+    NBG_TRY(cudaMemcpyAsync(&t->host_gp, t->gp, sizeof(GridParams), cudaMemcpyDeviceToHost, stream),
+            "grid params");
+    NBG_TRY(cudaStreamSynchronize(stream), "grid build");
+    const GridParams& g = t->host_gp;
+    if ((int64_t)g.maxx - g.minx >= (1 << 24) || (int64_t)g.maxy - g.miny >= (1 << 24) ||
+        (int64_t)g.maxz - g.minz >= (1 << 24))
+        return fail(ctx, NBG_ERR_UNSUPPORTED, "tile extent must be below 2^24 raw units per axis");
+    t->grid_valid = true;
+    t->grid_k1 = k1;
+    return NBG_OK;
+}
+
+struct HostOut {
+    const nbg_columns* user;
+    char* dev = nullptr;  // device staging (host outputs only)
+    size_t bytes = 0;
+};
+
+}  // namespace nbg
+
+extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stages,
+                       int32_t n_stages, const nbg_columns* outputs, const double* optimal_knn,
+                       const double* optimal_radius, int32_t aux_on_device,
+                       nbg_row_exception* exceptions, uint32_t exception_capacity,
+                       uint32_t* n_exceptions, nbg_run_stats* stats, void* stream_v) {
+    if (!h || !th) return NBG_ERR_INVALID;
+    Context* ctx = &h->c;
+    Tile* t = &th->t;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t stream = (cudaStream_t)stream_v;
+    if (n_exceptions) *n_exceptions = 0;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (n_stages < 0 || n_stages > NBG_MAX_STAGES || (n_stages && (!stages || !outputs)))
+        return fail(ctx, NBG_ERR_INVALID, "bad stage array");
+    bool need_aux = false;
+    for (int s = 0; s < n_stages; ++s) {
+        const nbg_stage_opts& o = stages[s];
+        if (o.kind < 1 || o.kind > 3) return fail(ctx, NBG_ERR_INVALID, "unknown stage kind");
+        if (o.knn < 0 || o.knn > 64)
+            return fail(ctx, NBG_ERR_INVALID, "knn must be in [0, 64]");
+        if (o.kind != NBG_STAGE_NORMAL && o.stride != 1 && o.stride != 0)
+            return fail(ctx, NBG_ERR_UNSUPPORTED, "stride > 1 is not supported");
+        if (o.kind == NBG_STAGE_COVARIANCEFEATURES && o.optimized)
+            return fail(ctx, NBG_ERR_UNSUPPORTED, "optimized is not supported");
+        if (o.kind == NBG_STAGE_COVARIANCEFEATURES &&
+            (o.mode < NBG_MODE_RAW || o.mode > NBG_MODE_NORMALIZED))
+            return fail(ctx, NBG_ERR_INVALID, "invalid mode");
+        if (outputs[s].ndims != ndims_of(o))
+            return fail(ctx, NBG_ERR_INVALID, "output ndims does not match the stage");
+        if (o.kind == NBG_STAGE_COVARIANCEFEATURES && (o.feature_mask & NBG_FEAT_DENSITY))
+            need_aux = true;
+    }
+    if (need_aux && (!optimal_knn || !optimal_radius))
+        return fail(ctx, NBG_ERR_INVALID, "Density needs OptimalKNN and OptimalRadius");
+    const uint64_t n = t->n;
+    if (n == 0 || n_stages == 0) return NBG_OK;
+    int rc = ensure_scratch(ctx, n, std::max<uint64_t>(exception_capacity, 1));
+    if (rc) return rc;
+
+    // host-side outputs: device staging in column layout, copied back after
+    std::vector<HostOut> hout(n_stages);
+    std::vector<nbg_columns> dcols(n_stages);
+    double* aux_dev[2] = {nullptr, nullptr};
+    auto cleanup = [&]() {
+        for (auto& o : hout)
+            if (o.dev) dev_free(ctx, o.dev, o.bytes);
+        if (!aux_on_device) {
+            if (aux_dev[0]) dev_free(ctx, aux_dev[0], n * 8);
+            if (aux_dev[1]) dev_free(ctx, aux_dev[1], n * 8);
+        }
+    };
+    for (int s = 0; s < n_stages; ++s) {
+        hout[s].user = &outputs[s];
+        dcols[s] = outputs[s];
+        if (outputs[s].on_device != 1 && outputs[s].ndims > 0) {
+            hout[s].bytes = n * 8 * outputs[s].ndims;
+            rc = dev_alloc(ctx, (void**)&hout[s].dev, hout[s].bytes, nullptr);
+            if (rc) { cleanup(); return rc; }
+            dcols[s].base = hout[s].dev;
+            dcols[s].point_stride = 8;
+            dcols[s].on_device = 1;
+            for (int d = 0; d < outputs[s].ndims; ++d) dcols[s].offset[d] = (int64_t)d * n * 8;
+            if (outputs[s].on_device == 2) {
+                // fresh dimensions: skipped rows read 0, as in a new PDAL table
+                cudaError_t e = cudaMemsetAsync(hout[s].dev, 0, hout[s].bytes, stream);
+                if (e) { cleanup(); return cuda_fail(ctx, e, "output staging"); }
+                continue;
+            }
+            // rows the reference skips keep the caller's values
+            for (int d = 0; d < outputs[s].ndims; ++d) {
+                const nbg_columns& u = outputs[s];
+                cudaError_t e;
+                if (u.point_stride == 8)
+                    e = cudaMemcpyAsync(hout[s].dev + (size_t)d * n * 8, (char*)u.base + u.offset[d],
+                                        n * 8, cudaMemcpyHostToDevice, stream);
+                else
+                    e = cudaMemcpy2DAsync(hout[s].dev + (size_t)d * n * 8, 8,
+                                          (char*)u.base + u.offset[d], u.point_stride, 8, n,
+                                          cudaMemcpyHostToDevice, stream);
+                if (e) { cleanup(); return cuda_fail(ctx, e, "output staging"); }
+            }
+        }
+    }
+    const double* kopt = optimal_knn;
+    const double* ropt = optimal_radius;
+    if (need_aux && !aux_on_device) {
+        rc = dev_alloc(ctx, (void**)&aux_dev[0], n * 8, nullptr);
+        if (!rc) rc = dev_alloc(ctx, (void**)&aux_dev[1], n * 8, nullptr);
+        if (rc) { cleanup(); return rc; }
+        cudaMemcpyAsync(aux_dev[0], optimal_knn, n * 8, cudaMemcpyHostToDevice, stream);
+        cudaMemcpyAsync(aux_dev[1], optimal_radius, n * 8, cudaMemcpyHostToDevice, stream);
+        kopt = aux_dev[0];
+        ropt = aux_dev[1];
+    }
+
+    // group stages by neighbour count
+    std::vector<int> order(n_stages);
+    for (int s = 0; s < n_stages; ++s) order[s] = s;
+    std::vector<std::vector<int>> groups;
+    for (int s = 0; s < n_stages; ++s) {
+        const int K = (int)std::min<uint64_t>(n, (uint64_t)stages[s].knn + 1);
+        bool placed = false;
+        for (auto& gr : groups) {
+            const int K0 = (int)std::min<uint64_t>(n, (uint64_t)stages[gr[0]].knn + 1);
+            if (K0 == K) { gr.push_back(s); placed = true; break; }
+        }
+        if (!placed) groups.push_back({s});
+    }
+
+    cudaEventRecord(ctx->ev[0], stream);
+    float grid_ms = 0, query_ms = 0, tree_ms = 0;
+    uint64_t tie_rows = 0, deferred_rows = 0;
+    ExceptionSink sink{ctx->ex_rows, ctx->counters + 3, (uint32_t)std::max<uint32_t>(exception_capacity, 1)};
+    if (cudaMemsetAsync(ctx->counters, 0, 64 * sizeof(uint32_t), stream)) { cleanup(); return NBG_ERR_CUDA; }
+    for (auto& gr : groups) {
+        const int K = (int)std::min<uint64_t>(n, (uint64_t)stages[gr[0]].knn + 1);
+        cudaEventRecord(ctx->ev[1], stream);
+        rc = ensure_grid(ctx, t, K, stream);
+        if (rc) { cleanup(); return rc; }
+        cudaEventRecord(ctx->ev[2], stream);
+        StageGroup g{};
+        g.nstages = (int)gr.size();
+        g.optimal_knn = kopt;
+        g.optimal_radius = ropt;
+        for (int i = 0; i < g.nstages; ++i) {
+            const int s = gr[i];
+            const nbg_stage_opts& o = stages[s];
+            StageDev& d = g.st[i];
+            g.stage_index[i] = s;
+            d.kind = o.kind;
+            d.always_up = o.always_up;
+            d.has_viewpoint = o.has_viewpoint;
+            d.normalize = o.normalize;
+            for (int k = 0; k < 3; ++k) d.viewpoint[k] = o.viewpoint[k];
+            d.feature_mask = o.feature_mask & NBG_FEAT_ALL;
+            d.mode = o.mode;
+            d.ndims = dcols[s].ndims;
+            d.base = (char*)dcols[s].base;
+            d.point_stride = dcols[s].point_stride;
+            for (int k = 0; k < NBG_MAX_DIMS; ++k) d.offset[k] = dcols[s].offset[k];
+        }
+        if (cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(uint32_t), stream)) { cleanup(); return NBG_ERR_CUDA; }
+        QueryLaunch ql;
+        ql.tile = t;
+        ql.K = K;
+        ql.rmax = 8;
+        ql.grp = g;
+        ql.ex = sink;
+        ql.exact_rows = ctx->exact_rows;
+        ql.counters = ctx->counters;
+        rc = launch_query(ctx, ql, stream);
+        if (rc) { cleanup(); return fail(ctx, rc, std::string("query launch failed: ") +
+                                                 cudaGetErrorString(cudaGetLastError())); }
+        cudaEventRecord(ctx->ev[3], stream);
+        uint32_t cnt[3] = {0, 0, 0};
+        cudaError_t e = cudaMemcpyAsync(cnt, ctx->counters, 3 * sizeof(uint32_t),
+                                        cudaMemcpyDeviceToHost, stream);
+        if (!e) e = cudaStreamSynchronize(stream);
+        if (e) { cleanup(); return cuda_fail(ctx, e, "query kernel"); }
+        tie_rows += cnt[1];
+        deferred_rows += cnt[2];
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+        grid_ms += ms;
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        query_ms += ms;
+        if (cnt[0]) {
+            cudaEventRecord(ctx->ev[4], stream);
+            rc = kd_ensure(ctx, t, stream);
+            if (!rc) rc = kd_run_rows(ctx, t, K, g, sink, ctx->exact_rows, cnt[0], stream);
+            if (rc) { cleanup(); return rc; }
+            cudaEventRecord(ctx->ev[5], stream);
+            e = cudaStreamSynchronize(stream);
+            if (e) { cleanup(); return cuda_fail(ctx, e, "exact KD path"); }
+            cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+            tree_ms += ms;
+        }
+    }
+    // results back to host layouts
+    for (int s = 0; s < n_stages; ++s) {
+        if (!hout[s].dev) continue;
+        const nbg_columns& u = outputs[s];
+        for (int d = 0; d < u.ndims; ++d) {
+            cudaError_t e;
+            if (u.point_stride == 8)
+                e = cudaMemcpyAsync((char*)u.base + u.offset[d], hout[s].dev + (size_t)d * n * 8, n * 8,
+                                    cudaMemcpyDeviceToHost, stream);
+            else
+                e = cudaMemcpy2DAsync((char*)u.base + u.offset[d], u.point_stride,
+                                      hout[s].dev + (size_t)d * n * 8, 8, 8, n,
+                                      cudaMemcpyDeviceToHost, stream);
+            if (e) { cleanup(); return cuda_fail(ctx, e, "output copy"); }
+        }
+    }
+    uint32_t nex = 0;
+    cudaError_t e = cudaMemcpyAsync(&nex, ctx->counters + 3, 4, cudaMemcpyDeviceToHost, stream);
+    if (!e) e = cudaStreamSynchronize(stream);
+    if (e) { cleanup(); return cuda_fail(ctx, e, "exception count"); }
+    const uint32_t ncopy = std::min(nex, exception_capacity);
+    if (ncopy && exceptions) {
+        e = cudaMemcpyAsync(exceptions, ctx->ex_rows, ncopy * sizeof(nbg_row_exception),
+                            cudaMemcpyDeviceToHost, stream);
+        if (!e) e = cudaStreamSynchronize(stream);
+        if (e) { cleanup(); return cuda_fail(ctx, e, "exception copy"); }
+    }
+    cudaEventRecord(ctx->ev[6], stream);
+    cudaStreamSynchronize(stream);
+    if (n_exceptions) *n_exceptions = nex;
+    if (stats) {
+        stats->points = n * groups.size();
+        stats->tie_rows = tie_rows;
+        stats->deferred_rows = deferred_rows;
+        stats->grid_ms = grid_ms;
+        stats->query_ms = query_ms;
+        stats->tree_ms = tree_ms;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[6]);
+        stats->total_ms = ms;
+    }
+    cleanup();
+    if (nex > exception_capacity)
+        return fail(ctx, NBG_ERR_EXCEPTIONS, "row-exception list overflowed");
+    return NBG_OK;
+}
+
+extern "C" int nbg_neighbor_sets(nbg_context* h, nbg_tile* th, int32_t knn, uint32_t* ids_out,
+                                 int32_t ids_on_device, nbg_run_stats* stats, void* stream_v) {
+    if (!h || !th || !ids_out) return NBG_ERR_INVALID;
+    Context* ctx = &h->c;
+    Tile* t = &th->t;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t stream = (cudaStream_t)stream_v;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (knn < 0 || knn > 64) return fail(ctx, NBG_ERR_INVALID, "knn must be in [0, 64]");
+    const uint64_t n = t->n;
+    if (n == 0) return NBG_OK;
+    const int K = (int)std::min<uint64_t>(n, (uint64_t)knn + 1);
+    int rc = ensure_scratch(ctx, n, 1);
+    if (rc) return rc;
+    rc = ensure_grid(ctx, t, K, stream);
+    if (rc) return rc;
+    uint32_t* dev_ids = ids_out;
+    const size_t bytes = n * (size_t)K * 4;
+    if (!ids_on_device) {
+        rc = dev_alloc(ctx, (void**)&dev_ids, bytes, nullptr);
+        if (rc) return rc;
+    }
+    cudaMemsetAsync(ctx->counters, 0, 64 * sizeof(uint32_t), stream);
+    rc = launch_neighbor_sets(ctx, t, K, 8, dev_ids, ctx->exact_rows, ctx->counters, stream);
+    uint32_t cnt[3] = {0, 0, 0};
+    cudaError_t e = cudaSuccess;
+    if (!rc) {
+        e = cudaMemcpyAsync(cnt, ctx->counters, 12, cudaMemcpyDeviceToHost, stream);
+        if (!e) e = cudaStreamSynchronize(stream);
+    }
+    if (!rc && !e && cnt[0]) {
+        rc = kd_ensure(ctx, t, stream);
+        if (!rc) rc = kd_neighbor_rows(ctx, t, K, ctx->exact_rows, cnt[0], dev_ids, stream);
+    }
+    if (!rc && !e && !ids_on_device) e = cudaMemcpyAsync(ids_out, dev_ids, bytes, cudaMemcpyDeviceToHost, stream);
+    if (!e) e = cudaStreamSynchronize(stream);
+    if (!ids_on_device) dev_free(ctx, dev_ids, bytes);
+    if (stats) {
+        stats->points = n;
+        stats->tie_rows = cnt[1];
+        stats->deferred_rows = cnt[2];
+    }
+    if (rc) return rc;
+    if (e) return cuda_fail(ctx, e, "neighbour sets");
+    return NBG_OK;
+}
+
+extern "C" int nbg_debug_kd_export(nbg_context* h, nbg_tile* th, uint32_t* vind, uint32_t* n_nodes,
+                                   int32_t* child1, int32_t* child2, int32_t* divfeat,
+                                   double* divlow, double* divhigh, uint32_t* begin,
+                                   uint32_t* end, uint32_t node_capacity) {
+    if (!h || !th || !vind || !n_nodes) return NBG_ERR_INVALID;
+    Context* ctx = &h->c;
+    Tile* t = &th->t;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (t->n == 0) {
+        *n_nodes = 0;
+        return NBG_OK;
+    }
+    int rc = ensure_grid(ctx, t, (int)std::min<uint64_t>(t->n, 9), 0);
+    if (rc) return rc;
+    return kd_export(ctx, t, vind, n_nodes, child1, child2, divfeat, divlow, divhigh, begin, end,
+                     node_capacity, 0);
+}

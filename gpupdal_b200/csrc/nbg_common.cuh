@@ -1,0 +1,352 @@
+// nbg_common.cuh — shared device definitions of the B200 neighbourhood path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+#include "../../include/nbg_b200.h"
+
+#define NBG_MAX_STAGES 4
+#define NBG_MAX_RING 24
+
+// Grid of one tile, written on the device by grid_config_kernel so that the
+// build never waits on the host.  Coordinates are raw int32 relative to the
+// tile minimum; cells are cubes of `cell` raw units, keyed x-fastest so that
+// a run of cells along x is one contiguous range of the sorted points.
+struct GridParams {
+    int32_t minx, miny, minz;
+    int32_t maxx, maxy, maxz;
+    int32_t cell;
+    int32_t gx, gy, gz;
+    uint32_t ncells;
+    uint32_t cap_hit;  // cell size had to grow to fit the cell table
+};
+
+// One stage of a fused group, resolved for the device.
+struct StageDev {
+    int32_t kind;
+    int32_t always_up;
+    int32_t has_viewpoint;
+    int32_t normalize;
+    double viewpoint[3];
+    uint32_t feature_mask;
+    int32_t mode;
+    int32_t ndims;
+    int32_t pad;
+    char* base;
+    int64_t point_stride;
+    int64_t offset[NBG_MAX_DIMS];
+};
+
+struct StageGroup {
+    int32_t nstages;
+    int32_t stage_index[NBG_MAX_STAGES];  // index in the caller's array
+    StageDev st[NBG_MAX_STAGES];
+    const double* optimal_knn;     // device, may be null
+    const double* optimal_radius;  // device, may be null
+};
+
+// Per-row exception sink.
+struct ExceptionSink {
+    nbg_row_exception* rows;
+    uint32_t* count;
+    uint32_t capacity;
+};
+
+// Tile scale/offset as seen by the reference: value = raw*scale + offset.
+struct Transform {
+    double scale[3];
+    double offset[3];
+};
+
+// ---------------------------------------------------------------------------
+// The reference's coordinate, fl(fl(raw*scale) + offset), with no contraction.
+__device__ __forceinline__ double ref_coord(int32_t raw, double s, double o) {
+    return __dadd_rn(__dmul_rn((double)raw, s), o);
+}
+
+// ---------------------------------------------------------------------------
+// Eigen 3.4 SelfAdjointEigenSolver<Matrix3d> chain on the device (3x3
+// Householder tridiagonalisation, implicit symmetric QR with Wilkinson shift,
+// continuous Givens rotations, selection sort).  Keeping the same chain keeps
+// the same eigenvector signs as the reference, which filters.normal exposes
+// when always_up is false and no viewpoint is given.  evec column-major.
+__device__ __forceinline__ void nbg_make_givens(double p, double q, double& c, double& s) {
+    if (q == 0.0) {
+        c = p < 0.0 ? -1.0 : 1.0;
+        s = 0.0;
+    } else if (p == 0.0) {
+        c = 0.0;
+        s = q < 0.0 ? 1.0 : -1.0;
+    } else if (fabs(p) > fabs(q)) {
+        double t = __ddiv_rn(q, p);
+        double u = __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(t, t)));
+        if (p < 0.0) u = -u;
+        c = __ddiv_rn(1.0, u);
+        s = __dmul_rn(-t, c);
+    } else {
+        double t = __ddiv_rn(p, q);
+        double u = __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(t, t)));
+        if (q < 0.0) u = -u;
+        s = __ddiv_rn(-1.0, u);
+        c = __dmul_rn(-t, s);
+    }
+}
+
+__device__ __forceinline__ double nbg_pos_hypot(double x, double y) {
+    double p = fmax(x, y);
+    if (p == 0.0) return 0.0;
+    double qp = __ddiv_rn(fmin(y, x), p);
+    return __dmul_rn(p, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(qp, qp))));
+}
+
+// a: symmetric 3x3 (a00,a10,a11,a20,a21,a22 lower triangle).  Returns 1 on
+// success.  eval ascending; evec[c*3+r].
+__device__ inline int nbg_eigen_chain(const double low[6], double eval[3], double evec[9]) {
+    double m00 = low[0], m10 = low[1], m11 = low[2], m20 = low[3], m21 = low[4], m22 = low[5];
+    double scale = fmax(fmax(fmax(fabs(m00), fabs(m10)), fmax(fabs(m11), fabs(m20))),
+                        fmax(fabs(m21), fabs(m22)));
+    if (scale == 0.0) scale = 1.0;
+    m00 = __ddiv_rn(m00, scale);
+    m10 = __ddiv_rn(m10, scale);
+    m11 = __ddiv_rn(m11, scale);
+    m20 = __ddiv_rn(m20, scale);
+    m21 = __ddiv_rn(m21, scale);
+    m22 = __ddiv_rn(m22, scale);
+    double diag[3], sub[2];
+    double Q[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    diag[0] = m00;
+    double v1norm2 = __dmul_rn(m20, m20);
+    if (v1norm2 <= DBL_MIN) {
+        diag[1] = m11;
+        diag[2] = m22;
+        sub[0] = m10;
+        sub[1] = m21;
+    } else {
+        double beta = __dsqrt_rn(__dadd_rn(__dmul_rn(m10, m10), v1norm2));
+        double invBeta = __ddiv_rn(1.0, beta);
+        double m01 = __dmul_rn(m10, invBeta);
+        double m02 = __dmul_rn(m20, invBeta);
+        double q = __dadd_rn(__dmul_rn(__dmul_rn(2.0, m01), m21),
+                             __dmul_rn(m02, __dsub_rn(m22, m11)));
+        diag[1] = __dadd_rn(m11, __dmul_rn(m02, q));
+        diag[2] = __dsub_rn(m22, __dmul_rn(m02, q));
+        sub[0] = beta;
+        sub[1] = __dsub_rn(m21, __dmul_rn(m01, q));
+        Q[4] = m01;
+        Q[5] = m02;
+        Q[7] = m02;
+        Q[8] = -m01;
+    }
+    int end = 2, start = 0, iter = 0;
+    const double precision_inv = 1.0 / DBL_EPSILON;
+    while (end > 0) {
+        for (int i = start; i < end; ++i) {
+            if (fabs(sub[i]) < DBL_MIN) sub[i] = 0.0;
+            else {
+                double sc = __dmul_rn(precision_inv, sub[i]);
+                if (__dmul_rn(sc, sc) <= __dadd_rn(fabs(diag[i]), fabs(diag[i + 1]))) sub[i] = 0.0;
+            }
+        }
+        while (end > 0 && sub[end - 1] == 0.0) end--;
+        if (end <= 0) break;
+        iter++;
+        if (iter > 90) break;
+        start = end - 1;
+        while (start > 0 && sub[start - 1] != 0.0) start--;
+        double td = __dmul_rn(__dsub_rn(diag[end - 1], diag[end]), 0.5);
+        double e = sub[end - 1];
+        double mu = diag[end];
+        if (td == 0.0) {
+            mu = __dsub_rn(mu, fabs(e));
+        } else if (e != 0.0) {
+            double e2 = __dmul_rn(e, e);
+            double h = nbg_pos_hypot(fabs(td), fabs(e));
+            double den = __dadd_rn(td, td > 0.0 ? h : -h);
+            if (e2 == 0.0) mu = __dsub_rn(mu, __ddiv_rn(e, __ddiv_rn(den, e)));
+            else mu = __dsub_rn(mu, __ddiv_rn(e2, den));
+        }
+        double x = __dsub_rn(diag[start], mu);
+        double z = sub[start];
+        for (int k = start; k < end && z != 0.0; ++k) {
+            double c, s;
+            nbg_make_givens(x, z, c, s);
+            double sdk = __dadd_rn(__dmul_rn(s, diag[k]), __dmul_rn(c, sub[k]));
+            double dkp1 = __dadd_rn(__dmul_rn(s, sub[k]), __dmul_rn(c, diag[k + 1]));
+            double t1 = __dsub_rn(__dmul_rn(c, diag[k]), __dmul_rn(s, sub[k]));
+            double t2 = __dsub_rn(__dmul_rn(c, sub[k]), __dmul_rn(s, diag[k + 1]));
+            diag[k] = __dsub_rn(__dmul_rn(c, t1), __dmul_rn(s, t2));
+            diag[k + 1] = __dadd_rn(__dmul_rn(s, sdk), __dmul_rn(c, dkp1));
+            sub[k] = __dsub_rn(__dmul_rn(c, sdk), __dmul_rn(s, dkp1));
+            if (k > start) sub[k - 1] = __dsub_rn(__dmul_rn(c, sub[k - 1]), __dmul_rn(s, z));
+            x = sub[k];
+            if (k < end - 1) {
+                z = __dmul_rn(-s, sub[k + 1]);
+                sub[k + 1] = __dmul_rn(c, sub[k + 1]);
+            }
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                double xi = Q[k * 3 + r], yi = Q[(k + 1) * 3 + r];
+                Q[k * 3 + r] = __dsub_rn(__dmul_rn(c, xi), __dmul_rn(s, yi));
+                Q[(k + 1) * 3 + r] = __dadd_rn(__dmul_rn(s, xi), __dmul_rn(c, yi));
+            }
+        }
+    }
+    int ok = iter <= 90;
+    if (ok) {
+        for (int i = 0; i < 2; ++i) {
+            int k = i;
+            for (int j = i + 1; j < 3; ++j)
+                if (diag[j] < diag[k]) k = j;
+            if (k != i) {
+                double t = diag[i];
+                diag[i] = diag[k];
+                diag[k] = t;
+                for (int r = 0; r < 3; ++r) {
+                    double u = Q[i * 3 + r];
+                    Q[i * 3 + r] = Q[k * 3 + r];
+                    Q[k * 3 + r] = u;
+                }
+            }
+        }
+    }
+    eval[0] = __dmul_rn(diag[0], scale);
+    eval[1] = __dmul_rn(diag[1], scale);
+    eval[2] = __dmul_rn(diag[2], scale);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) evec[i] = Q[i];
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+// Row epilogue shared by the grid path and the exact KD path.
+//
+// M = n*S2 - S1*S1^T over the neighbours' raw offsets from the query (exact
+// int64), so cov = M * s_i*s_j / (n*(n-1)).  Writes every stage's outputs,
+// or appends the reference's skip/throw code to the exception sink.
+__device__ inline void nbg_append_exception(const ExceptionSink& ex, uint32_t id, int stage,
+                                            int code) {
+    uint32_t slot = atomicAdd(ex.count, 1u);
+    if (slot < ex.capacity) {
+        nbg_row_exception r;
+        r.point_id = id;
+        r.stage = (uint8_t)stage;
+        r.code = (uint8_t)code;
+        r.reserved = 0;
+        ex.rows[slot] = r;
+    }
+}
+
+__device__ __forceinline__ void nbg_store(const StageDev& st, uint32_t id, int d, double v) {
+    *reinterpret_cast<double*>(st.base + (int64_t)id * st.point_stride + st.offset[d]) = v;
+}
+
+__device__ inline void nbg_finish_row(const StageGroup& g, const Transform& tf,
+                                      const ExceptionSink& ex, uint32_t id, int nnb,
+                                      const long long M[6], const int32_t qraw[3]) {
+    // covariance as the reference forms it, up to its float narrowing
+    const double s0 = tf.scale[0], s1 = tf.scale[1], s2 = tf.scale[2];
+    double denom = (double)nnb * (double)(nnb - 1);
+    double C[6];  // c00, c10, c11, c20, c21, c22
+    C[0] = (double)M[0] * (s0 * s0) / denom;
+    C[1] = (double)M[1] * (s1 * s0) / denom;
+    C[2] = (double)M[2] * (s1 * s1) / denom;
+    C[3] = (double)M[3] * (s2 * s0) / denom;
+    C[4] = (double)M[4] * (s2 * s1) / denom;
+    C[5] = (double)M[5] * (s2 * s2) / denom;
+    bool zero = true;
+    int nonfinite = nnb <= 1;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) zero = zero && (fabs(C[i]) <= 1e-12);
+    if (nnb <= 1) zero = false;
+    if (nnb == 0) zero = true;
+    double ev[3] = {0, 0, 0}, V[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int ok = 1;
+    if (!zero) {
+        if (nonfinite) ok = 0;
+        else ok = nbg_eigen_chain(C, ev, V);
+    }
+    double p[3] = {ref_coord(qraw[0], tf.scale[0], tf.offset[0]),
+                   ref_coord(qraw[1], tf.scale[1], tf.offset[1]),
+                   ref_coord(qraw[2], tf.scale[2], tf.offset[2])};
+    for (int si = 0; si < g.nstages; ++si) {
+        const StageDev& st = g.st[si];
+        const int sidx = g.stage_index[si];
+        if (st.kind == NBG_STAGE_NORMAL) {
+            if (nnb < 3) { nbg_append_exception(ex, id, sidx, NBG_ROW_TOO_FEW); continue; }
+            if (zero) { nbg_append_exception(ex, id, sidx, NBG_ROW_ZERO_COV); continue; }
+            if (!ok) { nbg_append_exception(ex, id, sidx, NBG_ROW_EIGEN_FAIL); continue; }
+            double sum = ev[0] + ev[1] + ev[2];
+            double curv = sum != 0.0 ? fabs(ev[0] / sum) : 0.0;
+            double n0 = V[0], n1 = V[1], n2 = V[2];
+            if (st.has_viewpoint) {
+                double dx = st.viewpoint[0] - p[0];
+                double dy = st.viewpoint[1] - p[1];
+                double dz = st.viewpoint[2] - p[2];
+                double dot = __dadd_rn(__dadd_rn(__dmul_rn(dx, n0), __dmul_rn(dy, n1)),
+                                       __dmul_rn(dz, n2));
+                if (dot < 0) { n0 = -n0; n1 = -n1; n2 = -n2; }
+            } else if (st.always_up) {
+                if (n2 < 0) { n0 = -n0; n1 = -n1; n2 = -n2; }
+            }
+            nbg_store(st, id, 0, n0);
+            nbg_store(st, id, 1, n1);
+            nbg_store(st, id, 2, n2);
+            nbg_store(st, id, 3, curv);
+        } else if (st.kind == NBG_STAGE_EIGENVALUES) {
+            if (zero) { nbg_append_exception(ex, id, sidx, NBG_ROW_ZERO_COV); continue; }
+            if (!ok) { nbg_append_exception(ex, id, sidx, NBG_ROW_EIGEN_FAIL); continue; }
+            double e0 = ev[0], e1 = ev[1], e2 = ev[2];
+            if (st.normalize) {
+                double sum = e0 + e1 + e2;
+                e0 /= sum;
+                e1 /= sum;
+                e2 /= sum;
+            }
+            nbg_store(st, id, 0, e0);
+            nbg_store(st, id, 1, e1);
+            nbg_store(st, id, 2, e2);
+        } else {
+            if (zero) { nbg_append_exception(ex, id, sidx, NBG_ROW_ZERO_COV); continue; }
+            if (!ok) { nbg_append_exception(ex, id, sidx, NBG_ROW_EIGEN_FAIL); continue; }
+            double l0 = fmax(ev[2], 0.0), l1 = fmax(ev[1], 0.0), l2 = fmax(ev[0], 0.0);
+            double sum = ((0.0 + l0) + l1) + l2;
+            if (l0 == 0.0) { nbg_append_exception(ex, id, sidx, NBG_ROW_ZERO_LAMBDA); continue; }
+            if (st.mode == NBG_MODE_SQRT) {
+                l0 = sqrt(l0);
+                l1 = sqrt(l1);
+                l2 = sqrt(l2);
+            } else if (st.mode == NBG_MODE_NORMALIZED) {
+                l0 /= sum;
+                l1 /= sum;
+                l2 /= sum;
+            }
+            int w = 0;
+            const uint32_t mask = st.feature_mask;
+            if (mask & NBG_FEAT_LINEARITY) nbg_store(st, id, w++, (l0 - l1) / l0);
+            if (mask & NBG_FEAT_PLANARITY) nbg_store(st, id, w++, (l1 - l2) / l0);
+            if (mask & NBG_FEAT_SCATTERING) nbg_store(st, id, w++, l2 / l0);
+            if (mask & NBG_FEAT_VERTICALITY) {
+                double u0 = l0 * fabs(V[6]) + l1 * fabs(V[3]) + l2 * fabs(V[0]);
+                double u1 = l0 * fabs(V[7]) + l1 * fabs(V[4]) + l2 * fabs(V[1]);
+                double u2 = l0 * fabs(V[8]) + l1 * fabs(V[5]) + l2 * fabs(V[2]);
+                double norm = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
+                nbg_store(st, id, w++, u2 / norm);
+            }
+            if (mask & NBG_FEAT_OMNIVARIANCE) nbg_store(st, id, w++, cbrt(l2 * l1 * l0));
+            if (mask & NBG_FEAT_ANISOTROPY) nbg_store(st, id, w++, (l0 - l2) / l0);
+            if (mask & NBG_FEAT_EIGENENTROPY)
+                nbg_store(st, id, w++, -(l2 * log(l2) + l1 * log(l1) + l0 * log(l0)));
+            if (mask & NBG_FEAT_EIGENVALUESUM) nbg_store(st, id, w++, sum);
+            if (mask & NBG_FEAT_SURFACEVARIATION) nbg_store(st, id, w++, l2 / sum);
+            if (mask & NBG_FEAT_DEMANTKEVERTICALITY) nbg_store(st, id, w++, 1.0 - fabs(V[2]));
+            if (mask & NBG_FEAT_DENSITY) {
+                double kopt = g.optimal_knn ? g.optimal_knn[id] : 0.0;
+                double ropt = g.optimal_radius ? g.optimal_radius[id] : 0.0;
+                const double pi = 3.14159265;
+                nbg_store(st, id, w++, (kopt + 1.0) / ((4.0 / 3.0) * pi * (ropt * ropt * ropt)));
+            }
+        }
+    }
+}

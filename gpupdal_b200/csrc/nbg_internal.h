@@ -1,0 +1,90 @@
+// nbg_internal.h — host-side internals shared by the library's .cu files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "nbg_common.cuh"
+
+namespace nbg {
+
+struct KdReplica;  // exact nanoflann replica (nbg_kdtree.cu)
+
+struct Context {
+    int device = 0;
+    int sm_count = 148;
+    uint64_t budget = 0;   // HBM budget in bytes (0 = no limit)
+    uint64_t used = 0;     // bytes held by tiles and scratch
+    std::string err;
+    std::mutex mu;
+    // per-call scratch (grown on demand)
+    uint32_t* exact_rows = nullptr;
+    uint64_t exact_cap = 0;
+    uint32_t* counters = nullptr;   // [0] exact rows, [1] tie rows, [2] deferred, [3] exceptions
+    nbg_row_exception* ex_rows = nullptr;
+    uint64_t ex_cap = 0;
+    cudaEvent_t ev[8];
+    bool events = false;
+};
+
+struct Tile {
+    uint64_t n = 0;
+    int32_t* x = nullptr;
+    int32_t* y = nullptr;
+    int32_t* z = nullptr;
+    Transform tf{};
+    // grid
+    int32_t* bbox = nullptr;
+    GridParams* gp = nullptr;
+    uint32_t* keys = nullptr;
+    uint32_t* cell_start = nullptr;
+    uint32_t* cursor = nullptr;
+    float4* sorted = nullptr;
+    void* scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    uint64_t ncells_cap = 0;
+    float cell_factor = 1.0f;
+    int32_t fixed_cell = 0;
+    int grid_k1 = 0;
+    bool grid_valid = false;
+    GridParams host_gp{};
+    // exact replica of the reference's KD tree (built on first need)
+    KdReplica* kd = nullptr;
+    uint64_t bytes = 0;
+};
+
+int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream);
+size_t scan_temp_bytes(uint64_t items);
+
+struct QueryLaunch {
+    const Tile* tile;
+    int K;          // neighbours including the point itself
+    int rmax;
+    StageGroup grp;
+    ExceptionSink ex;
+    uint32_t* exact_rows;
+    uint32_t* counters;
+};
+int launch_query(Context* ctx, const QueryLaunch& q, cudaStream_t stream);
+
+// Exact path: nanoflann replica build (lazy) + DFS for the listed rows.
+int kd_ensure(Context* ctx, Tile* t, cudaStream_t stream);
+int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const ExceptionSink& ex,
+                const uint32_t* rows, uint32_t nrows, cudaStream_t stream);
+int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
+                     uint32_t* ids_out, cudaStream_t stream);
+void kd_free(Context* ctx, Tile* t);
+uint64_t kd_bytes(uint64_t n);
+int kd_export(Context* ctx, Tile* t, uint32_t* vind, uint32_t* nnodes, int32_t* c1, int32_t* c2,
+              int32_t* feat, double* dlo, double* dhi, uint32_t* nb, uint32_t* ne, uint32_t cap,
+              cudaStream_t st);
+
+// neighbour-set export of the grid path
+int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
+                         uint32_t* exact_rows, uint32_t* counters, cudaStream_t stream);
+
+}  // namespace nbg

@@ -1,0 +1,999 @@
+// nbg_kdtree.cu — exact replica of the reference's KD3 tree, and its search,
+// for the rows whose neighbour set depends on nanoflann's tie order.
+//
+// The reference keeps, among points at equal FP64 distance, the ones its
+// depth-first search meets first (vendor/nanoflann/nanoflann.hpp:178-205
+// shifts only on strict >, :1191-1197 admits only dist < worst).  That order
+// is a function of the tree, so rows whose k-th distance ties (and rows the
+// ring search could not finish) are answered by replaying the reference's
+// search over an identical tree built on the device.
+//
+// Tree build (nanoflann.hpp:640-690 divideTree, :779-828 middleSplit_,
+// :837-873 planeSplit), level-synchronous over all segments of a level:
+//   minmax    per-segment min/max of the raw coordinates (monotone in the
+//             double coordinate raw*scale+offset)
+//   split     cut feature among dims whose top-down span > (1-1e-5)*max span,
+//             largest actual spread first; cut value = top-down midpoint
+//             clamped to the segment's extent
+//   pass 1/2  the two Hoare passes.  Their effect is exactly: with L the
+//             count of elements satisfying the predicate, the t-th element
+//             from the left failing it inside [0, L) swaps with the t-th
+//             element from the right satisfying it inside [L, n).  Ranks
+//             come from per-tile counts and block scans.
+//   children  split index lim1 / lim2 / count/2 rule; segments of at most
+//             100 points become leaves
+// divlow/divhigh (child extents) are filled bottom-up afterwards.
+//
+// Search (nanoflann.hpp:875-893, 1059-1079, 1184-1250) is replayed per row
+// in FP64 with every operation rounded as the reference rounds it.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "nbg_common.cuh"
+#include "nbg_internal.h"
+
+namespace nbg {
+
+static constexpr int KD_LEAF = 100;
+static constexpr int KD_TILE = 256;
+static constexpr int KD_STACK = 96;
+static constexpr int KD_CAP = 66;
+
+struct KdSeg {
+    uint32_t begin, end;
+    int32_t node;
+    int32_t pad;
+    double lo[3], hi[3];
+};
+
+struct KdSplit {
+    int32_t f;
+    int32_t pad;
+    double cutval;
+    uint32_t L, m;    // pass 1: count below, misplaced pairs
+    uint32_t L2, m2;  // pass 2 on [L, n)
+    int32_t mn[3], mx[3];
+};
+
+struct KdDev {
+    const int32_t* rx;
+    const int32_t* ry;
+    const int32_t* rz;
+    const uint32_t* rid;
+    const int32_t* c1;
+    const int32_t* c2;
+    const int32_t* feat;
+    const uint32_t* nb;
+    const uint32_t* ne;
+    const double* dlo;
+    const double* dhi;
+    double root_lo[3], root_hi[3];
+};
+
+struct KdReplica {
+    uint64_t n = 0;
+    int32_t* rx = nullptr;
+    int32_t* ry = nullptr;
+    int32_t* rz = nullptr;
+    uint32_t* rid = nullptr;
+    uint32_t* mlpos = nullptr;
+    uint32_t* mrpos = nullptr;
+    // nodes
+    uint32_t node_cap = 0, node_count = 0;
+    int32_t* c1 = nullptr;
+    int32_t* c2 = nullptr;
+    int32_t* feat = nullptr;
+    uint32_t* nb = nullptr;
+    uint32_t* ne = nullptr;
+    double* dlo = nullptr;
+    double* dhi = nullptr;
+    int32_t* bmin = nullptr;  // 3 per node
+    int32_t* bmax = nullptr;
+    // segments of the current and next level, pass-2 views
+    KdSeg* seg[2] = {nullptr, nullptr};
+    KdSeg* seg2 = nullptr;
+    KdSplit* split = nullptr;
+    uint32_t seg_cap = 0;
+    // tiles
+    uint32_t* nt = nullptr;        // per segment tile count, then prefix (seg_cap+1)
+    uint32_t* tile_seg = nullptr;
+    uint32_t* tile_cnt = nullptr;  // per tile count, then prefix (tile_cap+1)
+    uint32_t tile_cap = 0;
+    void* scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+    uint32_t* counters = nullptr;  // [0] next segments, [1] nodes, [2] errors
+    std::vector<uint32_t> level_begin;  // node id range per level (host)
+    double root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
+    bool built = false;
+    uint64_t bytes = 0;
+};
+
+// ---------------------------------------------------------------------------
+// build kernels
+// ---------------------------------------------------------------------------
+__global__ void kd_init_kernel(const int32_t* x, const int32_t* y, const int32_t* z, uint64_t n,
+                               int32_t* rx, int32_t* ry, int32_t* rz, uint32_t* rid) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        rx[i] = x[i];
+        ry[i] = y[i];
+        rz[i] = z[i];
+        rid[i] = (uint32_t)i;
+    }
+}
+
+__global__ void kd_seg_tiles_kernel(const KdSeg* segs, uint32_t S, uint32_t* nt) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < S) nt[s] = (segs[s].end - segs[s].begin + KD_TILE - 1) / KD_TILE;
+    if (s == S) nt[s] = 0;
+}
+
+__global__ void kd_fill_tiles_kernel(const uint32_t* tile_first, uint32_t S, uint32_t ntiles,
+                                     uint32_t* tile_seg) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    // last segment whose first tile <= t
+    uint32_t lo = 0, hi = S;  // answer in [lo, hi)
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (tile_first[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    tile_seg[t] = lo;
+}
+
+__global__ void kd_minmax_init_kernel(KdSplit* sp, uint32_t S) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    for (int d = 0; d < 3; ++d) {
+        sp[s].mn[d] = INT32_MAX;
+        sp[s].mx[d] = INT32_MIN;
+    }
+}
+
+__global__ void __launch_bounds__(KD_TILE) kd_minmax_kernel(const KdSeg* segs, const uint32_t* tile_first,
+                                                            const uint32_t* tile_seg,
+                                                            const int32_t* rx, const int32_t* ry,
+                                                            const int32_t* rz, KdSplit* sp) {
+    const uint32_t t = blockIdx.x;
+    const uint32_t s = tile_seg[t];
+    const KdSeg sg = segs[s];
+    const uint32_t i = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
+    int32_t v[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, w[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    if (i < sg.end) {
+        v[0] = w[0] = rx[i];
+        v[1] = w[1] = ry[i];
+        v[2] = w[2] = rz[i];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        v[d] = __reduce_min_sync(0xffffffffu, v[d]);
+        w[d] = __reduce_max_sync(0xffffffffu, w[d]);
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            atomicMin(&sp[s].mn[d], v[d]);
+            atomicMax(&sp[s].mx[d], w[d]);
+        }
+    }
+}
+
+__global__ void kd_split_kernel(const KdSeg* segs, uint32_t S, KdSplit* sp, Transform tf) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const KdSeg sg = segs[s];
+    KdSplit p = sp[s];
+    const double EPS = 0.00001;
+    double max_span = __dsub_rn(sg.hi[0], sg.lo[0]);
+    for (int i = 1; i < 3; ++i) {
+        double span = __dsub_rn(sg.hi[i], sg.lo[i]);
+        if (span > max_span) max_span = span;
+    }
+    double max_spread = -1;
+    int cutfeat = 0;
+    for (int i = 0; i < 3; ++i) {
+        double span = __dsub_rn(sg.hi[i], sg.lo[i]);
+        if (span > __dmul_rn(__dsub_rn(1.0, EPS), max_span)) {
+            double mn = ref_coord(p.mn[i], tf.scale[i], tf.offset[i]);
+            double mx = ref_coord(p.mx[i], tf.scale[i], tf.offset[i]);
+            double spread = __dsub_rn(mx, mn);
+            if (spread > max_spread) {
+                cutfeat = i;
+                max_spread = spread;
+            }
+        }
+    }
+    double split_val = __ddiv_rn(__dadd_rn(sg.lo[cutfeat], sg.hi[cutfeat]), 2.0);
+    double mn = ref_coord(p.mn[cutfeat], tf.scale[cutfeat], tf.offset[cutfeat]);
+    double mx = ref_coord(p.mx[cutfeat], tf.scale[cutfeat], tf.offset[cutfeat]);
+    double cutval;
+    if (split_val < mn) cutval = mn;
+    else if (split_val > mx) cutval = mx;
+    else cutval = split_val;
+    sp[s].f = cutfeat;
+    sp[s].cutval = cutval;
+}
+
+__device__ __forceinline__ int32_t kd_coord(const int32_t* rx, const int32_t* ry,
+                                            const int32_t* rz, int f, uint32_t i) {
+    return f == 0 ? rx[i] : (f == 1 ? ry[i] : rz[i]);
+}
+
+// pass 1: x < cutval; pass 2: x <= cutval
+template <int PASS>
+__device__ __forceinline__ bool kd_pred(double v, double cut) {
+    return PASS == 1 ? (v < cut) : (v <= cut);
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(KD_TILE) kd_count_kernel(const KdSeg* segs, const uint32_t* tile_first,
+                                                           const uint32_t* tile_seg,
+                                                           const KdSplit* sp, const int32_t* rx,
+                                                           const int32_t* ry, const int32_t* rz,
+                                                           Transform tf, uint32_t* tile_cnt) {
+    const uint32_t t = blockIdx.x;
+    const uint32_t s = tile_seg[t];
+    const KdSeg sg = segs[s];
+    const int f = sp[s].f;
+    const double cut = sp[s].cutval;
+    const uint32_t i = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
+    bool p = false;
+    if (i < sg.end) p = kd_pred<PASS>(ref_coord(kd_coord(rx, ry, rz, f, i), tf.scale[f], tf.offset[f]), cut);
+    int c = __syncthreads_count(p);
+    if (threadIdx.x == 0) tile_cnt[t] = (uint32_t)c;
+}
+
+// L and the number of misplaced pairs m for each segment
+template <int PASS>
+__global__ void kd_seg_count_kernel(const KdSeg* segs, uint32_t S, const uint32_t* tile_first,
+                                    const uint32_t* tile_pref, KdSplit* sp, const int32_t* rx,
+                                    const int32_t* ry, const int32_t* rz, Transform tf) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const KdSeg sg = segs[s];
+    const uint32_t first = tile_first[s], nt = tile_first[s + 1] - first;
+    const uint32_t len = sg.end - sg.begin;
+    const int f = sp[s].f;
+    const double cut = sp[s].cutval;
+    uint32_t L = tile_pref[first + nt] - tile_pref[first];
+    uint32_t tl = L / KD_TILE;
+    uint32_t pleft = 0;
+    if (len) {
+        pleft = tile_pref[first + tl] - tile_pref[first];
+        for (uint32_t i = sg.begin + tl * KD_TILE; i < sg.begin + L; ++i)
+            pleft += kd_pred<PASS>(ref_coord(kd_coord(rx, ry, rz, f, i), tf.scale[f], tf.offset[f]), cut);
+    }
+    uint32_t m = L - pleft;
+    if (PASS == 1) {
+        sp[s].L = L;
+        sp[s].m = m;
+    } else {
+        sp[s].L2 = L;
+        sp[s].m2 = m;
+    }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(KD_TILE) kd_classify_kernel(const KdSeg* segs, const uint32_t* tile_first,
+                                                              const uint32_t* tile_seg,
+                                                              const uint32_t* tile_pref,
+                                                              const KdSplit* sp, const int32_t* rx,
+                                                              const int32_t* ry, const int32_t* rz,
+                                                              Transform tf, uint32_t* mlpos,
+                                                              uint32_t* mrpos) {
+    typedef cub::BlockScan<uint32_t, KD_TILE> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    const uint32_t t = blockIdx.x;
+    const uint32_t s = tile_seg[t];
+    const KdSeg sg = segs[s];
+    const int f = sp[s].f;
+    const double cut = sp[s].cutval;
+    const uint32_t L = PASS == 1 ? sp[s].L : sp[s].L2;
+    const uint32_t m = PASS == 1 ? sp[s].m : sp[s].m2;
+    const uint32_t i = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
+    uint32_t p = 0;
+    if (i < sg.end) p = kd_pred<PASS>(ref_coord(kd_coord(rx, ry, rz, f, i), tf.scale[f], tf.offset[f]), cut);
+    uint32_t rank;
+    Scan(tmp).ExclusiveSum(p, rank);
+    if (i >= sg.end) return;
+    const uint32_t prank = tile_pref[t] - tile_pref[tile_first[s]] + rank;  // P before i in segment
+    const uint32_t li = i - sg.begin;
+    if (li < L) {
+        if (!p) mlpos[sg.begin + (li - prank)] = i;
+    } else if (p) {
+        const uint32_t rml = prank - (L - m);
+        mrpos[sg.begin + (m - 1 - rml)] = i;
+    }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(KD_TILE) kd_swap_kernel(const KdSeg* segs, const uint32_t* tile_first,
+                                                          const uint32_t* tile_seg, const KdSplit* sp,
+                                                          const uint32_t* mlpos,
+                                                          const uint32_t* mrpos, int32_t* rx,
+                                                          int32_t* ry, int32_t* rz, uint32_t* rid) {
+    const uint32_t t = blockIdx.x;
+    const uint32_t s = tile_seg[t];
+    const KdSeg sg = segs[s];
+    const uint32_t m = PASS == 1 ? sp[s].m : sp[s].m2;
+    const uint32_t li = (t - tile_first[s]) * KD_TILE + threadIdx.x;
+    if (li >= m) return;
+    const uint32_t a = mlpos[sg.begin + li], b = mrpos[sg.begin + li];
+    int32_t tx = rx[a], ty = ry[a], tz = rz[a];
+    uint32_t ti = rid[a];
+    rx[a] = rx[b];
+    ry[a] = ry[b];
+    rz[a] = rz[b];
+    rid[a] = rid[b];
+    rx[b] = tx;
+    ry[b] = ty;
+    rz[b] = tz;
+    rid[b] = ti;
+}
+
+__global__ void kd_pass2_segs_kernel(const KdSeg* segs, uint32_t S, const KdSplit* sp, KdSeg* seg2) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    KdSeg g = segs[s];
+    g.begin = g.begin + sp[s].L;
+    seg2[s] = g;
+}
+
+__global__ void kd_children_kernel(const KdSeg* segs, uint32_t S, const KdSplit* sp, KdSeg* next,
+                                   uint32_t* counters, int32_t* c1, int32_t* c2, int32_t* feat,
+                                   uint32_t* nb, uint32_t* ne, uint32_t node_cap, uint32_t seg_cap) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const KdSeg sg = segs[s];
+    const KdSplit p = sp[s];
+    const uint32_t count = sg.end - sg.begin;
+    const uint32_t lim1 = p.L, lim2 = p.L + p.L2;
+    uint32_t index;
+    if (lim1 > count / 2) index = lim1;
+    else if (lim2 < count / 2) index = lim2;
+    else index = count / 2;
+    const uint32_t cid = atomicAdd(&counters[1], 2u);
+    if (cid + 2 > node_cap) {
+        atomicAdd(&counters[2], 1u);
+        return;
+    }
+    c1[sg.node] = (int32_t)cid;
+    c2[sg.node] = (int32_t)(cid + 1);
+    feat[sg.node] = p.f;
+    for (int side = 0; side < 2; ++side) {
+        const uint32_t node = cid + side;
+        KdSeg ch = sg;
+        if (side == 0) {
+            ch.end = sg.begin + index;
+            ch.hi[p.f] = p.cutval;
+        } else {
+            ch.begin = sg.begin + index;
+            ch.lo[p.f] = p.cutval;
+        }
+        ch.node = (int32_t)node;
+        nb[node] = ch.begin;
+        ne[node] = ch.end;
+        c1[node] = -1;
+        c2[node] = -1;
+        feat[node] = 0;
+        if (ch.end - ch.begin > (uint32_t)KD_LEAF) {
+            const uint32_t slot = atomicAdd(&counters[0], 1u);
+            if (slot < seg_cap) next[slot] = ch;
+            else atomicAdd(&counters[2], 1u);
+        }
+    }
+}
+
+__global__ void kd_node_bbox_kernel(uint32_t first, uint32_t last, const int32_t* c1,
+                                    const int32_t* c2, const uint32_t* nb, const uint32_t* ne,
+                                    const int32_t* rx, const int32_t* ry, const int32_t* rz,
+                                    int32_t* bmin, int32_t* bmax) {
+    uint32_t node = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= last) return;
+    int32_t lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    if (c1[node] < 0 && ne[node] <= nb[node]) {
+        // empty leaf: cannot arise from the split rule; keep the empty box
+    } else if (c1[node] < 0) {
+        lo[0] = hi[0] = rx[nb[node]];
+        lo[1] = hi[1] = ry[nb[node]];
+        lo[2] = hi[2] = rz[nb[node]];
+        for (uint32_t i = nb[node] + 1; i < ne[node]; ++i) {
+            lo[0] = min(lo[0], rx[i]);
+            hi[0] = max(hi[0], rx[i]);
+            lo[1] = min(lo[1], ry[i]);
+            hi[1] = max(hi[1], ry[i]);
+            lo[2] = min(lo[2], rz[i]);
+            hi[2] = max(hi[2], rz[i]);
+        }
+    } else {
+        const int a = c1[node], b = c2[node];
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = min(bmin[3 * a + d], bmin[3 * b + d]);
+            hi[d] = max(bmax[3 * a + d], bmax[3 * b + d]);
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+        bmin[3 * node + d] = lo[d];
+        bmax[3 * node + d] = hi[d];
+    }
+}
+
+__global__ void kd_div_kernel(uint32_t nodes, const int32_t* c1, const int32_t* c2,
+                              const int32_t* feat, const int32_t* bmin, const int32_t* bmax,
+                              Transform tf, double* dlo, double* dhi) {
+    uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= nodes || c1[node] < 0) return;
+    const int f = feat[node];
+    dlo[node] = ref_coord(bmax[3 * c1[node] + f], tf.scale[f], tf.offset[f]);
+    dhi[node] = ref_coord(bmin[3 * c2[node] + f], tf.scale[f], tf.offset[f]);
+}
+
+// ---------------------------------------------------------------------------
+// search replay
+// ---------------------------------------------------------------------------
+struct KdResult {
+    double dist[KD_CAP];
+    uint32_t idx[KD_CAP];
+    int count, cap;
+    __device__ __forceinline__ void init(int c) {
+        cap = c;
+        count = 0;
+        dist[cap - 1] = DBL_MAX;
+    }
+    __device__ __forceinline__ double worst() const { return dist[cap - 1]; }
+    __device__ __forceinline__ void add(double d, uint32_t id) {
+        int i;
+        for (i = count; i > 0; --i) {
+            if (dist[i - 1] > d) {
+                if (i < cap) {
+                    dist[i] = dist[i - 1];
+                    idx[i] = idx[i - 1];
+                }
+            } else break;
+        }
+        if (i < cap) {
+            dist[i] = d;
+            idx[i] = id;
+        }
+        if (count < cap) count++;
+    }
+};
+
+// One DFS frame: the node, the bound it was entered with and, once its
+// best child is done, the saved per-dimension distance.  The child order
+// and cut distance are recomputed from the node when needed.
+struct KdFrame {
+    double mind, dst;
+    int32_t node, phase;
+};
+
+__device__ __forceinline__ double kd_sq(double a, double b) {
+    double d = __dsub_rn(a, b);
+    return __dmul_rn(d, d);
+}
+
+// Returns false when the explicit stack overflowed (never for sane trees).
+__device__ bool kd_search(const KdDev& kd, const Transform& tf, const double q[3], KdResult& rs) {
+    double dists[3] = {0.0, 0.0, 0.0};
+    double distsq = 0.0;
+    for (int i = 0; i < 3; ++i) {
+        if (q[i] < kd.root_lo[i]) {
+            dists[i] = kd_sq(q[i], kd.root_lo[i]);
+            distsq = __dadd_rn(distsq, dists[i]);
+        }
+        if (q[i] > kd.root_hi[i]) {
+            dists[i] = kd_sq(q[i], kd.root_hi[i]);
+            distsq = __dadd_rn(distsq, dists[i]);
+        }
+    }
+    KdFrame st[KD_STACK];
+    int top = 0;
+    st[0].node = 0;
+    st[0].mind = distsq;
+    st[0].phase = 0;
+    while (top >= 0) {
+        const int node = st[top].node;
+        const int phase = st[top].phase;
+        if (phase == 0 && kd.c1[node] < 0) {
+            const double worst = rs.worst();
+            for (uint32_t i = kd.nb[node]; i < kd.ne[node]; ++i) {
+                const double p0 = ref_coord(kd.rx[i], tf.scale[0], tf.offset[0]);
+                const double p1 = ref_coord(kd.ry[i], tf.scale[1], tf.offset[1]);
+                const double p2 = ref_coord(kd.rz[i], tf.scale[2], tf.offset[2]);
+                const double d0 = __dsub_rn(q[0], p0);
+                const double d1 = __dsub_rn(q[1], p1);
+                const double d2 = __dsub_rn(q[2], p2);
+                const double dist = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
+                                              __dmul_rn(d2, d2));
+                if (dist < worst) rs.add(dist, kd.rid[i]);
+            }
+            --top;
+            continue;
+        }
+        const int idx = kd.feat[node];
+        const double val = q[idx];
+        const double diff1 = __dsub_rn(val, kd.dlo[node]);
+        const double diff2 = __dsub_rn(val, kd.dhi[node]);
+        const bool left_first = __dadd_rn(diff1, diff2) < 0;
+        if (phase == 0) {
+            st[top].phase = 1;
+            if (top + 1 >= KD_STACK) return false;
+            ++top;
+            st[top].node = left_first ? kd.c1[node] : kd.c2[node];
+            st[top].mind = st[top - 1].mind;
+            st[top].phase = 0;
+        } else if (phase == 1) {
+            const double cut = left_first ? kd_sq(val, kd.dhi[node]) : kd_sq(val, kd.dlo[node]);
+            const double dst = dists[idx];
+            const double mind2 = __dsub_rn(__dadd_rn(st[top].mind, cut), dst);
+            dists[idx] = cut;
+            st[top].dst = dst;
+            st[top].phase = 2;
+            if (mind2 <= rs.worst()) {
+                if (top + 1 >= KD_STACK) return false;
+                ++top;
+                st[top].node = left_first ? kd.c2[node] : kd.c1[node];
+                st[top].mind = mind2;
+                st[top].phase = 0;
+            }
+        } else {
+            dists[idx] = st[top].dst;
+            --top;
+        }
+    }
+    return true;
+}
+
+// Replays the reference's search for each listed row and writes its K
+// neighbour ids (the reference's order) to nbr[r*K ...].
+__global__ void kd_search_kernel(KdDev kd, Transform tf, const int32_t* __restrict__ x,
+                                 const int32_t* __restrict__ y, const int32_t* __restrict__ z,
+                                 const uint32_t* __restrict__ rows, uint32_t nrows, int K,
+                                 uint32_t* __restrict__ nbr, uint32_t* __restrict__ counts,
+                                 uint32_t* errors) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    const uint32_t id = rows[r];
+    const double q[3] = {ref_coord(x[id], tf.scale[0], tf.offset[0]),
+                         ref_coord(y[id], tf.scale[1], tf.offset[1]),
+                         ref_coord(z[id], tf.scale[2], tf.offset[2])};
+    KdResult rs;
+    rs.init(K);
+    const bool ok = kd_search(kd, tf, q, rs);
+    for (int s = 0; s < K; ++s) nbr[(uint64_t)r * K + s] = s < rs.count ? rs.idx[s] : 0u;
+    counts[r] = ok ? (uint32_t)rs.count : 0u;
+    if (!ok) atomicAdd(errors, 1u);
+}
+
+// Covariance of the replayed neighbour lists and the stage projections.
+__global__ void kd_finish_kernel(Transform tf, const int32_t* __restrict__ x,
+                                 const int32_t* __restrict__ y, const int32_t* __restrict__ z,
+                                 const uint32_t* __restrict__ rows, uint32_t nrows, int K,
+                                 const uint32_t* __restrict__ nbr,
+                                 const uint32_t* __restrict__ counts, StageGroup g,
+                                 ExceptionSink ex) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    const uint32_t id = rows[r];
+    const int32_t qraw[3] = {x[id], y[id], z[id]};
+    const int cnt = (int)counts[r];
+    long long s1[3] = {0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < cnt; ++s) {
+        const uint32_t j = nbr[(uint64_t)r * K + s];
+        const long long d0 = (long long)x[j] - qraw[0];
+        const long long d1 = (long long)y[j] - qraw[1];
+        const long long d2 = (long long)z[j] - qraw[2];
+        s1[0] += d0;
+        s1[1] += d1;
+        s1[2] += d2;
+        s2[0] += d0 * d0;
+        s2[1] += d1 * d0;
+        s2[2] += d1 * d1;
+        s2[3] += d2 * d0;
+        s2[4] += d2 * d1;
+        s2[5] += d2 * d2;
+    }
+    const long long n = cnt;
+    long long M[6];
+    M[0] = n * s2[0] - s1[0] * s1[0];
+    M[1] = n * s2[1] - s1[1] * s1[0];
+    M[2] = n * s2[2] - s1[1] * s1[1];
+    M[3] = n * s2[3] - s1[2] * s1[0];
+    M[4] = n * s2[4] - s1[2] * s1[1];
+    M[5] = n * s2[5] - s1[2] * s1[2];
+    nbg_finish_row(g, tf, ex, id, cnt, M, qraw);
+}
+
+// Neighbour-set export: ascending ids into ids_out[id*K ...].
+__global__ void kd_scatter_ids_kernel(const uint32_t* __restrict__ rows, uint32_t nrows, int K,
+                                      const uint32_t* __restrict__ nbr,
+                                      const uint32_t* __restrict__ counts, uint32_t* ids_out) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    uint32_t* row = ids_out + (uint64_t)rows[r] * K;
+    const int cnt = (int)counts[r];
+    for (int s = 0; s < cnt; ++s) {
+        const uint32_t v = nbr[(uint64_t)r * K + s];
+        int t = s - 1;
+        while (t >= 0 && row[t] > v) {
+            row[t + 1] = row[t];
+            --t;
+        }
+        row[t + 1] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static int kd_alloc(Context* ctx, void** p, size_t bytes, KdReplica* kd) {
+    if (bytes == 0) bytes = 16;
+    if (ctx->budget && ctx->used + bytes > ctx->budget) {
+        ctx->err = "HBM budget exceeded (KD replica)";
+        return NBG_ERR_BUDGET;
+    }
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->err = "cudaMalloc failed (KD replica)";
+        return NBG_ERR_OOM;
+    }
+    ctx->used += bytes;
+    kd->bytes += bytes;
+    return NBG_OK;
+}
+
+template <class T>
+static int kd_grow(Context* ctx, T** p, size_t old_n, size_t new_n, KdReplica* kd, cudaStream_t st) {
+    T* q = nullptr;
+    int rc = kd_alloc(ctx, (void**)&q, new_n * sizeof(T), kd);
+    if (rc) return rc;
+    if (*p) {
+        cudaMemcpyAsync(q, *p, old_n * sizeof(T), cudaMemcpyDeviceToDevice, st);
+        cudaStreamSynchronize(st);
+        cudaFree(*p);
+        ctx->used -= old_n * sizeof(T);
+        kd->bytes -= old_n * sizeof(T);
+    }
+    *p = q;
+    return NBG_OK;
+}
+
+uint64_t kd_bytes(uint64_t n) { return n * 24 + (n / 16 + 1024) * 64; }
+
+void kd_free(Context* ctx, Tile* t) {
+    KdReplica* kd = t->kd;
+    if (!kd) return;
+    ctx->used = ctx->used >= kd->bytes ? ctx->used - kd->bytes : 0;
+    void* ptrs[] = {kd->rx, kd->ry, kd->rz, kd->rid, kd->mlpos, kd->mrpos, kd->c1, kd->c2,
+                    kd->feat, kd->nb, kd->ne, kd->dlo, kd->dhi, kd->bmin, kd->bmax, kd->seg[0],
+                    kd->seg[1], kd->seg2, kd->split, kd->nt, kd->tile_seg, kd->tile_cnt,
+                    kd->scan_tmp, kd->counters};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete kd;
+    t->kd = nullptr;
+}
+
+// Builds the tile list of `S` segments; returns the number of tiles.
+static int kd_tiles(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, uint32_t* ntiles,
+                    cudaStream_t st) {
+    kd_seg_tiles_kernel<<<(S + 1 + 255) / 256, 256, 0, st>>>(segs, S, kd->nt);
+    size_t tb = kd->scan_bytes;
+    cub::DeviceScan::ExclusiveSum(kd->scan_tmp, tb, kd->nt, kd->nt, (int)(S + 1), st);
+    uint32_t total = 0;
+    cudaMemcpyAsync(&total, kd->nt + S, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        ctx->err = "KD tile scan failed";
+        return NBG_ERR_CUDA;
+    }
+    if (total + 1 > kd->tile_cap) {
+        uint32_t cap = std::max<uint32_t>(total + 1, kd->tile_cap * 2);
+        if (kd->tile_seg) cudaFree(kd->tile_seg);
+        if (kd->tile_cnt) cudaFree(kd->tile_cnt);
+        kd->tile_seg = kd->tile_cnt = nullptr;
+        int rc = kd_alloc(ctx, (void**)&kd->tile_seg, (size_t)cap * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->tile_cnt, (size_t)(cap + 1) * 4, kd);
+        if (rc) return rc;
+        kd->tile_cap = cap;
+    }
+    if (total) kd_fill_tiles_kernel<<<(total + 255) / 256, 256, 0, st>>>(kd->nt, S, total, kd->tile_seg);
+    *ntiles = total;
+    return NBG_OK;
+}
+
+template <int PASS>
+static int kd_pass(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, const Transform& tf,
+                   cudaStream_t st) {
+    uint32_t ntiles = 0;
+    int rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
+    if (rc) return rc;
+    if (ntiles) {
+        kd_count_kernel<PASS><<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->split,
+                                                          kd->rx, kd->ry, kd->rz, tf, kd->tile_cnt);
+    }
+    cudaMemsetAsync(kd->tile_cnt + ntiles, 0, 4, st);
+    size_t tb = kd->scan_bytes;
+    cub::DeviceScan::ExclusiveSum(kd->scan_tmp, tb, kd->tile_cnt, kd->tile_cnt, (int)(ntiles + 1), st);
+    kd_seg_count_kernel<PASS><<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->nt, kd->tile_cnt,
+                                                               kd->split, kd->rx, kd->ry, kd->rz, tf);
+    if (ntiles) {
+        kd_classify_kernel<PASS><<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg,
+                                                             kd->tile_cnt, kd->split, kd->rx,
+                                                             kd->ry, kd->rz, tf, kd->mlpos,
+                                                             kd->mrpos);
+        kd_swap_kernel<PASS><<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->split,
+                                                         kd->mlpos, kd->mrpos, kd->rx, kd->ry,
+                                                         kd->rz, kd->rid);
+    }
+    return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+}
+
+int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
+    if (t->kd && t->kd->built) return NBG_OK;
+    if (!t->kd) t->kd = new KdReplica();
+    KdReplica* kd = t->kd;
+    const uint64_t n = t->n;
+    kd->n = n;
+    int rc = NBG_OK;
+    if (!kd->rx) {
+        rc = kd_alloc(ctx, (void**)&kd->rx, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->ry, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->rz, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->rid, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->mlpos, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->mrpos, n * 4, kd);
+        kd->seg_cap = (uint32_t)(n / 50 + 64);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[0], kd->seg_cap * sizeof(KdSeg), kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[1], kd->seg_cap * sizeof(KdSeg), kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg2, kd->seg_cap * sizeof(KdSeg), kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->split, kd->seg_cap * sizeof(KdSplit), kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->nt, (kd->seg_cap + 1) * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->counters, 64, kd);
+        size_t b1 = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, b1, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                      (int)(n / KD_TILE + kd->seg_cap + 2));
+        kd->scan_bytes = b1;
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->scan_tmp, b1, kd);
+        kd->node_cap = 0;
+        if (rc) return rc;
+    }
+    // nodes: initial guess, grown per level as needed
+    const uint32_t want_nodes = (uint32_t)(n / 25 + 64);
+    if (kd->node_cap < want_nodes) {
+        const uint32_t old = kd->node_cap;
+        rc = kd_grow(ctx, &kd->c1, old, want_nodes, kd, st);
+        if (!rc) rc = kd_grow(ctx, &kd->c2, old, want_nodes, kd, st);
+        if (!rc) rc = kd_grow(ctx, &kd->feat, old, want_nodes, kd, st);
+        if (!rc) rc = kd_grow(ctx, &kd->nb, old, want_nodes, kd, st);
+        if (!rc) rc = kd_grow(ctx, &kd->ne, old, want_nodes, kd, st);
+        if (rc) return rc;
+        kd->node_cap = want_nodes;
+    }
+    kd_init_kernel<<<std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, ctx->sm_count * 8)), 256, 0,
+                     st>>>(t->x, t->y, t->z, n, kd->rx, kd->ry, kd->rz, kd->rid);
+    // root: actual bbox, as calculateBounds
+    const GridParams& g = t->host_gp;
+    const Transform& tf = t->tf;
+    KdSeg root;
+    root.begin = 0;
+    root.end = (uint32_t)n;
+    root.node = 0;
+    root.pad = 0;
+    int32_t mn[3] = {g.minx, g.miny, g.minz}, mx[3] = {g.maxx, g.maxy, g.maxz};
+    for (int d = 0; d < 3; ++d) {
+        root.lo[d] = (double)mn[d] * tf.scale[d] + tf.offset[d];
+        root.hi[d] = (double)mx[d] * tf.scale[d] + tf.offset[d];
+        kd->root_lo[d] = root.lo[d];
+        kd->root_hi[d] = root.hi[d];
+    }
+    int32_t neg = -1;
+    uint32_t zero = 0, rootend = (uint32_t)n;
+    cudaMemcpyAsync(kd->c1, &neg, 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->c2, &neg, 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->feat, &zero, 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->nb, &zero, 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->ne, &rootend, 4, cudaMemcpyHostToDevice, st);
+    kd->node_count = 1;
+    kd->level_begin.assign(1, 0);
+    uint32_t S = 0;
+    if (n > (uint64_t)KD_LEAF) {
+        cudaMemcpyAsync(kd->seg[0], &root, sizeof(KdSeg), cudaMemcpyHostToDevice, st);
+        S = 1;
+    }
+    int cur = 0;
+    while (S > 0) {
+        // room for this level's children
+        if (kd->node_count + 2 * S > kd->node_cap) {
+            const uint32_t old = kd->node_cap;
+            const uint32_t nc = std::max<uint32_t>(old * 2, kd->node_count + 2 * S + 64);
+            rc = kd_grow(ctx, &kd->c1, old, nc, kd, st);
+            if (!rc) rc = kd_grow(ctx, &kd->c2, old, nc, kd, st);
+            if (!rc) rc = kd_grow(ctx, &kd->feat, old, nc, kd, st);
+            if (!rc) rc = kd_grow(ctx, &kd->nb, old, nc, kd, st);
+            if (!rc) rc = kd_grow(ctx, &kd->ne, old, nc, kd, st);
+            if (rc) return rc;
+            kd->node_cap = nc;
+        }
+        const KdSeg* segs = kd->seg[cur];
+        uint32_t ntiles = 0;
+        kd_minmax_init_kernel<<<(S + 127) / 128, 128, 0, st>>>(kd->split, S);
+        rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
+        if (rc) return rc;
+        if (ntiles)
+            kd_minmax_kernel<<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->rx, kd->ry,
+                                                         kd->rz, kd->split);
+        kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, tf);
+        rc = kd_pass<1>(ctx, kd, segs, S, tf, st);
+        if (rc) return rc;
+        kd_pass2_segs_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg2);
+        rc = kd_pass<2>(ctx, kd, kd->seg2, S, tf, st);
+        if (rc) return rc;
+        uint32_t cnt[3] = {0, kd->node_count, 0};
+        cudaMemcpyAsync(kd->counters, cnt, 12, cudaMemcpyHostToDevice, st);
+        kd_children_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg[cur ^ 1],
+                                                            kd->counters, kd->c1, kd->c2, kd->feat,
+                                                            kd->nb, kd->ne, kd->node_cap,
+                                                            kd->seg_cap);
+        cudaMemcpyAsync(cnt, kd->counters, 12, cudaMemcpyDeviceToHost, st);
+        cudaError_t be = cudaGetLastError();
+        if (be == cudaSuccess) be = cudaStreamSynchronize(st);
+        if (be != cudaSuccess) {
+            ctx->err = std::string("KD replica build failed: ") + cudaGetErrorString(be);
+            return NBG_ERR_CUDA;
+        }
+        if (cnt[2]) {
+            ctx->err = "KD replica build ran out of node or segment capacity";
+            return NBG_ERR_UNSUPPORTED;
+        }
+        kd->level_begin.push_back(kd->node_count);
+        kd->node_count = cnt[1];
+        S = cnt[0];
+        cur ^= 1;
+    }
+    kd->level_begin.push_back(kd->node_count);
+    // extents bottom-up, then divlow / divhigh
+    const uint32_t nn = kd->node_count;
+    rc = kd_alloc(ctx, (void**)&kd->bmin, (size_t)nn * 12, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->bmax, (size_t)nn * 12, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->dlo, (size_t)nn * 8, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->dhi, (size_t)nn * 8, kd);
+    if (rc) return rc;
+    for (int lv = (int)kd->level_begin.size() - 2; lv >= 0; --lv) {
+        const uint32_t a = kd->level_begin[lv], b = kd->level_begin[lv + 1];
+        if (b > a)
+            kd_node_bbox_kernel<<<(b - a + 127) / 128, 128, 0, st>>>(a, b, kd->c1, kd->c2, kd->nb,
+                                                                   kd->ne, kd->rx, kd->ry, kd->rz,
+                                                                   kd->bmin, kd->bmax);
+    }
+    kd_div_kernel<<<(nn + 127) / 128, 128, 0, st>>>(nn, kd->c1, kd->c2, kd->feat, kd->bmin,
+                                                    kd->bmax, tf, kd->dlo, kd->dhi);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        ctx->err = "KD replica extents failed";
+        return NBG_ERR_CUDA;
+    }
+    kd->built = true;
+    return NBG_OK;
+}
+
+static KdDev kd_view(const KdReplica* kd) {
+    KdDev v;
+    v.rx = kd->rx;
+    v.ry = kd->ry;
+    v.rz = kd->rz;
+    v.rid = kd->rid;
+    v.c1 = kd->c1;
+    v.c2 = kd->c2;
+    v.feat = kd->feat;
+    v.nb = kd->nb;
+    v.ne = kd->ne;
+    v.dlo = kd->dlo;
+    v.dhi = kd->dhi;
+    for (int d = 0; d < 3; ++d) {
+        v.root_lo[d] = kd->root_lo[d];
+        v.root_hi[d] = kd->root_hi[d];
+    }
+    return v;
+}
+
+// Searches the listed rows into per-call scratch (nbr, counts).
+static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
+                          uint32_t** nbr, uint32_t** counts, cudaStream_t st) {
+    if (K > KD_CAP) return NBG_ERR_INVALID;
+    KdReplica* kd = t->kd;
+    *nbr = nullptr;
+    *counts = nullptr;
+    if (cudaMalloc((void**)nbr, (size_t)nrows * K * 4) != cudaSuccess ||
+        cudaMalloc((void**)counts, (size_t)nrows * 4) != cudaSuccess) {
+        cudaGetLastError();
+        if (*nbr) cudaFree(*nbr);
+        *nbr = nullptr;
+        ctx->err = "cudaMalloc failed (exact rows)";
+        return NBG_ERR_OOM;
+    }
+    cudaMemsetAsync(kd->counters + 2, 0, 4, st);
+    kd_search_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(kd_view(kd), t->tf, t->x, t->y, t->z,
+                                                          rows, nrows, K, *nbr, *counts,
+                                                          kd->counters + 2);
+    cudaError_t le = cudaGetLastError();
+    uint32_t err = 0;
+    if (le == cudaSuccess) le = cudaMemcpyAsync(&err, kd->counters + 2, 4, cudaMemcpyDeviceToHost, st);
+    if (le == cudaSuccess) le = cudaStreamSynchronize(st);
+    if (le != cudaSuccess) {
+        ctx->err = std::string("exact KD rows: ") + cudaGetErrorString(le);
+        return NBG_ERR_CUDA;
+    }
+    if (err) {
+        ctx->err = "KD search stack overflow";
+        return NBG_ERR_UNSUPPORTED;
+    }
+    return NBG_OK;
+}
+
+int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const ExceptionSink& ex,
+                const uint32_t* rows, uint32_t nrows, cudaStream_t st) {
+    if (!nrows) return NBG_OK;
+    uint32_t *nbr = nullptr, *counts = nullptr;
+    int rc = kd_search_rows(ctx, t, K, rows, nrows, &nbr, &counts, st);
+    if (!rc) {
+        kd_finish_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(t->tf, t->x, t->y, t->z, rows, nrows,
+                                                              K, nbr, counts, grp, ex);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            ctx->err = std::string("exact KD finish: ") + cudaGetErrorString(e);
+            rc = NBG_ERR_CUDA;
+        }
+    }
+    if (nbr) cudaFree(nbr);
+    if (counts) cudaFree(counts);
+    return rc;
+}
+
+int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
+                     uint32_t* ids_out, cudaStream_t st) {
+    if (!nrows) return NBG_OK;
+    uint32_t *nbr = nullptr, *counts = nullptr;
+    int rc = kd_search_rows(ctx, t, K, rows, nrows, &nbr, &counts, st);
+    if (!rc) {
+        kd_scatter_ids_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(rows, nrows, K, nbr, counts,
+                                                                   ids_out);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            ctx->err = std::string("exact KD ids: ") + cudaGetErrorString(e);
+            rc = NBG_ERR_CUDA;
+        }
+    }
+    if (nbr) cudaFree(nbr);
+    if (counts) cudaFree(counts);
+    return rc;
+}
+
+// Test hook: copies the replica's point order (ids) and node arrays out.
+int kd_export(Context* ctx, Tile* t, uint32_t* vind, uint32_t* nnodes, int32_t* c1, int32_t* c2,
+              int32_t* feat, double* dlo, double* dhi, uint32_t* nb, uint32_t* ne, uint32_t cap,
+              cudaStream_t st) {
+    int rc = kd_ensure(ctx, t, st);
+    if (rc) return rc;
+    KdReplica* kd = t->kd;
+    *nnodes = kd->node_count;
+    cudaMemcpyAsync(vind, kd->rid, t->n * 4, cudaMemcpyDeviceToHost, st);
+    const uint32_t m = std::min(cap, kd->node_count);
+    if (m) {
+        cudaMemcpyAsync(c1, kd->c1, m * 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(c2, kd->c2, m * 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(feat, kd->feat, m * 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(dlo, kd->dlo, m * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(dhi, kd->dhi, m * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(nb, kd->nb, m * 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(ne, kd->ne, m * 4, cudaMemcpyDeviceToHost, st);
+    }
+    return cudaStreamSynchronize(st) == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+}
+
+}  // namespace nbg
+

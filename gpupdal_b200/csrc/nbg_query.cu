@@ -1,0 +1,390 @@
+// nbg_query.cu — fused kNN + covariance + eigensolve + stage projection.
+//
+// Replaces the reference's per-point loop (KD3Index::neighbors ->
+// computeCovariance -> SelfAdjointEigenSolver -> projection:
+// filters/NormalFilter.cpp:140-182, filters/EigenvaluesFilter.cpp:115-172,
+// filters/CovarianceFeaturesFilter.cpp:204-367) and the fork's
+// knnGatherKernel + eigenSystemsKernel + projection kernels
+// (src/index/SpatialIndexKernels.cu:716-1086,1716-1769,
+// src/stages/NeighborhoodKernels.cu:67-119,421-498).
+//
+// One thread per query, queries in cell order (neighbouring lanes share
+// cells, so candidate loads hit L1).  The neighbour list never reaches HBM:
+//   pass 1  ring expansion over cells; register top-(K+1) of exact integer
+//           squared distances (FP32 FMA with a 2^23 bias yields the integer
+//           in the mantissa: exact below 2^23 raw units^2)
+//   check   complete iff the K-th distance is below the squared gap to the
+//           unscanned cells; a row whose K-th and (K+1)-th distances are equal
+//           (or whose search is incomplete within rmax rings) goes to the
+//           exact KD path, which reproduces nanoflann's tie order
+//   pass 2  exact int32 sums of the neighbours' offsets and outer products
+//   finish  cov = (n*S2 - S1*S1^T) s^2/(n(n-1)), eigensolve, projections
+// Distinct integer distances order points exactly as the reference's FP64
+// distances do (the FP64 rounding error is far below one raw unit^2), so a
+// row with no boundary tie has exactly the reference's neighbour set.
+#include "nbg_common.cuh"
+#include "nbg_internal.h"
+
+namespace nbg {
+
+static constexpr uint32_t KEY_BASE = 0x4B000000u;    // bits of 2^23f
+static constexpr uint32_t KEY_EXACT_END = 0x4B800000u;  // bits of 2^24f
+
+__device__ __forceinline__ uint32_t dist_key(float dx, float dy, float dz) {
+    return __float_as_uint(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 8388608.0f))));
+}
+
+// integer value of an exact small float (|v| < 2^22)
+__device__ __forceinline__ int small_int(float v) {
+    return __float_as_int(v + 12582912.0f) - 0x4B400000;
+}
+
+struct QueryCell {
+    int qx, qy, qz;     // raw, relative to tile min
+    int cx, cy, cz;     // cell coords
+};
+
+// Calls f(float4) for every point of the cells at Chebyshev distance R.
+template <class F>
+__device__ __forceinline__ void scan_shell(const float4* __restrict__ sorted,
+                                           const uint32_t* __restrict__ cs, const GridParams& g,
+                                           const QueryCell& qc, int R, F& f) {
+    for (int dz = -R; dz <= R; ++dz) {
+        const int z = qc.cz + dz;
+        if (z < 0 || z >= g.gz) continue;
+        const int adz = dz < 0 ? -dz : dz;
+        for (int dy = -R; dy <= R; ++dy) {
+            const int y = qc.cy + dy;
+            if (y < 0 || y >= g.gy) continue;
+            const int ady = dy < 0 ? -dy : dy;
+            const uint32_t rowbase = ((uint32_t)z * (uint32_t)g.gy + (uint32_t)y) * (uint32_t)g.gx;
+            if (max(adz, ady) == R) {
+                const int x0 = max(qc.cx - R, 0), x1 = min(qc.cx + R, g.gx - 1);
+                const uint32_t b = __ldg(&cs[rowbase + x0]), e = __ldg(&cs[rowbase + x1 + 1]);
+                for (uint32_t j = b; j < e; ++j) f(__ldg(&sorted[j]));
+            } else {
+                if (qc.cx - R >= 0) {
+                    const uint32_t b = __ldg(&cs[rowbase + qc.cx - R]),
+                                   e = __ldg(&cs[rowbase + qc.cx - R + 1]);
+                    for (uint32_t j = b; j < e; ++j) f(__ldg(&sorted[j]));
+                }
+                if (qc.cx + R < g.gx) {
+                    const uint32_t b = __ldg(&cs[rowbase + qc.cx + R]),
+                                   e = __ldg(&cs[rowbase + qc.cx + R + 1]);
+                    for (uint32_t j = b; j < e; ++j) f(__ldg(&sorted[j]));
+                }
+            }
+        }
+    }
+}
+
+// Squared raw gap from the query to any point outside the scanned cube of
+// radius R; UINT64_MAX when the cube covers the whole grid.
+__device__ __forceinline__ unsigned long long outside_gap2(const GridParams& g,
+                                                           const QueryCell& qc, int R) {
+    long long gap = LLONG_MAX;
+    const int c = g.cell;
+    if (qc.cx - R > 0) gap = min(gap, (long long)qc.qx - (long long)(qc.cx - R) * c + 1);
+    if (qc.cx + R < g.gx - 1) gap = min(gap, (long long)(qc.cx + R + 1) * c - qc.qx);
+    if (qc.cy - R > 0) gap = min(gap, (long long)qc.qy - (long long)(qc.cy - R) * c + 1);
+    if (qc.cy + R < g.gy - 1) gap = min(gap, (long long)(qc.cy + R + 1) * c - qc.qy);
+    if (qc.cz - R > 0) gap = min(gap, (long long)qc.qz - (long long)(qc.cz - R) * c + 1);
+    if (qc.cz + R < g.gz - 1) gap = min(gap, (long long)(qc.cz + R + 1) * c - qc.qz);
+    if (gap == LLONG_MAX) return ~0ull;
+    return (unsigned long long)gap * (unsigned long long)gap;
+}
+
+template <int KS>
+struct TopK {
+    uint32_t k[KS];
+    __device__ __forceinline__ void init(int off) {
+#pragma unroll
+        for (int s = 0; s < KS; ++s) k[s] = s < off ? 0u : 0xFFFFFFFFu;
+    }
+    __device__ __forceinline__ void insert(uint32_t key) {
+#pragma unroll
+        for (int s = 0; s < KS; ++s) {
+            const uint32_t lo = min(k[s], key);
+            key = max(k[s], key);
+            k[s] = lo;
+        }
+    }
+    __device__ __forceinline__ uint32_t at(int i) const {
+        uint32_t v = 0xFFFFFFFFu;
+#pragma unroll
+        for (int s = 0; s < KS; ++s)
+            if (s == i) v = k[s];
+        return v;
+    }
+};
+
+struct Pass1 {
+    float qx, qy, qz;
+};
+
+template <int KS>
+struct Pass1Fn {
+    float qx, qy, qz;
+    TopK<KS>* top;
+    __device__ __forceinline__ void operator()(const float4 p) {
+        const uint32_t key = dist_key(p.x - qx, p.y - qy, p.z - qz);
+        if (key < top->k[KS - 1]) top->insert(key);
+    }
+};
+
+struct Pass2Fn {
+    float qx, qy, qz;
+    uint32_t kk;
+    int s1x, s1y, s1z, sxx, syx, syy, szx, szy, szz, cnt;
+    __device__ __forceinline__ void operator()(const float4 p) {
+        const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+        const uint32_t key = dist_key(dx, dy, dz);
+        if (key <= kk) {
+            const int ix = small_int(dx), iy = small_int(dy), iz = small_int(dz);
+            s1x += ix;
+            s1y += iy;
+            s1z += iz;
+            sxx += ix * ix;
+            syx += iy * ix;
+            syy += iy * iy;
+            szx += iz * ix;
+            szy += iz * iy;
+            szz += iz * iz;
+            ++cnt;
+        }
+    }
+};
+
+struct CollectFn {
+    float qx, qy, qz;
+    uint32_t kk;
+    uint32_t* row;
+    int cnt, cap;
+    __device__ __forceinline__ void operator()(const float4 p) {
+        const uint32_t key = dist_key(p.x - qx, p.y - qy, p.z - qz);
+        if (key <= kk) {
+            if (cnt < cap) row[cnt] = __float_as_uint(p.w);
+            ++cnt;
+        }
+    }
+};
+
+struct QueryArgs {
+    const float4* sorted;
+    const uint32_t* cs;
+    const GridParams* gp;
+    uint64_t n;
+    int K;
+    int rmax;
+    StageGroup grp;
+    Transform tf;
+    ExceptionSink ex;
+    uint32_t* exact_rows;
+    uint32_t* counters;  // [0] exact rows, [1] tie rows, [2] incomplete rows
+    uint32_t* ids_out;   // neighbour-set export (null in the fused path)
+};
+
+// Pass 1 + completeness/tie decision.  Returns true when the row is exact on
+// the grid path; `R` is the final ring and `kk` the K-th key.
+template <int KS>
+__device__ __forceinline__ bool select_kth(const QueryArgs& a, const GridParams& g,
+                                           const QueryCell& qc, const float4 q, int& R,
+                                           uint32_t& kk) {
+    const int K = a.K;
+    const int off = KS - (K + 1);
+    TopK<KS> top;
+    top.init(off);
+    Pass1Fn<KS> f1{q.x, q.y, q.z, &top};
+    bool complete = false;
+    for (R = 0; R <= a.rmax; ++R) {
+        scan_shell(a.sorted, a.cs, g, qc, R, f1);
+        const uint32_t kth = top.at(off + K - 1);
+        const unsigned long long gap2 = outside_gap2(g, qc, R);
+        if (gap2 == ~0ull) {
+            complete = kth != 0xFFFFFFFFu;
+            break;
+        }
+        if (kth < KEY_EXACT_END && (unsigned long long)(kth - KEY_BASE) < gap2) {
+            complete = true;
+            break;
+        }
+    }
+    if (R > a.rmax) R = a.rmax;
+    kk = top.at(off + K - 1);
+    const uint32_t kk1 = top.at(off + K);
+    if (!complete || kk >= KEY_EXACT_END) {
+        atomicAdd(&a.counters[2], 1u);
+        return false;
+    }
+    if (kk1 == kk) {
+        atomicAdd(&a.counters[1], 1u);
+        return false;
+    }
+    return true;
+}
+
+template <int KS>
+__global__ void __launch_bounds__(128) knn_fused_kernel(const QueryArgs a) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const GridParams g = *a.gp;
+    const float4 q = __ldg(&a.sorted[i]);
+    const uint32_t id = __float_as_uint(q.w);
+    QueryCell qc;
+    qc.qx = __float2int_rz(q.x);
+    qc.qy = __float2int_rz(q.y);
+    qc.qz = __float2int_rz(q.z);
+    qc.cx = qc.qx / g.cell;
+    qc.cy = qc.qy / g.cell;
+    qc.cz = qc.qz / g.cell;
+    int R;
+    uint32_t kk;
+    if (!select_kth<KS>(a, g, qc, q, R, kk)) {
+        const uint32_t slot = atomicAdd(&a.counters[0], 1u);
+        a.exact_rows[slot] = id;
+        return;
+    }
+    Pass2Fn f2{q.x, q.y, q.z, kk, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int r = 0; r <= R; ++r) scan_shell(a.sorted, a.cs, g, qc, r, f2);
+    if (f2.cnt != a.K) {  // cannot happen for a complete, tie-free row; stay exact
+        const uint32_t slot = atomicAdd(&a.counters[0], 1u);
+        a.exact_rows[slot] = id;
+        return;
+    }
+    const long long n = f2.cnt;
+    long long M[6];
+    M[0] = n * f2.sxx - (long long)f2.s1x * f2.s1x;
+    M[1] = n * f2.syx - (long long)f2.s1y * f2.s1x;
+    M[2] = n * f2.syy - (long long)f2.s1y * f2.s1y;
+    M[3] = n * f2.szx - (long long)f2.s1z * f2.s1x;
+    M[4] = n * f2.szy - (long long)f2.s1z * f2.s1y;
+    M[5] = n * f2.szz - (long long)f2.s1z * f2.s1z;
+    const int32_t qraw[3] = {qc.qx + g.minx, qc.qy + g.miny, qc.qz + g.minz};
+    nbg_finish_row(a.grp, a.tf, a.ex, id, (int)n, M, qraw);
+}
+
+template <int KS>
+__global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const GridParams g = *a.gp;
+    const float4 q = __ldg(&a.sorted[i]);
+    const uint32_t id = __float_as_uint(q.w);
+    QueryCell qc;
+    qc.qx = __float2int_rz(q.x);
+    qc.qy = __float2int_rz(q.y);
+    qc.qz = __float2int_rz(q.z);
+    qc.cx = qc.qx / g.cell;
+    qc.cy = qc.qy / g.cell;
+    qc.cz = qc.qz / g.cell;
+    int R;
+    uint32_t kk;
+    if (!select_kth<KS>(a, g, qc, q, R, kk)) {
+        const uint32_t slot = atomicAdd(&a.counters[0], 1u);
+        a.exact_rows[slot] = id;
+        return;
+    }
+    uint32_t* row = a.ids_out + (uint64_t)id * a.K;
+    CollectFn f{q.x, q.y, q.z, kk, row, 0, a.K};
+    for (int r = 0; r <= R; ++r) scan_shell(a.sorted, a.cs, g, qc, r, f);
+    // ascending ids (insertion sort of at most 66 entries)
+    for (int s = 1; s < a.K; ++s) {
+        uint32_t v = row[s];
+        int t = s - 1;
+        while (t >= 0 && row[t] > v) {
+            row[t + 1] = row[t];
+            --t;
+        }
+        row[t + 1] = v;
+    }
+}
+
+static int slots_for(int K) {
+    const int need = K + 1;
+    if (need <= 10) return 10;
+    if (need <= 12) return 12;
+    if (need <= 14) return 14;
+    if (need <= 18) return 18;
+    if (need <= 26) return 26;
+    if (need <= 34) return 34;
+    if (need <= 50) return 50;
+    if (need <= 66) return 66;
+    return -1;
+}
+
+template <template <int> class Launcher>
+static int dispatch_slots(int K, typename Launcher<10>::Args args) {
+    switch (slots_for(K)) {
+        case 10: return Launcher<10>::run(args);
+        case 12: return Launcher<12>::run(args);
+        case 14: return Launcher<14>::run(args);
+        case 18: return Launcher<18>::run(args);
+        case 26: return Launcher<26>::run(args);
+        case 34: return Launcher<34>::run(args);
+        case 50: return Launcher<50>::run(args);
+        case 66: return Launcher<66>::run(args);
+    }
+    return NBG_ERR_INVALID;
+}
+
+struct LaunchArgs {
+    QueryArgs q;
+    cudaStream_t stream;
+    bool ids;
+};
+
+template <int KS>
+struct KnnLauncher {
+    using Args = LaunchArgs;
+    static int run(const LaunchArgs& la) {
+        const int threads = 128;
+        const uint64_t blocks = (la.q.n + threads - 1) / threads;
+        if (blocks == 0) return NBG_OK;
+        if (la.ids)
+            knn_ids_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
+        else
+            knn_fused_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
+        return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+    }
+};
+
+int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
+    (void)ctx;
+    LaunchArgs la;
+    la.q.sorted = ql.tile->sorted;
+    la.q.cs = ql.tile->cell_start;
+    la.q.gp = ql.tile->gp;
+    la.q.n = ql.tile->n;
+    la.q.K = ql.K;
+    la.q.rmax = ql.rmax;
+    la.q.grp = ql.grp;
+    la.q.tf = ql.tile->tf;
+    la.q.ex = ql.ex;
+    la.q.exact_rows = ql.exact_rows;
+    la.q.counters = ql.counters;
+    la.q.ids_out = nullptr;
+    la.stream = stream;
+    la.ids = false;
+    return dispatch_slots<KnnLauncher>(ql.K, la);
+}
+
+int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
+                         uint32_t* exact_rows, uint32_t* counters, cudaStream_t stream) {
+    (void)ctx;
+    LaunchArgs la{};
+    la.q.sorted = t->sorted;
+    la.q.cs = t->cell_start;
+    la.q.gp = t->gp;
+    la.q.n = t->n;
+    la.q.K = K;
+    la.q.rmax = rmax;
+    la.q.tf = t->tf;
+    la.q.exact_rows = exact_rows;
+    la.q.counters = counters;
+    la.q.ids_out = ids_out;
+    la.stream = stream;
+    la.ids = true;
+    return dispatch_slots<KnnLauncher>(K, la);
+}
+
+}  // namespace nbg

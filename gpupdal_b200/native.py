@@ -1,0 +1,163 @@
+"""Python handle on the native library (C ABI in include/nbg_b200.h).
+
+Host buffers are numpy arrays; device buffers are torch CUDA tensors (torch is
+used only for device memory and streams).  Every call goes to the sm_100a
+library; a missing library raises instead of falling back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import abi
+
+
+class NbgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"nbg error {code}: {msg}")
+        self.code = code
+
+
+def _dptr(a):
+    return ctypes.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+
+
+class Context:
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self.lib = abi.load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.nbg_create(ctypes.byref(h), int(device), int(hbm_budget))
+        if rc != abi.NBG_OK:
+            raise NbgError(rc, "nbg_create failed (no sm_100 device?)")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nbg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != abi.NBG_OK:
+            raise NbgError(rc, self.lib.nbg_last_error(self.h).decode())
+
+    def tile(self, x, y, z, scale=(0.01, 0.01, 0.01), offset=(0.0, 0.0, 0.0), stream=None):
+        return Tile(self, x, y, z, scale, offset, stream)
+
+    # -- stages -----------------------------------------------------------
+    def run(self, tile, stages, optimal_knn=None, optimal_radius=None, device_out=False,
+            fresh=True, exception_capacity=None, stream=None, out=None):
+        """Runs `stages` (list of abi.StageOpts) over `tile`.
+
+        Returns (outputs, exceptions, stats): outputs[i] is a (ndims, n)
+        array (numpy, or a torch tensor when device_out) for stage i;
+        exceptions is a structured numpy array (point_id, stage, code)."""
+        n = tile.n
+        ns = len(stages)
+        opts = (abi.StageOpts * max(ns, 1))(*stages)
+        cols = (abi.Columns * max(ns, 1))()
+        outs = []
+        for i, st in enumerate(stages):
+            nd = len(abi.stage_dims(st))
+            if out is not None:
+                buf = out[i]
+            elif device_out:
+                import torch
+                buf = torch.zeros((max(nd, 1), n), dtype=torch.float64, device=f"cuda:{self.device}")
+            else:
+                buf = np.zeros((max(nd, 1), n), dtype=np.float64)
+            outs.append(buf)
+            c = cols[i]
+            c.base = _dptr(buf).value
+            c.point_stride = 8
+            c.ndims = nd
+            c.on_device = 1 if device_out else (2 if fresh else 0)
+            for d in range(nd):
+                c.offset[d] = d * n * 8
+        cap = exception_capacity if exception_capacity is not None else max(1024, n)
+        exc = (abi.RowException * cap)()
+        nexc = ctypes.c_uint32(0)
+        stats = abi.RunStats()
+        kp = rp = None
+        aux_dev = 0
+        if optimal_knn is not None:
+            if isinstance(optimal_knn, np.ndarray):
+                optimal_knn = np.ascontiguousarray(optimal_knn, dtype=np.float64)
+                optimal_radius = np.ascontiguousarray(optimal_radius, dtype=np.float64)
+            else:
+                aux_dev = 1
+            kp, rp = _dptr(optimal_knn), _dptr(optimal_radius)
+        rc = self.lib.nbg_run(self.h, tile.h, opts, ns, cols, kp, rp, aux_dev, exc, cap,
+                              ctypes.byref(nexc), ctypes.byref(stats),
+                              ctypes.c_void_p(stream) if stream else None)
+        self._check(rc)
+        m = min(nexc.value, cap)
+        ex = np.zeros(m, dtype=[("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8)])
+        for j in range(m):
+            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code)
+        return [o[: len(abi.stage_dims(s))] for o, s in zip(outs, stages)], ex, stats
+
+    def kd_export(self, tile):
+        """The device KD replica: (vind, nodes dict) for parity tests."""
+        n = tile.n
+        cap = max(16, n // 10 + 64)
+        vind = np.zeros(n, np.uint32)
+        nn = ctypes.c_uint32(0)
+        arr = dict(child1=np.zeros(cap, np.int32), child2=np.zeros(cap, np.int32),
+                   divfeat=np.zeros(cap, np.int32), divlow=np.zeros(cap), divhigh=np.zeros(cap),
+                   begin=np.zeros(cap, np.uint32), end=np.zeros(cap, np.uint32))
+        rc = self.lib.nbg_debug_kd_export(
+            self.h, tile.h, _dptr(vind), ctypes.byref(nn), *[_dptr(arr[k]) for k in
+                                                            ("child1", "child2", "divfeat",
+                                                             "divlow", "divhigh", "begin", "end")],
+            cap)
+        self._check(rc)
+        m = min(nn.value, cap)
+        return vind, {k: v[:m] for k, v in arr.items()}
+
+    def neighbor_sets(self, tile, knn):
+        k1 = min(tile.n, knn + 1)
+        ids = np.zeros((tile.n, k1), dtype=np.uint32)
+        stats = abi.RunStats()
+        rc = self.lib.nbg_neighbor_sets(self.h, tile.h, int(knn), _dptr(ids), 0,
+                                        ctypes.byref(stats), None)
+        self._check(rc)
+        return ids, stats
+
+
+class Tile:
+    def __init__(self, ctx: Context, x, y, z, scale, offset, stream=None):
+        self.ctx = ctx
+        on_device = not isinstance(x, np.ndarray)
+        if not on_device:
+            x = np.ascontiguousarray(x, dtype=np.int32)
+            y = np.ascontiguousarray(y, dtype=np.int32)
+            z = np.ascontiguousarray(z, dtype=np.int32)
+        self._keep = (x, y, z)
+        self.n = int(len(x))
+        sc = (ctypes.c_double * 3)(*scale)
+        of = (ctypes.c_double * 3)(*offset)
+        h = ctypes.c_void_p()
+        rc = ctx.lib.nbg_tile_upload(ctx.h, _dptr(x), _dptr(y), _dptr(z), self.n, sc, of,
+                                     int(on_device), ctypes.c_void_p(stream) if stream else None,
+                                     ctypes.byref(h))
+        ctx._check(rc)
+        self.h = h
+
+    def free(self):
+        if getattr(self, "h", None) and self.ctx.h:
+            self.ctx.lib.nbg_tile_free(self.ctx.h, self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -110,7 +110,9 @@ typedef struct nbg_columns {
     void* base;
     int64_t point_stride;
     int32_t ndims;
-    int32_t on_device;     /* 1: base is device memory; 0: host memory      */
+    int32_t on_device;     /* 1: base is device memory; 0: host memory whose
+                              skipped rows keep their values; 2: host memory of
+                              freshly added dimensions (skipped rows read 0) */
     int64_t offset[NBG_MAX_DIMS];
 } nbg_columns;
 
@@ -178,6 +180,16 @@ int nbg_run(nbg_context* ctx, nbg_tile* tile, const nbg_stage_opts* stages,
 int nbg_neighbor_sets(nbg_context* ctx, nbg_tile* tile, int32_t knn,
                       uint32_t* ids_out, int32_t ids_on_device,
                       nbg_run_stats* stats, void* stream);
+
+/* Diagnostic: the device replica of the reference's KD tree for a tile
+ * (built on demand): point order `vind` (n ids) and up to `node_capacity`
+ * nodes (child ids or -1, cut dim, divlow, divhigh, vind range).  Mirrors
+ * nanoflann's tree (vendor/nanoflann/nanoflann.hpp:640-873) for parity
+ * tests; not needed for normal use. */
+int nbg_debug_kd_export(nbg_context* ctx, nbg_tile* tile, uint32_t* vind, uint32_t* n_nodes,
+                        int32_t* child1, int32_t* child2, int32_t* divfeat, double* divlow,
+                        double* divhigh, uint32_t* begin, uint32_t* end,
+                        uint32_t node_capacity);
 
 #ifdef __cplusplus
 }
