@@ -1,0 +1,311 @@
+#!/usr/bin/env python
+"""Benchmark of the neighbourhood-geometry path on B200.
+
+Workload (one "step"): filters.eigenvalues knn=16 followed by filters.normal
+knn=16 on one 32,000,000-point tile of the stress mixture (terrain, building
+faces, vegetation, 2 % exact duplicates, 3 % collinear wire points; seeded
+synthetic, int32 at 0.01 m) — index build, kNN, covariance, eigensolve and
+all seven output dimensions, the tie rows answered by the exact KD replica.
+
+  value  Mpts/s with the tile's coordinates resident in HBM when the timed
+         region starts (device-to-device tile upload + nbg_run, device outputs)
+  e2e    the same through the C ABI with pinned host buffers: H2D of the
+         coordinates, nbg_run, D2H of the outputs inside the timed region
+
+Multi-GPU (torchrun): one replica tile per rank (different seeds), no
+collective on the data path; value = all ranks' points / max-over-ranks time.
+
+--impl reference times the reference's CPU implementation (oracle/_ref:
+nanoflann 1.3.1 + Eigen 3.4 built from the reference's sources; the oracle
+port when that library is absent) on the host cores, on a bounded window of
+the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpts/s k=16 normals+eigen, served vs plain @<=1e-5 rel err; p50/p99 latency"
+BYTES_PER_POINT = 20 + 8 * 7 + 1  # sorted xyz+id, id permutation, 7 f64 outputs, status
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--points", type=int, default=32_000_000)
+    ap.add_argument("--knn", type=int, default=16)
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (read-only queries)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(points, seed):
+    from gpupdal_b200 import synthetic as syn
+    return syn.stress(points, seed)
+
+
+def stages(knn):
+    from gpupdal_b200 import abi
+    return [abi.make_opts(abi.STAGE_EIGENVALUES, knn=knn),
+            abi.make_opts(abi.STAGE_NORMAL, knn=knn, always_up=True)]
+
+
+def cpu_reference(x, y, z, knn, sample, kind=None):
+    """Times the reference's CPU path (KD build + eigenvalues + normal) on a
+    spatially contiguous window of `sample` points; all host threads."""
+    from gpupdal_b200 import synthetic as syn
+    from oracle import oracle as orc
+    if kind is None:
+        kind = "reference" if orc.available("reference") else "port"
+    if not orc.available(kind):
+        orc.build()
+    o = orc.Oracle(kind)
+    # square window from the tile's corner holding about `sample` points
+    frac = min(1.0, sample / len(x))
+    side = int(round(50000 * np.sqrt(frac)))
+    m = (x < side) & (y < side)
+    xs, ys, zs = x[m], y[m], z[m]
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    t = o.tree(*(syn.to_double(v) for v in (xs, ys, zs)))
+    for st in stages(knn):
+        t.run_stage(st, mode=0, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": len(xs) / dt / 1e6, "unit": "Mpts/s", "cores": threads,
+            "kind": kind, "sample": f"{len(xs)}-point window ({side / 100:.0f} x "
+                                    f"{side / 100:.0f} m) of the same tile: KD build + "
+                                    f"eigenvalues + normal, {threads} threads",
+            "seconds": dt}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    x, y, z = workload(args.points, 2)
+    for _ in range(args.warmup):
+        cpu_reference(x, y, z, args.knn, args.cpu_sample)
+    vals = [cpu_reference(x, y, z, args.knn, args.cpu_sample) for _ in range(args.steps)]
+    v = statistics.median(r["value"] for r in vals)
+    base = dict(vals[-1])
+    base["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": "Mpts/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * statistics.median(r["seconds"] for r in vals),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"stress tile {args.points} points (seed 2), eigenvalues "
+                                   f"knn={args.knn} then normal knn={args.knn}",
+                       "sample": base["sample"]},
+            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": "Mpts/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import torch
+    from gpupdal_b200.native import Context
+    from gpupdal_b200 import abi
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    x, y, z = workload(args.points, 2 + rank)
+    n = len(x)
+    ctx = Context(local)
+    sts = stages(args.knn)
+    nd = [len(abi.stage_dims(s)) for s in sts]
+    # device-resident inputs and outputs
+    dx, dy, dz = (torch.from_numpy(v).to(dev) for v in (x, y, z))
+    dout = [torch.empty((d, n), dtype=torch.float64, device=dev) for d in nd]
+    # pinned host inputs and outputs for the end-to-end form
+    hx, hy, hz = (torch.from_numpy(v).pin_memory() for v in (x, y, z))
+    hout = [torch.empty((d, n), dtype=torch.float64).pin_memory() for d in nd]
+    hxn, hyn, hzn = hx.numpy(), hy.numpy(), hz.numpy()
+    houtn = [h.numpy() for h in hout]
+
+    def step_device():
+        tile = ctx.tile(dx, dy, dz)
+        _, ex, st = ctx.run(tile, sts, device_out=True, out=dout, exception_capacity=1 << 16)
+        tile.free()
+        return st
+
+    def step_e2e():
+        tile = ctx.tile(hxn, hyn, hzn)
+        _, ex, st = ctx.run(tile, sts, out=houtn, fresh=True, exception_capacity=1 << 16)
+        tile.free()
+        return st
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if ws == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps):
+        stats = []
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            stats.append(fn())
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        return e0.elapsed_time(e1), stats
+
+    for _ in range(max(args.warmup, 3)):
+        step_device()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, stats = timed(step_device, args.steps)
+    clk = clocks.stop()
+    ms = max_over_ranks(ms)
+    per_step = ms / args.steps
+    value = ws * n / (per_step / 1e3) / 1e6
+    query_ms = statistics.mean(s.query_ms for s in stats)
+    launches = int(sum(s.kernel_launches for s in stats))
+    hbm, peak_kind = peaks()
+    achieved = n * BYTES_PER_POINT / (query_ms / 1e3) / 1e9
+    # end to end through the C ABI with host buffers
+    for _ in range(2):
+        step_e2e()
+    ms_e2e, stats_e2e = timed(step_e2e, args.steps)
+    ms_e2e = max_over_ranks(ms_e2e)
+    e2e_value = ws * n / (ms_e2e / args.steps / 1e3) / 1e6
+    last = stats[-1]
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+i64+f64", "data": "synthetic",
+        "config": {"workload": f"stress tile {n} points per GPU (seed 2+rank), filters.eigenvalues "
+                               f"knn={args.knn} then filters.normal knn={args.knn}, one grid",
+                   "points_per_gpu": n, "knn": args.knn, "form": "plain per-tile launch",
+                   "l2": "inputs larger than L2 (tile 384 MB + sorted copy 512 MB per step)",
+                   "tie_rows": int(last.tie_rows), "deferred_rows": int(last.deferred_rows),
+                   "grid_ms": last.grid_ms, "query_ms": last.query_ms, "tree_ms": last.tree_ms},
+        "e2e": {"value": e2e_value, "unit": "Mpts/s", "h2d_bytes_per_step": 12 * n,
+                "d2h_bytes_per_step": 8 * sum(nd) * n},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "kernel": "knn_fused_kernel", "peak_source": peak_kind,
+                     "bytes_per_point": BYTES_PER_POINT},
+        "clocks": clk,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference(x, y, z, args.knn, args.cpu_sample)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -105,6 +105,7 @@ class RunStats(ctypes.Structure):
         ("query_ms", ctypes.c_double),
         ("tree_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
+        ("kernel_launches", ctypes.c_uint64),
     ]
 
 

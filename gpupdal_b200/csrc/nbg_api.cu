@@ -41,27 +41,58 @@ static int cuda_fail(Context* c, cudaError_t e, const char* what) {
         if (e__ != cudaSuccess) return cuda_fail(ctx, e__, what); \
     } while (0)
 
-static int dev_alloc(Context* ctx, void** p, size_t bytes, uint64_t* account) {
-    if (bytes == 0) bytes = 16;
+std::atomic<uint64_t> g_launches{0};
+
+static size_t round_bytes(size_t bytes) { return bytes == 0 ? 256 : ((bytes + 255) / 256) * 256; }
+
+void ctx_trim(Context* ctx) {
+    for (auto& kv : ctx->cache) cudaFree(kv.second);
+    ctx->used -= std::min<uint64_t>(ctx->used, ctx->cached);
+    ctx->cache.clear();
+    ctx->cached = 0;
+}
+
+int ctx_alloc(Context* ctx, void** p, size_t bytes) {
+    bytes = round_bytes(bytes);
+    auto it = ctx->cache.find(bytes);
+    if (it != ctx->cache.end()) {
+        *p = it->second;
+        ctx->cache.erase(it);
+        ctx->cached -= bytes;
+        return NBG_OK;
+    }
+    if (ctx->budget && ctx->used + bytes > ctx->budget) ctx_trim(ctx);
     if (ctx->budget && ctx->used + bytes > ctx->budget)
         return fail(ctx, NBG_ERR_BUDGET, "HBM budget exceeded");
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        *p = nullptr;
-        return fail(ctx, NBG_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        ctx_trim(ctx);
+        e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            return fail(ctx, NBG_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
     }
     ctx->used += bytes;
-    if (account) *account += bytes;
     return NBG_OK;
 }
 
-static void dev_free(Context* ctx, void* p, size_t bytes) {
+void ctx_free(Context* ctx, void* p, size_t bytes) {
     if (!p) return;
-    cudaFree(p);
-    if (bytes == 0) bytes = 16;
-    ctx->used = ctx->used >= bytes ? ctx->used - bytes : 0;
+    bytes = round_bytes(bytes);
+    ctx->cache.emplace(bytes, p);
+    ctx->cached += bytes;
 }
+
+static int dev_alloc(Context* ctx, void** p, size_t bytes, uint64_t* account) {
+    int rc = ctx_alloc(ctx, p, bytes);
+    if (rc == NBG_OK && account) *account += round_bytes(bytes);
+    return rc;
+}
+
+static void dev_free(Context* ctx, void* p, size_t bytes) { ctx_free(ctx, p, bytes); }
 
 static int ensure_scratch(Context* ctx, uint64_t n, uint64_t ex_cap) {
     if (ctx->exact_cap < n) {
@@ -163,6 +194,7 @@ int nbg_destroy(nbg_context* h) {
     dev_free(ctx, ctx->exact_rows, ctx->exact_cap * 4);
     dev_free(ctx, ctx->ex_rows, ctx->ex_cap * sizeof(nbg_row_exception));
     dev_free(ctx, ctx->counters, 64 * sizeof(uint32_t));
+    ctx_trim(ctx);
     if (ctx->events)
         for (int i = 0; i < 8; ++i) cudaEventDestroy(ctx->ev[i]);
     delete h;
@@ -284,6 +316,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     cudaStream_t stream = (cudaStream_t)stream_v;
     if (n_exceptions) *n_exceptions = 0;
     if (stats) std::memset(stats, 0, sizeof(*stats));
+    const uint64_t launches0 = g_launches.load();
     if (n_stages < 0 || n_stages > NBG_MAX_STAGES || (n_stages && (!stages || !outputs)))
         return fail(ctx, NBG_ERR_INVALID, "bad stage array");
     bool need_aux = false;
@@ -490,6 +523,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         float ms = 0;
         cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[6]);
         stats->total_ms = ms;
+        stats->kernel_launches = g_launches.load() - launches0;
     }
     cleanup();
     if (nex > exception_capacity)

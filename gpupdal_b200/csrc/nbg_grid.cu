@@ -156,6 +156,7 @@ int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
         return NBG_ERR_CUDA;
     cell_scatter_kernel<<<grid_blocks(n, 256, sms), 256, 0, stream>>>(
         t->x, t->y, t->z, n, t->gp, t->keys, t->cursor, t->sorted);
+    NBG_LAUNCHED(7);  // five grid kernels + the two kernels of the scan
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
 }
 

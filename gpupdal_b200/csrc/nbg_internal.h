@@ -3,7 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -13,6 +15,10 @@
 namespace nbg {
 
 struct KdReplica;  // exact nanoflann replica (nbg_kdtree.cu)
+
+// Kernels launched by this library (all contexts), for the per-call count.
+extern std::atomic<uint64_t> g_launches;
+#define NBG_LAUNCHED(n) ::nbg::g_launches.fetch_add((n), std::memory_order_relaxed)
 
 struct Context {
     int device = 0;
@@ -29,7 +35,17 @@ struct Context {
     uint64_t ex_cap = 0;
     cudaEvent_t ev[8];
     bool events = false;
+    // device blocks released by earlier calls, kept for reuse by size
+    std::multimap<size_t, void*> cache;
+    uint64_t cached = 0;
 };
+
+// Device allocation through the context: reuses a cached block of the same
+// size, honours the HBM budget (cached blocks are released first when the
+// budget would be exceeded).  Returns NBG_OK, NBG_ERR_BUDGET or NBG_ERR_OOM.
+int ctx_alloc(Context* ctx, void** p, size_t bytes);
+void ctx_free(Context* ctx, void* p, size_t bytes);
+void ctx_trim(Context* ctx);
 
 struct Tile {
     uint64_t n = 0;

@@ -109,6 +109,7 @@ struct KdReplica {
     double root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
     bool built = false;
     uint64_t bytes = 0;
+    std::vector<std::pair<void*, size_t>> blocks;  // device blocks owned
 };
 
 // ---------------------------------------------------------------------------
@@ -631,19 +632,21 @@ __global__ void kd_scatter_ids_kernel(const uint32_t* __restrict__ rows, uint32_
 // host side
 // ---------------------------------------------------------------------------
 static int kd_alloc(Context* ctx, void** p, size_t bytes, KdReplica* kd) {
-    if (bytes == 0) bytes = 16;
-    if (ctx->budget && ctx->used + bytes > ctx->budget) {
-        ctx->err = "HBM budget exceeded (KD replica)";
-        return NBG_ERR_BUDGET;
-    }
-    if (cudaMalloc(p, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        ctx->err = "cudaMalloc failed (KD replica)";
-        return NBG_ERR_OOM;
-    }
-    ctx->used += bytes;
+    int rc = ctx_alloc(ctx, p, bytes);
+    if (rc) return rc;
     kd->bytes += bytes;
+    kd->blocks.emplace_back(*p, bytes);
     return NBG_OK;
+}
+
+static void kd_release(Context* ctx, KdReplica* kd, void* p) {
+    for (size_t i = 0; i < kd->blocks.size(); ++i)
+        if (kd->blocks[i].first == p) {
+            ctx_free(ctx, p, kd->blocks[i].second);
+            kd->bytes -= kd->blocks[i].second;
+            kd->blocks.erase(kd->blocks.begin() + i);
+            return;
+        }
 }
 
 template <class T>
@@ -654,9 +657,7 @@ static int kd_grow(Context* ctx, T** p, size_t old_n, size_t new_n, KdReplica* k
     if (*p) {
         cudaMemcpyAsync(q, *p, old_n * sizeof(T), cudaMemcpyDeviceToDevice, st);
         cudaStreamSynchronize(st);
-        cudaFree(*p);
-        ctx->used -= old_n * sizeof(T);
-        kd->bytes -= old_n * sizeof(T);
+        kd_release(ctx, kd, *p);
     }
     *p = q;
     return NBG_OK;
@@ -667,13 +668,7 @@ uint64_t kd_bytes(uint64_t n) { return n * 24 + (n / 16 + 1024) * 64; }
 void kd_free(Context* ctx, Tile* t) {
     KdReplica* kd = t->kd;
     if (!kd) return;
-    ctx->used = ctx->used >= kd->bytes ? ctx->used - kd->bytes : 0;
-    void* ptrs[] = {kd->rx, kd->ry, kd->rz, kd->rid, kd->mlpos, kd->mrpos, kd->c1, kd->c2,
-                    kd->feat, kd->nb, kd->ne, kd->dlo, kd->dhi, kd->bmin, kd->bmax, kd->seg[0],
-                    kd->seg[1], kd->seg2, kd->split, kd->nt, kd->tile_seg, kd->tile_cnt,
-                    kd->scan_tmp, kd->counters};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    for (auto& b : kd->blocks) ctx_free(ctx, b.first, b.second);
     delete kd;
     t->kd = nullptr;
 }
@@ -692,8 +687,8 @@ static int kd_tiles(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, 
     }
     if (total + 1 > kd->tile_cap) {
         uint32_t cap = std::max<uint32_t>(total + 1, kd->tile_cap * 2);
-        if (kd->tile_seg) cudaFree(kd->tile_seg);
-        if (kd->tile_cnt) cudaFree(kd->tile_cnt);
+        if (kd->tile_seg) kd_release(ctx, kd, kd->tile_seg);
+        if (kd->tile_cnt) kd_release(ctx, kd, kd->tile_cnt);
         kd->tile_seg = kd->tile_cnt = nullptr;
         int rc = kd_alloc(ctx, (void**)&kd->tile_seg, (size_t)cap * 4, kd);
         if (!rc) rc = kd_alloc(ctx, (void**)&kd->tile_cnt, (size_t)(cap + 1) * 4, kd);
@@ -701,6 +696,7 @@ static int kd_tiles(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, 
         kd->tile_cap = cap;
     }
     if (total) kd_fill_tiles_kernel<<<(total + 255) / 256, 256, 0, st>>>(kd->nt, S, total, kd->tile_seg);
+    NBG_LAUNCHED(3 + (total ? 1 : 0));
     *ntiles = total;
     return NBG_OK;
 }
@@ -729,6 +725,7 @@ static int kd_pass(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, c
                                                          kd->mlpos, kd->mrpos, kd->rx, kd->ry,
                                                          kd->rz, kd->rid);
     }
+    NBG_LAUNCHED(3 + (ntiles ? 3 : 0));
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
 }
 
@@ -775,6 +772,7 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
     }
     kd_init_kernel<<<std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, ctx->sm_count * 8)), 256, 0,
                      st>>>(t->x, t->y, t->z, n, kd->rx, kd->ry, kd->rz, kd->rid);
+    NBG_LAUNCHED(1);
     // root: actual bbox, as calculateBounds
     const GridParams& g = t->host_gp;
     const Transform& tf = t->tf;
@@ -827,6 +825,7 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
             kd_minmax_kernel<<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->rx, kd->ry,
                                                          kd->rz, kd->split);
         kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, tf);
+        NBG_LAUNCHED(2 + (ntiles ? 1 : 0));
         rc = kd_pass<1>(ctx, kd, segs, S, tf, st);
         if (rc) return rc;
         kd_pass2_segs_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg2);
@@ -834,6 +833,7 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
         if (rc) return rc;
         uint32_t cnt[3] = {0, kd->node_count, 0};
         cudaMemcpyAsync(kd->counters, cnt, 12, cudaMemcpyHostToDevice, st);
+        NBG_LAUNCHED(2);
         kd_children_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg[cur ^ 1],
                                                             kd->counters, kd->c1, kd->c2, kd->feat,
                                                             kd->nb, kd->ne, kd->node_cap,
@@ -871,6 +871,7 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
     }
     kd_div_kernel<<<(nn + 127) / 128, 128, 0, st>>>(nn, kd->c1, kd->c2, kd->feat, kd->bmin,
                                                     kd->bmax, tf, kd->dlo, kd->dhi);
+    NBG_LAUNCHED(kd->level_begin.size());
     if (cudaStreamSynchronize(st) != cudaSuccess) {
         ctx->err = "KD replica extents failed";
         return NBG_ERR_CUDA;
@@ -906,18 +907,19 @@ static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, ui
     KdReplica* kd = t->kd;
     *nbr = nullptr;
     *counts = nullptr;
-    if (cudaMalloc((void**)nbr, (size_t)nrows * K * 4) != cudaSuccess ||
-        cudaMalloc((void**)counts, (size_t)nrows * 4) != cudaSuccess) {
-        cudaGetLastError();
-        if (*nbr) cudaFree(*nbr);
+    int arc = ctx_alloc(ctx, (void**)nbr, (size_t)nrows * K * 4);
+    if (!arc) arc = ctx_alloc(ctx, (void**)counts, (size_t)nrows * 4);
+    if (arc) {
+        if (*nbr) ctx_free(ctx, *nbr, (size_t)nrows * K * 4);
         *nbr = nullptr;
-        ctx->err = "cudaMalloc failed (exact rows)";
-        return NBG_ERR_OOM;
+        *counts = nullptr;
+        return arc;
     }
     cudaMemsetAsync(kd->counters + 2, 0, 4, st);
     kd_search_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(kd_view(kd), t->tf, t->x, t->y, t->z,
                                                           rows, nrows, K, *nbr, *counts,
                                                           kd->counters + 2);
+    NBG_LAUNCHED(1);
     cudaError_t le = cudaGetLastError();
     uint32_t err = 0;
     if (le == cudaSuccess) le = cudaMemcpyAsync(&err, kd->counters + 2, 4, cudaMemcpyDeviceToHost, st);
@@ -941,6 +943,7 @@ int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const Excep
     if (!rc) {
         kd_finish_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(t->tf, t->x, t->y, t->z, rows, nrows,
                                                               K, nbr, counts, grp, ex);
+        NBG_LAUNCHED(1);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
@@ -948,8 +951,8 @@ int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const Excep
             rc = NBG_ERR_CUDA;
         }
     }
-    if (nbr) cudaFree(nbr);
-    if (counts) cudaFree(counts);
+    if (nbr) ctx_free(ctx, nbr, (size_t)nrows * K * 4);
+    if (counts) ctx_free(ctx, counts, (size_t)nrows * 4);
     return rc;
 }
 
@@ -961,6 +964,7 @@ int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_
     if (!rc) {
         kd_scatter_ids_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(rows, nrows, K, nbr, counts,
                                                                    ids_out);
+        NBG_LAUNCHED(1);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
@@ -968,8 +972,8 @@ int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_
             rc = NBG_ERR_CUDA;
         }
     }
-    if (nbr) cudaFree(nbr);
-    if (counts) cudaFree(counts);
+    if (nbr) ctx_free(ctx, nbr, (size_t)nrows * K * 4);
+    if (counts) ctx_free(ctx, counts, (size_t)nrows * 4);
     return rc;
 }
 

@@ -344,6 +344,7 @@ struct KnnLauncher {
             knn_ids_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
         else
             knn_fused_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
+        NBG_LAUNCHED(1);
         return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
     }
 };

@@ -32,6 +32,7 @@ class Context:
             raise NbgError(rc, "nbg_create failed (no sm_100 device?)")
         self.h = h
         self.device = device
+        self._exc_buf = {}
 
     def close(self):
         if getattr(self, "h", None):
@@ -82,7 +83,10 @@ class Context:
             for d in range(nd):
                 c.offset[d] = d * n * 8
         cap = exception_capacity if exception_capacity is not None else max(1024, n)
-        exc = (abi.RowException * cap)()
+        exc = self._exc_buf.get(cap)
+        if exc is None:
+            exc = (abi.RowException * cap)()
+            self._exc_buf = {cap: exc}
         nexc = ctypes.c_uint32(0)
         stats = abi.RunStats()
         kp = rp = None

@@ -134,6 +134,7 @@ typedef struct nbg_run_stats {
     double query_ms;          /* device time of the fused query kernel(s)       */
     double tree_ms;           /* device time of the KD replica build + DFS      */
     double total_ms;          /* device time of the whole call                  */
+    uint64_t kernel_launches; /* device kernels this library launched in the call */
 } nbg_run_stats;
 
 typedef struct nbg_context nbg_context;
