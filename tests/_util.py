@@ -7,9 +7,11 @@ Tolerances (the bar of the parity tests):
   * normals: ||d|| <= 1e-5 on rows whose relative eigen-gap
     (lambda1 - lambda0) / lambda2 is >= 1e-4 (below that the eigenvector is
     not determined by the data; the reference's own choice is arbitrary).
-    With always_up, a row whose NormalZ is within 1e-9 of zero has no
+    With always_up, a row whose NormalZ is within `sign_eps` of zero has no
     determined sign (the flip test n_z < 0 sees rounding residue); such rows
-    are compared up to sign
+    are compared up to sign.  sign_eps is 1e-9 against the FP64 oracle and
+    1e-6 against the reference's own outputs, whose float narrowing moves
+    NormalZ by up to ~1e-7
   * curvature and ratio features in [0, 1]: |d| <= 1e-5
   * EigenvalueSum, Omnivariance, Eigenentropy, Density: relative 1e-5 of
     max(|value|, lambda scale)
@@ -58,7 +60,7 @@ def eigen_scale(eig_f64):
 
 
 def compare_stage(opts, got, want, want_status, got_status, lam=None, label="", gap_min=1e-4,
-                  tol=TOL):
+                  tol=TOL, sign_eps=1e-9):
     """Asserts `got` (ndims, n) matches `want` within the stated bars.
 
     `lam` is the (3, n) ascending eigenvalue array of the accuracy oracle
@@ -81,7 +83,7 @@ def compare_stage(opts, got, want, want_status, got_status, lam=None, label="", 
         lscale = lmax
     vec_ok = gap >= gap_min
     if opts.kind == abi.STAGE_NORMAL and opts.always_up and not opts.has_viewpoint:
-        flat = np.abs(want[2]) < 1e-9
+        flat = np.abs(want[2]) < sign_eps
         if flat.any():
             got = got.copy()
             flip = flat & (np.abs(got[:3] - want[:3]).sum(0) > np.abs(got[:3] + want[:3]).sum(0))

@@ -59,7 +59,7 @@ def test_stages_match_reference_golden(nbg, port, name):
                         label=f"{name}/{sname} vs f64")
         # the reference's own outputs, on rows its float narrowing cannot blur
         U.compare_stage(o, outs[0], g[sname + "_out"], g[sname + "_status"], got_status, lam=lam,
-                        label=f"{name}/{sname} vs reference", gap_min=1e-2)
+                        label=f"{name}/{sname} vs reference", gap_min=1e-2, sign_eps=1e-6)
 
 
 def test_kd_replica_matches_reference_tree(nbg, port):
