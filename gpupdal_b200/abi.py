@@ -55,6 +55,7 @@ ROW_EIGEN_FAIL = 3
 ROW_ZERO_LAMBDA = 4
 
 MAX_DIMS = 16
+NOALLOC_MAX_POINTS = 524288
 
 NORMAL_DIMS = ["NormalX", "NormalY", "NormalZ", "Curvature"]
 EIGENVALUE_DIMS = ["Eigenvalue0", "Eigenvalue1", "Eigenvalue2"]
@@ -176,6 +177,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_run.restype = ctypes.c_int
     lib.nbg_neighbor_sets.argtypes = [vp, vp, i32, vp, i32, ctypes.POINTER(RunStats), vp]
     lib.nbg_neighbor_sets.restype = ctypes.c_int
+    lib.nbg_stage_noalloc.argtypes = [vp, vp, vp, u64, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(StageOpts),
+                                      ctypes.POINTER(Columns), vp, vp, vp,
+                                      ctypes.POINTER(ctypes.c_uint32), vp, ctypes.c_uint32,
+                                      ctypes.POINTER(ctypes.c_uint32), vp, ctypes.c_char_p,
+                                      ctypes.c_size_t]
+    lib.nbg_stage_noalloc.restype = ctypes.c_int
     lib.nbg_debug_kd_export.argtypes = [vp, vp] + [vp] * 9 + [ctypes.c_uint32]
     lib.nbg_debug_kd_export.restype = ctypes.c_int
     _LIB = lib

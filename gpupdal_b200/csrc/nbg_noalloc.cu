@@ -1,0 +1,199 @@
+// nbg_noalloc.cu — one stage over one tile without any device allocation.
+//
+// Some callers cannot allocate device memory at the time they need
+// neighbourhood geometry: code running inside another framework's memory
+// pool or allocator (a host application that owns every device byte), a
+// real-time loop that must not call cudaMalloc/cudaFree (they can block the
+// device), or a plug-in whose host forbids allocation in its processing
+// callback.  nbg_stage_noalloc serves them: the caller passes device inputs
+// and outputs, and every byte of working memory (the uniform grid: cell keys,
+// cell table, points in cell order, the scan's temporary storage and the
+// counters) comes from one file-scope device array of fixed size.
+//
+// What it runs: the grid build and the fused kNN + covariance + eigensolve +
+// projection kernel of the regular path.  Rows whose neighbour set depends on
+// the reference's tie order, or whose search did not finish within the ring
+// limit, need the exact KD replica, whose working memory grows with the tile;
+// this entry point does not build it and instead returns those point ids to
+// the caller (who can answer them later with nbg_run).
+//
+// The array is shared by every call in the process on a given device and
+// keeps the last call's contents; the entry point clears what must start at
+// zero.  Calls whose work overlaps on the same device race on it.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+
+#include "nbg_internal.h"
+
+namespace nbg {
+namespace {
+
+constexpr uint64_t kMaxPoints = NBG_NOALLOC_MAX_POINTS;
+constexpr uint64_t kCellsCap = 2 * kMaxPoints + 1024;
+constexpr size_t kScanReserve = 1u << 20;  // CUB scan temporary storage
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kOffBbox = 0;
+constexpr size_t kOffGp = kOffBbox + 256;
+constexpr size_t kOffCounters = kOffGp + align256(sizeof(GridParams));
+constexpr size_t kOffKeys = kOffCounters + 256;
+constexpr size_t kOffStart = kOffKeys + align256(kMaxPoints * 4);
+constexpr size_t kOffCursor = kOffStart + align256((kCellsCap + 1) * 4);
+constexpr size_t kOffSorted = kOffCursor + align256((kCellsCap + 1) * 4);
+constexpr size_t kOffScan = kOffSorted + align256(kMaxPoints * 16);
+constexpr size_t kArenaBytes = kOffScan + kScanReserve;
+
+// All working memory of nbg_stage_noalloc (about 19.4 MB); held by every
+// device that loads this library until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_arena[kArenaBytes];
+
+// Device address of g_noalloc_arena per device, looked up once per device.
+constexpr int kMaxDevices = 64;
+unsigned char* g_arena_ptr[kMaxDevices] = {nullptr};
+
+int set_msg(char* buf, size_t len, int code, const char* msg) {
+    if (buf && len) {
+        std::strncpy(buf, msg, len - 1);
+        buf[len - 1] = '\0';
+    }
+    return code;
+}
+
+}  // namespace
+}  // namespace nbg
+
+using namespace nbg;
+
+extern "C" int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32_t* z, uint64_t n,
+                                 const double scale[3], const double offset[3],
+                                 const nbg_stage_opts* opts, const nbg_columns* out,
+                                 const double* optimal_knn, const double* optimal_radius,
+                                 uint32_t* unresolved, uint32_t* n_unresolved,
+                                 nbg_row_exception* exceptions, uint32_t exception_capacity,
+                                 uint32_t* n_exceptions, void* stream_v, char* err_msg,
+                                 size_t err_len) {
+    if (n_unresolved) *n_unresolved = 0;
+    if (n_exceptions) *n_exceptions = 0;
+    if (!opts || !out || !scale || !offset || !n_unresolved || !n_exceptions)
+        return set_msg(err_msg, err_len, NBG_ERR_INVALID, "null argument");
+    if (n > kMaxPoints)
+        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED,
+                       "tile larger than NBG_NOALLOC_MAX_POINTS; use nbg_tile_upload + nbg_run");
+    if (n > 0 && (!x || !y || !z || !unresolved))
+        return set_msg(err_msg, err_len, NBG_ERR_INVALID, "null device array");
+    if (scale[0] != scale[1] || scale[0] != scale[2] || !(scale[0] > 0.0))
+        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "needs one positive scale for x, y, z");
+    if (opts->kind < 1 || opts->kind > 3 || opts->knn < 0 || opts->knn > 64)
+        return set_msg(err_msg, err_len, NBG_ERR_INVALID, "invalid stage options");
+    if (opts->kind != NBG_STAGE_NORMAL && opts->stride > 1)
+        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "stride > 1 is not supported");
+    if (opts->kind == NBG_STAGE_COVARIANCEFEATURES && opts->optimized)
+        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "optimized is not supported");
+    const int ndims = opts->kind == NBG_STAGE_NORMAL ? 4
+                      : opts->kind == NBG_STAGE_EIGENVALUES
+                          ? 3
+                          : __builtin_popcount(opts->feature_mask & NBG_FEAT_ALL);
+    if (out->ndims != ndims || out->on_device != 1)
+        return set_msg(err_msg, err_len, NBG_ERR_INVALID, "outputs must be device columns of the stage");
+    if (opts->kind == NBG_STAGE_COVARIANCEFEATURES && (opts->feature_mask & NBG_FEAT_DENSITY) &&
+        (!optimal_knn || !optimal_radius))
+        return set_msg(err_msg, err_len, NBG_ERR_INVALID, "Density needs OptimalKNN and OptimalRadius");
+    if (n == 0) return NBG_OK;
+    cudaStream_t stream = (cudaStream_t)stream_v;
+
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return set_msg(err_msg, err_len, NBG_ERR_NO_DEVICE, "no current device");
+    // First call on this device: look up the array's device address (the
+    // host-side symbol is not a device address).  Make this first call
+    // outside any stream capture.
+    if (!g_arena_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_arena);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return set_msg(err_msg, err_len, NBG_ERR_CUDA, "cudaGetSymbolAddress failed");
+        }
+        g_arena_ptr[dev] = (unsigned char*)p;
+    }
+    unsigned char* arena = g_arena_ptr[dev];
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+
+    Context ctx;  // carries the SM count for the launch shapes; allocates nothing
+    ctx.device = dev;
+    ctx.sm_count = sms;
+    Tile t;
+    t.n = n;
+    t.x = const_cast<int32_t*>(x);
+    t.y = const_cast<int32_t*>(y);
+    t.z = const_cast<int32_t*>(z);
+    for (int d = 0; d < 3; ++d) {
+        t.tf.scale[d] = scale[d];
+        t.tf.offset[d] = offset[d];
+    }
+    t.bbox = (int32_t*)(arena + kOffBbox);
+    t.gp = (GridParams*)(arena + kOffGp);
+    t.keys = (uint32_t*)(arena + kOffKeys);
+    t.cell_start = (uint32_t*)(arena + kOffStart);
+    t.cursor = (uint32_t*)(arena + kOffCursor);
+    t.sorted = (float4*)(arena + kOffSorted);
+    t.ncells_cap = 2 * n + 1024;
+    t.scan_tmp = arena + kOffScan;
+    t.scan_tmp_bytes = scan_temp_bytes(t.ncells_cap + 1);
+    if (t.scan_tmp_bytes > kScanReserve)
+        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "scan storage exceeds its reserve");
+    uint32_t* counters = (uint32_t*)(arena + kOffCounters);
+    const int K = (int)(n < (uint64_t)opts->knn + 1 ? n : (uint64_t)opts->knn + 1);
+
+    // counters start at zero on every call (the array keeps the last call's)
+    if (cudaMemsetAsync(counters, 0, 256, stream) != cudaSuccess)
+        return set_msg(err_msg, err_len, NBG_ERR_CUDA, "counter reset failed");
+    int rc = build_grid(&ctx, &t, K, stream);
+    if (rc) return set_msg(err_msg, err_len, rc, "grid build failed");
+    GridParams hg;
+    cudaError_t e = cudaMemcpyAsync(&hg, t.gp, sizeof(GridParams), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return set_msg(err_msg, err_len, NBG_ERR_CUDA, cudaGetErrorString(e));
+    if ((int64_t)hg.maxx - hg.minx >= (1 << 24) || (int64_t)hg.maxy - hg.miny >= (1 << 24) ||
+        (int64_t)hg.maxz - hg.minz >= (1 << 24))
+        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "tile extent must be below 2^24 raw units");
+
+    StageGroup g{};
+    g.nstages = 1;
+    g.stage_index[0] = 0;
+    g.optimal_knn = optimal_knn;
+    g.optimal_radius = optimal_radius;
+    StageDev& d = g.st[0];
+    d.kind = opts->kind;
+    d.always_up = opts->always_up;
+    d.has_viewpoint = opts->has_viewpoint;
+    d.normalize = opts->normalize;
+    for (int k = 0; k < 3; ++k) d.viewpoint[k] = opts->viewpoint[k];
+    d.feature_mask = opts->feature_mask & NBG_FEAT_ALL;
+    d.mode = opts->mode;
+    d.ndims = ndims;
+    d.base = (char*)out->base;
+    d.point_stride = out->point_stride;
+    for (int k = 0; k < NBG_MAX_DIMS; ++k) d.offset[k] = out->offset[k];
+    QueryLaunch ql;
+    ql.tile = &t;
+    ql.K = K;
+    ql.rmax = 8;
+    ql.grp = g;
+    ql.ex = ExceptionSink{exceptions, counters + 3, exception_capacity};
+    ql.exact_rows = unresolved;
+    ql.counters = counters;
+    rc = launch_query(&ctx, ql, stream);
+    if (rc) return set_msg(err_msg, err_len, rc, "query launch failed");
+    uint32_t cnt[4] = {0, 0, 0, 0};
+    e = cudaMemcpyAsync(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return set_msg(err_msg, err_len, NBG_ERR_CUDA, cudaGetErrorString(e));
+    *n_unresolved = cnt[0];
+    *n_exceptions = cnt[3];
+    if (cnt[3] > exception_capacity)
+        return set_msg(err_msg, err_len, NBG_ERR_EXCEPTIONS, "row-exception list overflowed");
+    return NBG_OK;
+}

@@ -182,6 +182,40 @@ int nbg_neighbor_sets(nbg_context* ctx, nbg_tile* tile, int32_t knn,
                       uint32_t* ids_out, int32_t ids_on_device,
                       nbg_run_stats* stats, void* stream);
 
+/* No-allocation entry point.  This function has no counterpart in the
+ * reference; it exists for callers that cannot allocate device memory when
+ * they need results: code running inside another framework's allocator or
+ * memory pool, real-time loops that must not call cudaMalloc/cudaFree, and
+ * plug-in hosts that forbid allocation in their processing callbacks.
+ *
+ * Runs one stage over one tile of at most NBG_NOALLOC_MAX_POINTS points.
+ * x/y/z, outputs (on_device must be 1), `unresolved` (capacity n),
+ * `exceptions`, `optimal_knn`/`optimal_radius` are device memory owned by the
+ * caller; n_unresolved / n_exceptions are host pointers.  All working memory
+ * (uniform grid, scan storage, counters: about 19.4 MB) is one fixed device
+ * array inside this library, present on every GPU that loads it until the
+ * process exits; nothing is allocated or freed.  Larger tiles are rejected
+ * with NBG_ERR_UNSUPPORTED and a message in err_msg (caller buffer, may be
+ * null).
+ *
+ * Rows whose neighbour set depends on the reference's tie order (or whose
+ * ring search did not finish) need the exact KD replica, whose memory grows
+ * with the tile; their point ids are written to `unresolved` and their
+ * outputs are left untouched, so the caller can answer them with nbg_run.
+ * Every other row equals what nbg_run writes.
+ *
+ * The first call on each device looks up the array's device address; make
+ * that first call outside any stream capture.  Every call shares the array:
+ * calls whose work overlaps on one device race. */
+#define NBG_NOALLOC_MAX_POINTS 524288u
+int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32_t* z, uint64_t n,
+                      const double scale[3], const double offset[3],
+                      const nbg_stage_opts* opts, const nbg_columns* out,
+                      const double* optimal_knn, const double* optimal_radius,
+                      uint32_t* unresolved, uint32_t* n_unresolved,
+                      nbg_row_exception* exceptions, uint32_t exception_capacity,
+                      uint32_t* n_exceptions, void* stream, char* err_msg, size_t err_len);
+
 /* Diagnostic: the device replica of the reference's KD tree for a tile
  * (built on demand): point order `vind` (n ids) and up to `node_capacity`
  * nodes (child ids or -1, cut dim, divlow, divhigh, vind range).  Mirrors
