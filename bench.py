@@ -210,24 +210,27 @@ def main():
     ctx = Context(local)
     sts = stages(args.knn)
     nd = [len(abi.stage_dims(s)) for s in sts]
-    # device-resident inputs and outputs
+    from gpupdal_b200.native import record_columns
+    # device-resident inputs; outputs as one 64-byte record per point
+    # (Eigenvalue0..2, NormalX/Y/Z, Curvature, unused), sector aligned
     dx, dy, dz = (torch.from_numpy(v).to(dev) for v in (x, y, z))
-    dout = [torch.empty((d, n), dtype=torch.float64, device=dev) for d in nd]
-    # pinned host inputs and outputs for the end-to-end form
+    drec = torch.empty((n, 8), dtype=torch.float64, device=dev)
+    dcols = record_columns(drec.data_ptr(), sts, 64, 1)
+    # pinned host inputs and packed 56-byte host records for the end-to-end form
     hx, hy, hz = (torch.from_numpy(v).pin_memory() for v in (x, y, z))
-    hout = [torch.empty((d, n), dtype=torch.float64).pin_memory() for d in nd]
+    hrec = torch.empty((n, 7), dtype=torch.float64).pin_memory()
+    hcols = record_columns(hrec.data_ptr(), sts, 56, 2)
     hxn, hyn, hzn = hx.numpy(), hy.numpy(), hz.numpy()
-    houtn = [h.numpy() for h in hout]
 
     def step_device():
         tile = ctx.tile(dx, dy, dz)
-        _, ex, st = ctx.run(tile, sts, device_out=True, out=dout, exception_capacity=1 << 16)
+        ex, st = ctx.run_columns(tile, sts, dcols)
         tile.free()
         return st
 
     def step_e2e():
         tile = ctx.tile(hxn, hyn, hzn)
-        _, ex, st = ctx.run(tile, sts, out=houtn, fresh=True, exception_capacity=1 << 16)
+        ex, st = ctx.run_columns(tile, sts, hcols)
         tile.free()
         return st
 

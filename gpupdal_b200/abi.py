@@ -169,6 +169,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_tile_upload.restype = ctypes.c_int
     lib.nbg_tile_free.argtypes = [vp, vp]
     lib.nbg_tile_free.restype = ctypes.c_int
+    lib.nbg_tile_tune.argtypes = [vp, vp, ctypes.c_float, i32]
+    lib.nbg_tile_tune.restype = ctypes.c_int
     lib.nbg_tile_size.argtypes = [vp]
     lib.nbg_tile_size.restype = u64
     lib.nbg_run.argtypes = [vp, vp, ctypes.POINTER(StageOpts), i32, ctypes.POINTER(Columns),

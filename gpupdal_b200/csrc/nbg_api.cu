@@ -116,17 +116,55 @@ static int ensure_scratch(Context* ctx, uint64_t n, uint64_t ex_cap) {
 
 static void tile_release(Context* ctx, Tile* t) {
     kd_free(ctx, t);
-    dev_free(ctx, t->x, t->n * 4);
-    dev_free(ctx, t->y, t->n * 4);
-    dev_free(ctx, t->z, t->n * 4);
+    const uint64_t n = t->n;
+    dev_free(ctx, t->x, n * 4);
+    dev_free(ctx, t->y, n * 4);
+    dev_free(ctx, t->z, n * 4);
     dev_free(ctx, t->bbox, 64);
     dev_free(ctx, t->gp, sizeof(GridParams));
-    dev_free(ctx, t->keys, t->n * 4);
-    dev_free(ctx, t->cell_start, (t->ncells_cap + 1) * 4);
-    dev_free(ctx, t->cursor, (t->ncells_cap + 1) * 4);
-    dev_free(ctx, t->sorted, t->n * 16);
-    dev_free(ctx, t->scan_tmp, t->scan_tmp_bytes);
+    dev_free(ctx, t->colinfo, t->cols_cap * 16);
+    dev_free(ctx, t->ext, (t->cols_cap + 1) * 4);
+    dev_free(ctx, t->table_dev, 16);
+    dev_free(ctx, t->keys, n * 4);
+    dev_free(ctx, t->cstart, t->table_cap * 4);
+    dev_free(ctx, t->cursor, t->table_cap * 4);
+    dev_free(ctx, t->sorted, n * 16);
+    dev_free(ctx, t->grid_tmp, t->grid_tmp_bytes);
     t->x = t->y = t->z = nullptr;
+}
+
+}  // namespace nbg
+
+namespace nbg {
+// Grows the cell table (cstart, cursor) and the scan storage to `entries`.
+int grid_grow_table(Context* ctx, Tile* t, uint64_t entries) {
+    if (t->fixed_storage) {
+        ctx->err = "cell table exceeds the fixed storage";
+        return NBG_ERR_UNSUPPORTED;
+    }
+    const uint64_t cap = std::max<uint64_t>(entries, 2 * t->table_cap);
+    uint32_t *cs = nullptr, *cu = nullptr;
+    int rc = dev_alloc(ctx, (void**)&cs, cap * 4, &t->bytes);
+    if (!rc) rc = dev_alloc(ctx, (void**)&cu, cap * 4, &t->bytes);
+    if (rc) {
+        if (cs) dev_free(ctx, cs, cap * 4);
+        return rc;
+    }
+    dev_free(ctx, t->cstart, t->table_cap * 4);
+    dev_free(ctx, t->cursor, t->table_cap * 4);
+    t->cstart = cs;
+    t->cursor = cu;
+    t->table_cap = cap;
+    const size_t need = grid_temp_bytes(std::max<uint64_t>(cap, t->cols_cap + 1));
+    if (need > t->grid_tmp_bytes) {
+        void* tmp = nullptr;
+        rc = dev_alloc(ctx, &tmp, need, &t->bytes);
+        if (rc) return rc;
+        dev_free(ctx, t->grid_tmp, t->grid_tmp_bytes);
+        t->grid_tmp = tmp;
+        t->grid_tmp_bytes = need;
+    }
+    return NBG_OK;
 }
 
 static int ndims_of(const nbg_stage_opts& o) {
@@ -230,7 +268,8 @@ int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const in
         t->tf.scale[d] = scale[d];
         t->tf.offset[d] = offset[d];
     }
-    t->ncells_cap = 2 * n + 1024;
+    t->cols_cap = std::max<uint64_t>(2 * n + 1024, 1u << 20);
+    t->table_cap = 4 * n + 1024;
     int rc = NBG_OK;
 #define ALLOC(PTR_, NBYTES_) \
     if (!rc) rc = dev_alloc(ctx, (void**)&(PTR_), (NBYTES_), &t->bytes);
@@ -239,12 +278,15 @@ int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const in
     ALLOC(t->z, n * 4);
     ALLOC(t->bbox, 64);
     ALLOC(t->gp, sizeof(GridParams));
+    ALLOC(t->colinfo, t->cols_cap * 16);
+    ALLOC(t->ext, (t->cols_cap + 1) * 4);
+    ALLOC(t->table_dev, 16);
     ALLOC(t->keys, n * 4);
-    ALLOC(t->cell_start, (t->ncells_cap + 1) * 4);
-    ALLOC(t->cursor, (t->ncells_cap + 1) * 4);
+    ALLOC(t->cstart, t->table_cap * 4);
+    ALLOC(t->cursor, t->table_cap * 4);
     ALLOC(t->sorted, n * 16);
-    t->scan_tmp_bytes = scan_temp_bytes(t->ncells_cap + 1);
-    ALLOC(t->scan_tmp, t->scan_tmp_bytes);
+    t->grid_tmp_bytes = grid_temp_bytes(std::max<uint64_t>(t->table_cap, t->cols_cap + 1));
+    ALLOC(t->grid_tmp, t->grid_tmp_bytes);
 #undef ALLOC
     if (rc) {
         tile_release(ctx, t);
@@ -263,6 +305,17 @@ int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const in
         }
     }
     *out = th;
+    return NBG_OK;
+}
+
+int nbg_tile_tune(nbg_context* h, nbg_tile* th, float cell_factor, int32_t fixed_cell) {
+    if (!h || !th) return NBG_ERR_INVALID;
+    if (!(cell_factor > 0.0f) || cell_factor > 64.0f || fixed_cell < 0)
+        return fail(&h->c, NBG_ERR_INVALID, "cell_factor must be in (0, 64], fixed_cell >= 0");
+    std::lock_guard<std::mutex> lock(h->c.mu);
+    th->t.cell_factor = cell_factor;
+    th->t.fixed_cell = fixed_cell;
+    th->t.grid_valid = false;
     return NBG_OK;
 }
 
@@ -348,7 +401,10 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     std::vector<HostOut> hout(n_stages);
     std::vector<nbg_columns> dcols(n_stages);
     double* aux_dev[2] = {nullptr, nullptr};
+    char* packed_dev_c = nullptr;
+    size_t packed_bytes_c = 0;
     auto cleanup = [&]() {
+        if (packed_dev_c) dev_free(ctx, packed_dev_c, packed_bytes_c);
         for (auto& o : hout)
             if (o.dev) dev_free(ctx, o.dev, o.bytes);
         if (!aux_on_device) {
@@ -356,7 +412,46 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             if (aux_dev[1]) dev_free(ctx, aux_dev[1], n * 8);
         }
     };
-    for (int s = 0; s < n_stages; ++s) {
+    // Host outputs that form one packed record (every stage writes fresh
+    // dims into the same base, and the record holds exactly those dims) are
+    // staged on the device in the caller's own layout and copied back with a
+    // single contiguous transfer.
+    char* packed_dev = nullptr;
+    size_t packed_bytes = 0;
+    bool packed = n_stages > 0;
+    {
+        int total = 0;
+        uint64_t seen = 0;
+        for (int s = 0; s < n_stages && packed; ++s) {
+            const nbg_columns& u = outputs[s];
+            if (u.on_device != 2 || u.base != outputs[0].base ||
+                u.point_stride != outputs[0].point_stride)
+                packed = false;
+            for (int d = 0; packed && d < u.ndims; ++d) {
+                const int64_t off = u.offset[d];
+                if (off < 0 || off % 8 || off / 8 >= 64 || (seen >> (off / 8) & 1)) packed = false;
+                else seen |= 1ull << (off / 8);
+            }
+            total += u.ndims;
+        }
+        if (packed && (total == 0 || outputs[0].point_stride != 8 * total)) packed = false;
+    }
+    if (packed) {
+        packed_bytes = n * (size_t)outputs[0].point_stride;
+        rc = dev_alloc(ctx, (void**)&packed_dev, packed_bytes, nullptr);
+        if (rc) return rc;
+        packed_dev_c = packed_dev;
+        packed_bytes_c = packed_bytes;
+        cudaError_t e = cudaMemsetAsync(packed_dev, 0, packed_bytes, stream);
+        if (e) { cleanup(); return cuda_fail(ctx, e, "output staging"); }
+        for (int s = 0; s < n_stages; ++s) {
+            hout[s].user = &outputs[s];
+            dcols[s] = outputs[s];
+            dcols[s].base = packed_dev;
+            dcols[s].on_device = 1;
+        }
+    }
+    for (int s = 0; s < n_stages && !packed; ++s) {
         hout[s].user = &outputs[s];
         dcols[s] = outputs[s];
         if (outputs[s].on_device != 1 && outputs[s].ndims > 0) {
@@ -445,6 +540,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             d.base = (char*)dcols[s].base;
             d.point_stride = dcols[s].point_stride;
             for (int k = 0; k < NBG_MAX_DIMS; ++k) d.offset[k] = dcols[s].offset[k];
+            if (o.kind == NBG_STAGE_NORMAL && !o.always_up && !o.has_viewpoint) g.sign_exact = 1;
         }
         if (cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(uint32_t), stream)) { cleanup(); return NBG_ERR_CUDA; }
         QueryLaunch ql;
@@ -484,6 +580,11 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         }
     }
     // results back to host layouts
+    if (packed) {
+        cudaError_t e = cudaMemcpyAsync(outputs[0].base, packed_dev, packed_bytes,
+                                        cudaMemcpyDeviceToHost, stream);
+        if (e) { cleanup(); return cuda_fail(ctx, e, "output copy"); }
+    }
     for (int s = 0; s < n_stages; ++s) {
         if (!hout[s].dev) continue;
         const nbg_columns& u = outputs[s];

@@ -11,16 +11,25 @@
 #define NBG_MAX_RING 24
 
 // Grid of one tile, written on the device by grid_config_kernel so that the
-// build never waits on the host.  Coordinates are raw int32 relative to the
-// tile minimum; cells are cubes of `cell` raw units, keyed x-fastest so that
-// a run of cells along x is one contiguous range of the sorted points.
+// build never waits on the host for its shape.  Coordinates are raw int32
+// relative to the tile minimum; cells are cubes of `cell` raw units.  Each
+// (cx, cy) column stores a dense run of cells over its own occupied z-range:
+// colinfo[col] = {base, zmin, zmax, 0}, cell (cx, cy, cz) is table entry
+// base + cz - zmin, and cstart[entry] is the cell's first point.
 struct GridParams {
     int32_t minx, miny, minz;
     int32_t maxx, maxy, maxz;
     int32_t cell;
     int32_t gx, gy, gz;
-    uint32_t ncells;
-    uint32_t cap_hit;  // cell size had to grow to fit the cell table
+    uint32_t ncols;    // gx*gy
+    uint32_t cap_hit;  // cell size had to grow to fit the column directory
+};
+
+// Device pointers of a tile's grid.
+struct GridView {
+    const float4* sorted;   // points in cell order {x, y, z, id bits}
+    const int4* colinfo;    // per column {base, zmin, zmax, 0}
+    const uint32_t* cstart; // first point of each table entry (T + 1 entries)
 };
 
 // One stage of a fused group, resolved for the device.
@@ -41,6 +50,7 @@ struct StageDev {
 
 struct StageGroup {
     int32_t nstages;
+    int32_t sign_exact;  // a stage exposes the eigenvector sign: use the Eigen chain
     int32_t stage_index[NBG_MAX_STAGES];  // index in the caller's array
     StageDev st[NBG_MAX_STAGES];
     const double* optimal_knn;     // device, may be null
@@ -220,6 +230,142 @@ __device__ inline int nbg_eigen_chain(const double low[6], double eval[3], doubl
 }
 
 // ---------------------------------------------------------------------------
+// Fast symmetric 3x3 eigensolve: four fixed cyclic Jacobi sweeps in FP32 on
+// the covariance scaled to [-1, 1], then one Jacobi sweep in FP64 on V^T C V
+// (nearly diagonal, so its rotations are small-angle: t = a_pq/(a_qq - a_pp))
+// and FP64 eigenvalues from the polished diagonal.  Uniform control flow, no
+// data-dependent iteration count.  Returns 0 when a polish rotation is not
+// small (|t| > 1e-3: eigenvalues too close for the FP32 basis to be a good
+// start); the caller then re-solves with the FP64 Eigen chain.
+__device__ __forceinline__ void nbg_jrot32(float& app, float& aqq, float& apq, float& arp,
+                                           float& arq, float* vp, float* vq) {
+    if (apq == 0.0f) return;
+    const float theta = 0.5f * (aqq - app) / apq;
+    const float t = copysignf(1.0f, theta) / (fabsf(theta) + sqrtf(fmaf(theta, theta, 1.0f)));
+    const float c = rsqrtf(fmaf(t, t, 1.0f));
+    const float s = t * c;
+    app = fmaf(-t, apq, app);
+    aqq = fmaf(t, apq, aqq);
+    apq = 0.0f;
+    const float rp = arp, rq = arq;
+    arp = c * rp - s * rq;
+    arq = s * rp + c * rq;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float a = vp[k], b = vq[k];
+        vp[k] = c * a - s * b;
+        vq[k] = s * a + c * b;
+    }
+}
+
+__device__ __forceinline__ bool nbg_jrot64(double& app, double& aqq, double& apq, double& arp,
+                                           double& arq, double* vp, double* vq) {
+    if (apq == 0.0) return true;
+    const double den = aqq - app;
+    const double t = apq / den;  // tan of the rotation, first order
+    if (!(fabs(t) <= 1e-3)) return false;
+    const double c = 1.0 - 0.5 * t * t;
+    const double s = t * c;
+    app = app - t * apq;
+    aqq = aqq + t * apq;
+    apq = 0.0;
+    const double rp = arp, rq = arq;
+    arp = c * rp - s * rq;
+    arq = s * rp + c * rq;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double a = vp[k], b = vq[k];
+        vp[k] = c * a - s * b;
+        vq[k] = s * a + c * b;
+    }
+    return true;
+}
+
+// low = {c00, c10, c11, c20, c21, c22}; eval ascending; evec column-major.
+__device__ inline bool nbg_eigen_fast(const double low[6], double eval[3], double evec[9]) {
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) m = fmax(m, fabs(low[i]));
+    if (m == 0.0) m = 1.0;
+    const double inv = 1.0 / m;
+    float a00 = (float)(low[0] * inv), a10 = (float)(low[1] * inv), a11 = (float)(low[2] * inv);
+    float a20 = (float)(low[3] * inv), a21 = (float)(low[4] * inv), a22 = (float)(low[5] * inv);
+    float v0[3] = {1, 0, 0}, v1[3] = {0, 1, 0}, v2[3] = {0, 0, 1};
+#pragma unroll
+    for (int sweep = 0; sweep < 4; ++sweep) {
+        nbg_jrot32(a00, a11, a10, a20, a21, v0, v1);  // (0,1), r = 2
+        nbg_jrot32(a00, a22, a20, a10, a21, v0, v2);  // (0,2), r = 1 (a_10 is a_r0, a_21 a_r2)
+        nbg_jrot32(a11, a22, a21, a10, a20, v1, v2);  // (1,2), r = 0
+    }
+    // FP64 polish on B = V^T C V (C scaled by 1/m).  The FP32 basis is first
+    // made orthonormal in FP64 (Gram-Schmidt, third vector by cross product
+    // with the orientation of the FP32 one), so that B is similar to C.
+    double V[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        V[0][k] = v0[k];
+        V[1][k] = v1[k];
+        V[2][k] = v2[k];
+    }
+    {
+        double r0 = rsqrt(V[0][0] * V[0][0] + V[0][1] * V[0][1] + V[0][2] * V[0][2]);
+        for (int k = 0; k < 3; ++k) V[0][k] *= r0;
+        const double p01 = V[0][0] * V[1][0] + V[0][1] * V[1][1] + V[0][2] * V[1][2];
+        for (int k = 0; k < 3; ++k) V[1][k] -= p01 * V[0][k];
+        double r1 = rsqrt(V[1][0] * V[1][0] + V[1][1] * V[1][1] + V[1][2] * V[1][2]);
+        for (int k = 0; k < 3; ++k) V[1][k] *= r1;
+        const double cx = V[0][1] * V[1][2] - V[0][2] * V[1][1];
+        const double cy = V[0][2] * V[1][0] - V[0][0] * V[1][2];
+        const double cz = V[0][0] * V[1][1] - V[0][1] * V[1][0];
+        const double sg = (cx * V[2][0] + cy * V[2][1] + cz * V[2][2]) < 0 ? -1.0 : 1.0;
+        V[2][0] = sg * cx;
+        V[2][1] = sg * cy;
+        V[2][2] = sg * cz;
+    }
+    const double C00 = low[0] * inv, C10 = low[1] * inv, C11 = low[2] * inv;
+    const double C20 = low[3] * inv, C21 = low[4] * inv, C22 = low[5] * inv;
+    double W[3][3];  // W[i] = C * V[i]
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        W[i][0] = C00 * V[i][0] + C10 * V[i][1] + C20 * V[i][2];
+        W[i][1] = C10 * V[i][0] + C11 * V[i][1] + C21 * V[i][2];
+        W[i][2] = C20 * V[i][0] + C21 * V[i][1] + C22 * V[i][2];
+    }
+    double b00 = V[0][0] * W[0][0] + V[0][1] * W[0][1] + V[0][2] * W[0][2];
+    double b11 = V[1][0] * W[1][0] + V[1][1] * W[1][1] + V[1][2] * W[1][2];
+    double b22 = V[2][0] * W[2][0] + V[2][1] * W[2][1] + V[2][2] * W[2][2];
+    double b10 = V[1][0] * W[0][0] + V[1][1] * W[0][1] + V[1][2] * W[0][2];
+    double b20 = V[2][0] * W[0][0] + V[2][1] * W[0][1] + V[2][2] * W[0][2];
+    double b21 = V[2][0] * W[1][0] + V[2][1] * W[1][1] + V[2][2] * W[1][2];
+    bool ok = nbg_jrot64(b00, b11, b10, b20, b21, V[0], V[1]);
+    ok = ok && nbg_jrot64(b00, b22, b20, b10, b21, V[0], V[2]);
+    ok = ok && nbg_jrot64(b11, b22, b21, b10, b20, V[1], V[2]);
+    if (!ok) return false;
+    // normalise the polished vectors and sort ascending
+    double ev[3] = {b00 * m, b11 * m, b22 * m};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const double r = rsqrt(V[i][0] * V[i][0] + V[i][1] * V[i][1] + V[i][2] * V[i][2]);
+        V[i][0] *= r;
+        V[i][1] *= r;
+        V[i][2] *= r;
+    }
+    int o0 = 0, o1 = 1, o2 = 2;
+    if (ev[o1] < ev[o0]) { int t = o0; o0 = o1; o1 = t; }
+    if (ev[o2] < ev[o1]) { int t = o1; o1 = o2; o2 = t; }
+    if (ev[o1] < ev[o0]) { int t = o0; o0 = o1; o1 = t; }
+    const int ord[3] = {o0, o1, o2};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        eval[c] = ev[ord[c]];
+        evec[c * 3 + 0] = V[ord[c]][0];
+        evec[c * 3 + 1] = V[ord[c]][1];
+        evec[c * 3 + 2] = V[ord[c]][2];
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // Row epilogue shared by the grid path and the exact KD path.
 //
 // M = n*S2 - S1*S1^T over the neighbours' raw offsets from the query (exact
@@ -265,7 +411,7 @@ __device__ inline void nbg_finish_row(const StageGroup& g, const Transform& tf,
     int ok = 1;
     if (!zero) {
         if (nonfinite) ok = 0;
-        else ok = nbg_eigen_chain(C, ev, V);
+        else if (g.sign_exact || !nbg_eigen_fast(C, ev, V)) ok = nbg_eigen_chain(C, ev, V);
     }
     double p[3] = {ref_coord(qraw[0], tf.scale[0], tf.offset[0]),
                    ref_coord(qraw[1], tf.scale[1], tf.offset[1]),
@@ -286,8 +432,24 @@ __device__ inline void nbg_finish_row(const StageGroup& g, const Transform& tf,
                 double dz = st.viewpoint[2] - p[2];
                 double dot = __dadd_rn(__dadd_rn(__dmul_rn(dx, n0), __dmul_rn(dy, n1)),
                                        __dmul_rn(dz, n2));
+                // viewpoint in the tangent plane: the orientation test leaves the
+                // eigensolver's own sign, so take it from the Eigen chain
+                if (!g.sign_exact &&
+                    fabs(dot) <= 1e-12 * (fabs(dx) + fabs(dy) + fabs(dz))) {
+                    double ev2[3], V2[9];
+                    if (nbg_eigen_chain(C, ev2, V2)) {
+                        n0 = V2[0]; n1 = V2[1]; n2 = V2[2];
+                        dot = __dadd_rn(__dadd_rn(__dmul_rn(dx, n0), __dmul_rn(dy, n1)),
+                                        __dmul_rn(dz, n2));
+                    }
+                }
                 if (dot < 0) { n0 = -n0; n1 = -n1; n2 = -n2; }
             } else if (st.always_up) {
+                // horizontal normal: same rule as above, the chain's sign stands
+                if (!g.sign_exact && fabs(n2) <= 1e-12) {
+                    double ev2[3], V2[9];
+                    if (nbg_eigen_chain(C, ev2, V2)) { n0 = V2[0]; n1 = V2[1]; n2 = V2[2]; }
+                }
                 if (n2 < 0) { n0 = -n0; n1 = -n1; n2 = -n2; }
             }
             nbg_store(st, id, 0, n0);

@@ -1,17 +1,30 @@
-// nbg_grid.cu — device uniform grid over quantised int32 coordinates.
+// nbg_grid.cu — column-compacted device grid over quantised int32 coordinates.
 //
 // Replaces the reference's KD3 build on the query side (PointView::build3dIndex,
 // pdal/PointView.cpp:264-290) and the fork's Morton-key CUB sort
-// (src/index/SpatialIndexKernels.cu:1772-1906).  The build is a single-digit
-// radix (counting) sort keyed by the linear cell index:
-//   1. bbox      min/max of the raw coordinates (warp reductions + atomics)
-//   2. config    cell size and grid dims chosen on the device (no host sync)
-//   3. count     cell key per point, histogram of keys
-//   4. scan      exclusive prefix sum of the histogram = cell start table
-//   5. scatter   points into cell order as float4 {x, y, z, id} relative to
-//                the tile minimum (exact: extents < 2^24 raw units)
-// Within-cell order is not fixed; no output depends on it (neighbour sets
-// are exact, covariance sums are exact integers).
+// (src/index/SpatialIndexKernels.cu:1772-1906).
+//
+// Airborne point clouds are 2.5-dimensional with walls, vegetation and wires:
+// a dense 3D cell table over the tile's bounding box is mostly empty, and
+// capping it forces cells far larger than the neighbourhoods.  Here every
+// (cx, cy) column keeps a dense run of cells over its own occupied z-range
+// only:
+//   colinfo[col] = {base, zmin, zmax}      (one 16-byte load per column)
+//   cell (cx, cy, cz) -> table entry base + cz - zmin, for zmin <= cz <= zmax
+//   cstart[entry]     first point of the cell in the sorted point array
+// so a query finds any cell with two dependent loads and scans, per column,
+// one contiguous z-run of cells.  The build is a counting sort keyed by the
+// table entry:
+//   1. bbox      min/max of the raw coordinates
+//   2. config    cell edge from the planar density, grid dims (device)
+//   3. zrange    per-column min/max cell layer (atomics)
+//   4. bases     exclusive scan of the column extents -> table size T
+//   5. count     table entry per point, histogram
+//   6. scan      exclusive scan of the histogram -> cstart
+//   7. scatter   points into cell order as float4 {x, y, z, id} relative to
+//                the tile minimum (exact: extents < 2^24)
+// Within-cell order is not fixed; no output depends on it (neighbour sets are
+// exact, covariance sums are exact integers).
 #include <cub/cub.cuh>
 
 #include "nbg_common.cuh"
@@ -51,10 +64,11 @@ __global__ void bbox_kernel(const int32_t* __restrict__ x, const int32_t* __rest
     }
 }
 
-// Cell edge c = ceil(cell_factor * r_k), r_k the radius holding k1 points
-// on a surface of the tile's planar density; grown until the table fits.
+// Cell edge c = ceil(cell_factor * r_k), r_k the radius holding k1 points on
+// a surface of the tile's planar density; grown only when the column count
+// exceeds the directory.
 __global__ void grid_config_kernel(const int32_t* bb, uint64_t n, int k1, float cell_factor,
-                                   uint64_t ncells_cap, int32_t fixed_cell, GridParams* gp) {
+                                   uint64_t cols_cap, int32_t fixed_cell, GridParams* gp) {
     GridParams g;
     g.minx = bb[0];
     g.miny = bb[1];
@@ -62,48 +76,94 @@ __global__ void grid_config_kernel(const int32_t* bb, uint64_t n, int k1, float 
     g.maxx = bb[3];
     g.maxy = bb[4];
     g.maxz = bb[5];
-    double ex = (double)g.maxx - g.minx + 1.0;
-    double ey = (double)g.maxy - g.miny + 1.0;
-    double ez = (double)g.maxz - g.minz + 1.0;
+    const double ex = (double)g.maxx - g.minx + 1.0;
+    const double ey = (double)g.maxy - g.miny + 1.0;
+    const double ez = (double)g.maxz - g.minz + 1.0;
     double c;
     if (fixed_cell > 0) {
         c = fixed_cell;
     } else {
-        double rho2 = (double)n / (ex * ey);
-        double r = sqrt((double)k1 / (3.14159265358979 * rho2));
+        const double rho2 = (double)n / (ex * ey);
+        const double r = sqrt((double)k1 / (3.14159265358979 * rho2));
         c = ceil((double)cell_factor * r);
     }
     if (c < 1.0) c = 1.0;
     g.cap_hit = 0;
     for (;;) {
-        double gx = floor((ex - 1.0) / c) + 1.0;
-        double gy = floor((ey - 1.0) / c) + 1.0;
-        double gz = floor((ez - 1.0) / c) + 1.0;
-        if (gx * gy * gz <= (double)ncells_cap) {
+        const double gx = floor((ex - 1.0) / c) + 1.0;
+        const double gy = floor((ey - 1.0) / c) + 1.0;
+        if (gx * gy <= (double)cols_cap) {
             g.gx = (int32_t)gx;
             g.gy = (int32_t)gy;
-            g.gz = (int32_t)gz;
+            g.gz = (int32_t)(floor((ez - 1.0) / c) + 1.0);
             break;
         }
         c = ceil(c * 1.25 + 1.0);
         g.cap_hit = 1;
     }
     g.cell = (int32_t)c;
-    g.ncells = (uint32_t)g.gx * (uint32_t)g.gy * (uint32_t)g.gz;
+    g.ncols = (uint32_t)g.gx * (uint32_t)g.gy;
     *gp = g;
+}
+
+__global__ void col_init_kernel(uint32_t ncols_cap, int4* __restrict__ colinfo) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncols_cap;
+         c += gridDim.x * blockDim.x)
+        colinfo[c] = make_int4(0, INT32_MAX, -1, 0);
+}
+
+__global__ void col_zrange_kernel(const int32_t* __restrict__ x, const int32_t* __restrict__ y,
+                                  const int32_t* __restrict__ z, uint64_t n,
+                                  const GridParams* __restrict__ gpp, int4* __restrict__ colinfo) {
+    const GridParams g = *gpp;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t cx = (uint32_t)(x[i] - g.minx) / (uint32_t)g.cell;
+        const uint32_t cy = (uint32_t)(y[i] - g.miny) / (uint32_t)g.cell;
+        const int cz = (int)((uint32_t)(z[i] - g.minz) / (uint32_t)g.cell);
+        int4* ci = &colinfo[cy * (uint32_t)g.gx + cx];
+        atomicMin(&ci->y, cz);
+        atomicMax(&ci->z, cz);
+    }
+}
+
+__global__ void col_extent_kernel(const GridParams* __restrict__ gpp,
+                                  const int4* __restrict__ colinfo, uint32_t* __restrict__ ext) {
+    const uint32_t ncols = gpp->ncols;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncols;
+         c += gridDim.x * blockDim.x) {
+        uint32_t e = 0;
+        if (c < ncols) {
+            const int4 ci = colinfo[c];
+            e = ci.z >= ci.y ? (uint32_t)(ci.z - ci.y + 1) : 0u;
+        }
+        ext[c] = e;
+    }
+}
+
+__global__ void col_base_kernel(const GridParams* __restrict__ gpp, const uint32_t* __restrict__ ext,
+                                int4* __restrict__ colinfo, uint32_t* __restrict__ table_size) {
+    const uint32_t ncols = gpp->ncols;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncols;
+         c += gridDim.x * blockDim.x) {
+        if (c < ncols) colinfo[c].x = (int)ext[c];
+        else *table_size = ext[c];
+    }
 }
 
 __global__ void cell_count_kernel(const int32_t* __restrict__ x, const int32_t* __restrict__ y,
                                   const int32_t* __restrict__ z, uint64_t n,
-                                  const GridParams* __restrict__ gpp, uint32_t* __restrict__ keys,
+                                  const GridParams* __restrict__ gpp,
+                                  const int4* __restrict__ colinfo, uint32_t* __restrict__ keys,
                                   uint32_t* __restrict__ counts) {
     const GridParams g = *gpp;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t cx = (uint32_t)(x[i] - g.minx) / (uint32_t)g.cell;
-        uint32_t cy = (uint32_t)(y[i] - g.miny) / (uint32_t)g.cell;
-        uint32_t cz = (uint32_t)(z[i] - g.minz) / (uint32_t)g.cell;
-        uint32_t key = (cz * (uint32_t)g.gy + cy) * (uint32_t)g.gx + cx;
+        const uint32_t cx = (uint32_t)(x[i] - g.minx) / (uint32_t)g.cell;
+        const uint32_t cy = (uint32_t)(y[i] - g.miny) / (uint32_t)g.cell;
+        const int cz = (int)((uint32_t)(z[i] - g.minz) / (uint32_t)g.cell);
+        const int4 ci = colinfo[cy * (uint32_t)g.gx + cx];
+        const uint32_t key = (uint32_t)ci.x + (uint32_t)(cz - ci.y);
         keys[i] = key;
         atomicAdd(&counts[key], 1u);
     }
@@ -117,7 +177,7 @@ __global__ void cell_scatter_kernel(const int32_t* __restrict__ x, const int32_t
     const GridParams g = *gpp;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t pos = atomicAdd(&cursor[keys[i]], 1u);
+        const uint32_t pos = atomicAdd(&cursor[keys[i]], 1u);
         float4 r;
         r.x = (float)(x[i] - g.minx);
         r.y = (float)(y[i] - g.miny);
@@ -135,36 +195,58 @@ static int grid_blocks(uint64_t n, int threads, int sms) {
     return (int)b;
 }
 
-// Builds the grid of `t` on `stream`.  Scratch: keys (n), counts (cap+1).
+// Bytes of CUB scan storage for `items` entries.
+size_t grid_temp_bytes(uint64_t items) {
+    size_t b = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (int)items);
+    return b + 256;
+}
+
+// Builds the grid of `t` on `stream`.  One host synchronisation reads the
+// table size T (sum of the column extents); the table grows when needed.
 int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
     const uint64_t n = t->n;
     const int sms = ctx->sm_count;
+    const int nb = grid_blocks(n, 256, sms);
     bbox_init_kernel<<<1, 32, 0, stream>>>(t->bbox);
-    bbox_kernel<<<grid_blocks(n, 256, sms), 256, 0, stream>>>(t->x, t->y, t->z, n, t->bbox);
-    grid_config_kernel<<<1, 1, 0, stream>>>(t->bbox, n, k1, t->cell_factor, t->ncells_cap,
+    bbox_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->bbox);
+    grid_config_kernel<<<1, 1, 0, stream>>>(t->bbox, n, k1, t->cell_factor, t->cols_cap,
                                             t->fixed_cell, t->gp);
-    if (cudaMemsetAsync(t->cell_start, 0, (t->ncells_cap + 1) * sizeof(uint32_t), stream))
+    const int cb = grid_blocks(t->cols_cap + 1, 256, sms);
+    col_init_kernel<<<cb, 256, 0, stream>>>((uint32_t)t->cols_cap, t->colinfo);
+    col_zrange_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->colinfo);
+    col_extent_kernel<<<cb, 256, 0, stream>>>(t->gp, t->colinfo, t->ext);
+    size_t tmp = t->grid_tmp_bytes;
+    if (cub::DeviceScan::ExclusiveSum(t->grid_tmp, tmp, t->ext, t->ext, (int)(t->cols_cap + 1),
+                                      stream))
         return NBG_ERR_CUDA;
-    cell_count_kernel<<<grid_blocks(n, 256, sms), 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp,
-                                                                   t->keys, t->cell_start);
-    size_t tmp = t->scan_tmp_bytes;
-    if (cub::DeviceScan::ExclusiveSum(t->scan_tmp, tmp, t->cell_start, t->cell_start,
-                                      (int)(t->ncells_cap + 1), stream) != cudaSuccess)
+    col_base_kernel<<<cb, 256, 0, stream>>>(t->gp, t->ext, t->colinfo, t->table_dev);
+    uint32_t T = 0;
+    if (cudaMemcpyAsync(&T, t->table_dev, 4, cudaMemcpyDeviceToHost, stream) ||
+        cudaStreamSynchronize(stream))
         return NBG_ERR_CUDA;
-    if (cudaMemcpyAsync(t->cursor, t->cell_start, (t->ncells_cap + 1) * sizeof(uint32_t),
+    if ((uint64_t)T + 1 > t->table_cap) {
+        int rc = grid_grow_table(ctx, t, (uint64_t)T + 1);
+        if (rc) return rc;
+    }
+    t->table_size = T;
+    if (cudaMemsetAsync(t->cstart, 0, ((size_t)T + 1) * sizeof(uint32_t), stream))
+        return NBG_ERR_CUDA;
+    cell_count_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->colinfo, t->keys,
+                                              t->cstart);
+    tmp = t->grid_tmp_bytes;
+    if (cub::DeviceScan::ExclusiveSum(t->grid_tmp, tmp, t->cstart, t->cstart, (int)(T + 1),
+                                      stream))
+        return NBG_ERR_CUDA;
+    if (cudaMemcpyAsync(t->cursor, t->cstart, ((size_t)T + 1) * sizeof(uint32_t),
                         cudaMemcpyDeviceToDevice, stream))
         return NBG_ERR_CUDA;
-    cell_scatter_kernel<<<grid_blocks(n, 256, sms), 256, 0, stream>>>(
-        t->x, t->y, t->z, n, t->gp, t->keys, t->cursor, t->sorted);
-    NBG_LAUNCHED(7);  // five grid kernels + the two kernels of the scan
+    cell_scatter_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->keys, t->cursor,
+                                                t->sorted);
+    // bbox (2), config, col init, zrange, extent, scan (2), bases, count, scan (2), scatter
+    NBG_LAUNCHED(13);
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
-}
-
-size_t scan_temp_bytes(uint64_t items) {
-    size_t bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                  (int)items);
-    return bytes;
 }
 
 }  // namespace nbg

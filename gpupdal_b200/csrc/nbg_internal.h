@@ -56,14 +56,20 @@ struct Tile {
     // grid
     int32_t* bbox = nullptr;
     GridParams* gp = nullptr;
-    uint32_t* keys = nullptr;
-    uint32_t* cell_start = nullptr;
-    uint32_t* cursor = nullptr;
-    float4* sorted = nullptr;
-    void* scan_tmp = nullptr;
-    size_t scan_tmp_bytes = 0;
-    uint64_t ncells_cap = 0;
-    float cell_factor = 1.0f;
+    int4* colinfo = nullptr;     // cols_cap: {base, zmin, zmax, 0}
+    uint32_t* ext = nullptr;     // cols_cap + 1: column extents, then bases
+    uint32_t* table_dev = nullptr;
+    uint32_t* keys = nullptr;    // n: table entry of each point
+    uint32_t* cstart = nullptr;  // table_cap: first point of each entry
+    uint32_t* cursor = nullptr;  // table_cap: scatter cursor
+    float4* sorted = nullptr;    // n
+    void* grid_tmp = nullptr;
+    size_t grid_tmp_bytes = 0;
+    uint64_t cols_cap = 0;
+    uint64_t table_cap = 0;
+    uint64_t table_size = 0;
+    bool fixed_storage = false;  // storage provided by the caller: never grow
+    float cell_factor = 4.0f;
     int32_t fixed_cell = 0;
     int grid_k1 = 0;
     bool grid_valid = false;
@@ -74,7 +80,9 @@ struct Tile {
 };
 
 int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream);
-size_t scan_temp_bytes(uint64_t items);
+size_t grid_temp_bytes(uint64_t items);
+int grid_grow_table(Context* ctx, Tile* t, uint64_t entries);
+GridView grid_view(const Tile* t);
 
 struct QueryLaunch {
     const Tile* tile;

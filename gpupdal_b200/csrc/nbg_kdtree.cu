@@ -101,6 +101,7 @@ struct KdReplica {
     uint32_t* nt = nullptr;        // per segment tile count, then prefix (seg_cap+1)
     uint32_t* tile_seg = nullptr;
     uint32_t* tile_cnt = nullptr;  // per tile count, then prefix (tile_cap+1)
+    int32_t* tile_mm = nullptr;    // per tile extents (6 ints)
     uint32_t tile_cap = 0;
     void* scan_tmp = nullptr;
     size_t scan_bytes = 0;
@@ -155,10 +156,12 @@ __global__ void kd_minmax_init_kernel(KdSplit* sp, uint32_t S) {
     }
 }
 
+// Per-tile extents (block reduction) into tile_mm[6*t]: min x,y,z, max x,y,z.
 __global__ void __launch_bounds__(KD_TILE) kd_minmax_kernel(const KdSeg* segs, const uint32_t* tile_first,
                                                             const uint32_t* tile_seg,
                                                             const int32_t* rx, const int32_t* ry,
-                                                            const int32_t* rz, KdSplit* sp) {
+                                                            const int32_t* rz, int32_t* tile_mm) {
+    __shared__ int32_t red[KD_TILE / 32][6];
     const uint32_t t = blockIdx.x;
     const uint32_t s = tile_seg[t];
     const KdSeg sg = segs[s];
@@ -174,11 +177,44 @@ __global__ void __launch_bounds__(KD_TILE) kd_minmax_kernel(const KdSeg* segs, c
         v[d] = __reduce_min_sync(0xffffffffu, v[d]);
         w[d] = __reduce_max_sync(0xffffffffu, w[d]);
     }
-    if ((threadIdx.x & 31) == 0) {
-#pragma unroll
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
         for (int d = 0; d < 3; ++d) {
-            atomicMin(&sp[s].mn[d], v[d]);
-            atomicMax(&sp[s].mx[d], w[d]);
+            red[warp][d] = v[d];
+            red[warp][3 + d] = w[d];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        int32_t r = red[0][threadIdx.x];
+        for (int k = 1; k < KD_TILE / 32; ++k)
+            r = threadIdx.x < 3 ? min(r, red[k][threadIdx.x]) : max(r, red[k][threadIdx.x]);
+        tile_mm[6 * (size_t)t + threadIdx.x] = r;
+    }
+}
+
+// One warp per segment folds its tiles' extents.
+__global__ void kd_seg_minmax_kernel(uint32_t S, const uint32_t* tile_first, const int32_t* tile_mm,
+                                     KdSplit* sp) {
+    const uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (s >= S) return;
+    int32_t v[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, w[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    for (uint32_t t = tile_first[s] + lane; t < tile_first[s + 1]; t += 32) {
+        for (int d = 0; d < 3; ++d) {
+            v[d] = min(v[d], tile_mm[6 * (size_t)t + d]);
+            w[d] = max(w[d], tile_mm[6 * (size_t)t + 3 + d]);
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        v[d] = __reduce_min_sync(0xffffffffu, v[d]);
+        w[d] = __reduce_max_sync(0xffffffffu, w[d]);
+    }
+    if (lane == 0) {
+        for (int d = 0; d < 3; ++d) {
+            sp[s].mn[d] = v[d];
+            sp[s].mx[d] = w[d];
         }
     }
 }
@@ -689,9 +725,12 @@ static int kd_tiles(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, 
         uint32_t cap = std::max<uint32_t>(total + 1, kd->tile_cap * 2);
         if (kd->tile_seg) kd_release(ctx, kd, kd->tile_seg);
         if (kd->tile_cnt) kd_release(ctx, kd, kd->tile_cnt);
+        if (kd->tile_mm) kd_release(ctx, kd, kd->tile_mm);
         kd->tile_seg = kd->tile_cnt = nullptr;
+        kd->tile_mm = nullptr;
         int rc = kd_alloc(ctx, (void**)&kd->tile_seg, (size_t)cap * 4, kd);
         if (!rc) rc = kd_alloc(ctx, (void**)&kd->tile_cnt, (size_t)(cap + 1) * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->tile_mm, (size_t)cap * 24, kd);
         if (rc) return rc;
         kd->tile_cap = cap;
     }
@@ -821,9 +860,13 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
         kd_minmax_init_kernel<<<(S + 127) / 128, 128, 0, st>>>(kd->split, S);
         rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
         if (rc) return rc;
-        if (ntiles)
+        if (ntiles) {
             kd_minmax_kernel<<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->rx, kd->ry,
-                                                         kd->rz, kd->split);
+                                                         kd->rz, kd->tile_mm);
+            kd_seg_minmax_kernel<<<(S * 32 + 255) / 256, 256, 0, st>>>(S, kd->nt, kd->tile_mm,
+                                                                      kd->split);
+            NBG_LAUNCHED(1);
+        }
         kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, tf);
         NBG_LAUNCHED(2 + (ntiles ? 1 : 0));
         rc = kd_pass<1>(ctx, kd, segs, S, tf, st);

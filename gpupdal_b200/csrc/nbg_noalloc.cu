@@ -31,20 +31,24 @@ namespace nbg {
 namespace {
 
 constexpr uint64_t kMaxPoints = NBG_NOALLOC_MAX_POINTS;
-constexpr uint64_t kCellsCap = 2 * kMaxPoints + 1024;
-constexpr size_t kScanReserve = 1u << 20;  // CUB scan temporary storage
+constexpr uint64_t kColsCap = 2 * kMaxPoints + 1024;
+constexpr uint64_t kTableCap = 4 * kMaxPoints + 1024;
+constexpr size_t kTmpReserve = 1u << 20;  // CUB scan storage
 constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 constexpr size_t kOffBbox = 0;
 constexpr size_t kOffGp = kOffBbox + 256;
 constexpr size_t kOffCounters = kOffGp + align256(sizeof(GridParams));
-constexpr size_t kOffKeys = kOffCounters + 256;
-constexpr size_t kOffStart = kOffKeys + align256(kMaxPoints * 4);
-constexpr size_t kOffCursor = kOffStart + align256((kCellsCap + 1) * 4);
-constexpr size_t kOffSorted = kOffCursor + align256((kCellsCap + 1) * 4);
-constexpr size_t kOffScan = kOffSorted + align256(kMaxPoints * 16);
-constexpr size_t kArenaBytes = kOffScan + kScanReserve;
+constexpr size_t kOffTable = kOffCounters + 256;
+constexpr size_t kOffColinfo = kOffTable + 256;
+constexpr size_t kOffExt = kOffColinfo + align256(kColsCap * 16);
+constexpr size_t kOffKeys = kOffExt + align256((kColsCap + 1) * 4);
+constexpr size_t kOffCstart = kOffKeys + align256(kMaxPoints * 4);
+constexpr size_t kOffCursor = kOffCstart + align256(kTableCap * 4);
+constexpr size_t kOffSorted = kOffCursor + align256(kTableCap * 4);
+constexpr size_t kOffTmp = kOffSorted + align256(kMaxPoints * 16);
+constexpr size_t kArenaBytes = kOffTmp + kTmpReserve;
 
-// All working memory of nbg_stage_noalloc (about 19.4 MB); held by every
+// All working memory of nbg_stage_noalloc (about 49 MB); held by every
 // device that loads this library until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_arena[kArenaBytes];
 
@@ -135,15 +139,20 @@ extern "C" int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32
     }
     t.bbox = (int32_t*)(arena + kOffBbox);
     t.gp = (GridParams*)(arena + kOffGp);
+    t.table_dev = (uint32_t*)(arena + kOffTable);
+    t.colinfo = (int4*)(arena + kOffColinfo);
+    t.ext = (uint32_t*)(arena + kOffExt);
     t.keys = (uint32_t*)(arena + kOffKeys);
-    t.cell_start = (uint32_t*)(arena + kOffStart);
+    t.cstart = (uint32_t*)(arena + kOffCstart);
     t.cursor = (uint32_t*)(arena + kOffCursor);
     t.sorted = (float4*)(arena + kOffSorted);
-    t.ncells_cap = 2 * n + 1024;
-    t.scan_tmp = arena + kOffScan;
-    t.scan_tmp_bytes = scan_temp_bytes(t.ncells_cap + 1);
-    if (t.scan_tmp_bytes > kScanReserve)
-        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "scan storage exceeds its reserve");
+    t.cols_cap = 2 * n + 1024;
+    t.table_cap = kTableCap;
+    t.fixed_storage = true;
+    t.grid_tmp = arena + kOffTmp;
+    t.grid_tmp_bytes = kTmpReserve;
+    if (grid_temp_bytes(std::max<uint64_t>(kTableCap, t.cols_cap + 1)) > kTmpReserve)
+        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "grid storage exceeds its reserve");
     uint32_t* counters = (uint32_t*)(arena + kOffCounters);
     const int K = (int)(n < (uint64_t)opts->knn + 1 ? n : (uint64_t)opts->knn + 1);
 
@@ -151,7 +160,7 @@ extern "C" int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32
     if (cudaMemsetAsync(counters, 0, 256, stream) != cudaSuccess)
         return set_msg(err_msg, err_len, NBG_ERR_CUDA, "counter reset failed");
     int rc = build_grid(&ctx, &t, K, stream);
-    if (rc) return set_msg(err_msg, err_len, rc, "grid build failed");
+    if (rc) return set_msg(err_msg, err_len, rc, ctx.err.empty() ? "grid build failed" : ctx.err.c_str());
     GridParams hg;
     cudaError_t e = cudaMemcpyAsync(&hg, t.gp, sizeof(GridParams), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -177,6 +186,7 @@ extern "C" int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32
     d.base = (char*)out->base;
     d.point_stride = out->point_stride;
     for (int k = 0; k < NBG_MAX_DIMS; ++k) d.offset[k] = out->offset[k];
+    g.sign_exact = opts->kind == NBG_STAGE_NORMAL && !opts->always_up && !opts->has_viewpoint;
     QueryLaunch ql;
     ql.tile = &t;
     ql.K = K;

@@ -44,35 +44,62 @@ struct QueryCell {
     int cx, cy, cz;     // cell coords
 };
 
-// Calls f(float4) for every point of the cells at Chebyshev distance R.
+// Calls f(float4) for the points of cells zl..zh of a column (inclusive).
 template <class F>
-__device__ __forceinline__ void scan_shell(const float4* __restrict__ sorted,
-                                           const uint32_t* __restrict__ cs, const GridParams& g,
+__device__ __forceinline__ void scan_cells(const GridView& gv, const int4 ci, int zl, int zh, F& f) {
+    zl = max(zl, ci.y);
+    zh = min(zh, ci.z);
+    if (zl > zh) return;
+    const uint32_t e0 = (uint32_t)ci.x + (uint32_t)(zl - ci.y);
+    const uint32_t e1 = (uint32_t)ci.x + (uint32_t)(zh - ci.y) + 1;
+    const uint32_t pe = __ldg(&gv.cstart[e1]);
+    for (uint32_t j = __ldg(&gv.cstart[e0]); j < pe; ++j) f(__ldg(&gv.sorted[j]));
+}
+
+// Distance (raw units) from coordinate q to the cell slab [k*c, (k+1)*c - 1].
+__device__ __forceinline__ int slab_gap(int q, int k, int c) {
+    const int lo = k * c, hi = lo + c - 1;
+    return q < lo ? lo - q : (q > hi ? q - hi : 0);
+}
+
+// Calls f(float4) for every point of the cells at Chebyshev distance R that
+// can hold a point within the functor's current squared-distance limit
+// f.limit(): boundary columns contribute their cells with z in [cz-R, cz+R],
+// interior columns only the two cells at z = cz-R and z = cz+R; a column whose
+// horizontal gap already exceeds the limit, and cells beyond the ball's
+// z-reach, are skipped (they cannot hold a point at or below the limit).
+template <class F>
+__device__ __forceinline__ void scan_shell(const GridView& gv, const GridParams& g,
                                            const QueryCell& qc, int R, F& f) {
-    for (int dz = -R; dz <= R; ++dz) {
-        const int z = qc.cz + dz;
-        if (z < 0 || z >= g.gz) continue;
-        const int adz = dz < 0 ? -dz : dz;
-        for (int dy = -R; dy <= R; ++dy) {
-            const int y = qc.cy + dy;
-            if (y < 0 || y >= g.gy) continue;
-            const int ady = dy < 0 ? -dy : dy;
-            const uint32_t rowbase = ((uint32_t)z * (uint32_t)g.gy + (uint32_t)y) * (uint32_t)g.gx;
-            if (max(adz, ady) == R) {
-                const int x0 = max(qc.cx - R, 0), x1 = min(qc.cx + R, g.gx - 1);
-                const uint32_t b = __ldg(&cs[rowbase + x0]), e = __ldg(&cs[rowbase + x1 + 1]);
-                for (uint32_t j = b; j < e; ++j) f(__ldg(&sorted[j]));
+    const int zlo = qc.cz - R, zhi = qc.cz + R;
+    const int c = g.cell;
+    for (int dy = -R; dy <= R; ++dy) {
+        const int y = qc.cy + dy;
+        if (y < 0 || y >= g.gy) continue;
+        const int ady = dy < 0 ? -dy : dy;
+        const int gy_ = slab_gap(qc.qy, y, c);
+        for (int dx = -R; dx <= R; ++dx) {
+            const int x = qc.cx + dx;
+            if (x < 0 || x >= g.gx) continue;
+            const int gx_ = slab_gap(qc.qx, x, c);
+            const long long h2 = (long long)gx_ * gx_ + (long long)gy_ * gy_;
+            const unsigned long long lim = f.limit();
+            if ((unsigned long long)h2 > lim) continue;
+            const int4 ci = __ldg(&gv.colinfo[(uint32_t)y * (uint32_t)g.gx + (uint32_t)x]);
+            if (ci.z < ci.y) continue;
+            // z-cells within reach of the ball of squared radius lim
+            int zr0 = zlo, zr1 = zhi;
+            if (lim < (1ull << 46)) {
+                const float s = sqrtf((float)(lim - (unsigned long long)h2)) + 1.0f;
+                zr0 = max(zr0, (int)floorf(((float)qc.qz - s) / (float)c));
+                zr1 = min(zr1, (int)floorf(((float)qc.qz + s) / (float)c));
+            }
+            const int adx = dx < 0 ? -dx : dx;
+            if (max(ady, adx) == R) {
+                scan_cells(gv, ci, zr0, zr1, f);
             } else {
-                if (qc.cx - R >= 0) {
-                    const uint32_t b = __ldg(&cs[rowbase + qc.cx - R]),
-                                   e = __ldg(&cs[rowbase + qc.cx - R + 1]);
-                    for (uint32_t j = b; j < e; ++j) f(__ldg(&sorted[j]));
-                }
-                if (qc.cx + R < g.gx) {
-                    const uint32_t b = __ldg(&cs[rowbase + qc.cx + R]),
-                                   e = __ldg(&cs[rowbase + qc.cx + R + 1]);
-                    for (uint32_t j = b; j < e; ++j) f(__ldg(&sorted[j]));
-                }
+                if (zlo >= zr0 && zlo <= zr1) scan_cells(gv, ci, zlo, zlo, f);
+                if (zhi >= zr0 && zhi <= zr1) scan_cells(gv, ci, zhi, zhi, f);
             }
         }
     }
@@ -126,6 +153,12 @@ template <int KS>
 struct Pass1Fn {
     float qx, qy, qz;
     TopK<KS>* top;
+    // squared raw distance of the current (K+1)-th candidate: points beyond
+    // it can neither enter the set nor tie with its K-th element
+    __device__ __forceinline__ unsigned long long limit() const {
+        const uint32_t k = top->k[KS - 1];
+        return k < KEY_EXACT_END ? (unsigned long long)(k - KEY_BASE) : ~0ull;
+    }
     __device__ __forceinline__ void operator()(const float4 p) {
         const uint32_t key = dist_key(p.x - qx, p.y - qy, p.z - qz);
         if (key < top->k[KS - 1]) top->insert(key);
@@ -136,6 +169,9 @@ struct Pass2Fn {
     float qx, qy, qz;
     uint32_t kk;
     int s1x, s1y, s1z, sxx, syx, syy, szx, szy, szz, cnt;
+    __device__ __forceinline__ unsigned long long limit() const {
+        return (unsigned long long)(kk - KEY_BASE);
+    }
     __device__ __forceinline__ void operator()(const float4 p) {
         const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
         const uint32_t key = dist_key(dx, dy, dz);
@@ -160,6 +196,9 @@ struct CollectFn {
     uint32_t kk;
     uint32_t* row;
     int cnt, cap;
+    __device__ __forceinline__ unsigned long long limit() const {
+        return (unsigned long long)(kk - KEY_BASE);
+    }
     __device__ __forceinline__ void operator()(const float4 p) {
         const uint32_t key = dist_key(p.x - qx, p.y - qy, p.z - qz);
         if (key <= kk) {
@@ -170,8 +209,7 @@ struct CollectFn {
 };
 
 struct QueryArgs {
-    const float4* sorted;
-    const uint32_t* cs;
+    GridView gv;
     const GridParams* gp;
     uint64_t n;
     int K;
@@ -196,8 +234,9 @@ __device__ __forceinline__ bool select_kth(const QueryArgs& a, const GridParams&
     top.init(off);
     Pass1Fn<KS> f1{q.x, q.y, q.z, &top};
     bool complete = false;
-    for (R = 0; R <= a.rmax; ++R) {
-        scan_shell(a.sorted, a.cs, g, qc, R, f1);
+    const int rmax = a.rmax;
+    for (R = 0; R <= rmax; ++R) {
+        scan_shell(a.gv, g, qc, R, f1);
         const uint32_t kth = top.at(off + K - 1);
         const unsigned long long gap2 = outside_gap2(g, qc, R);
         if (gap2 == ~0ull) {
@@ -209,7 +248,7 @@ __device__ __forceinline__ bool select_kth(const QueryArgs& a, const GridParams&
             break;
         }
     }
-    if (R > a.rmax) R = a.rmax;
+    if (R > rmax) R = rmax;
     kk = top.at(off + K - 1);
     const uint32_t kk1 = top.at(off + K);
     if (!complete || kk >= KEY_EXACT_END) {
@@ -228,7 +267,7 @@ __global__ void __launch_bounds__(128) knn_fused_kernel(const QueryArgs a) {
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const GridParams g = *a.gp;
-    const float4 q = __ldg(&a.sorted[i]);
+    const float4 q = __ldg(&a.gv.sorted[i]);
     const uint32_t id = __float_as_uint(q.w);
     QueryCell qc;
     qc.qx = __float2int_rz(q.x);
@@ -245,7 +284,7 @@ __global__ void __launch_bounds__(128) knn_fused_kernel(const QueryArgs a) {
         return;
     }
     Pass2Fn f2{q.x, q.y, q.z, kk, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int r = 0; r <= R; ++r) scan_shell(a.sorted, a.cs, g, qc, r, f2);
+    for (int r = 0; r <= R; ++r) scan_shell(a.gv, g, qc, r, f2);
     if (f2.cnt != a.K) {  // cannot happen for a complete, tie-free row; stay exact
         const uint32_t slot = atomicAdd(&a.counters[0], 1u);
         a.exact_rows[slot] = id;
@@ -268,7 +307,7 @@ __global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const GridParams g = *a.gp;
-    const float4 q = __ldg(&a.sorted[i]);
+    const float4 q = __ldg(&a.gv.sorted[i]);
     const uint32_t id = __float_as_uint(q.w);
     QueryCell qc;
     qc.qx = __float2int_rz(q.x);
@@ -286,7 +325,7 @@ __global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
     }
     uint32_t* row = a.ids_out + (uint64_t)id * a.K;
     CollectFn f{q.x, q.y, q.z, kk, row, 0, a.K};
-    for (int r = 0; r <= R; ++r) scan_shell(a.sorted, a.cs, g, qc, r, f);
+    for (int r = 0; r <= R; ++r) scan_shell(a.gv, g, qc, r, f);
     // ascending ids (insertion sort of at most 66 entries)
     for (int s = 1; s < a.K; ++s) {
         uint32_t v = row[s];
@@ -349,11 +388,18 @@ struct KnnLauncher {
     }
 };
 
+GridView grid_view(const Tile* t) {
+    GridView v;
+    v.sorted = t->sorted;
+    v.colinfo = t->colinfo;
+    v.cstart = t->cstart;
+    return v;
+}
+
 int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
     (void)ctx;
     LaunchArgs la;
-    la.q.sorted = ql.tile->sorted;
-    la.q.cs = ql.tile->cell_start;
+    la.q.gv = grid_view(ql.tile);
     la.q.gp = ql.tile->gp;
     la.q.n = ql.tile->n;
     la.q.K = ql.K;
@@ -373,8 +419,7 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
                          uint32_t* exact_rows, uint32_t* counters, cudaStream_t stream) {
     (void)ctx;
     LaunchArgs la{};
-    la.q.sorted = t->sorted;
-    la.q.cs = t->cell_start;
+    la.q.gv = grid_view(t);
     la.q.gp = t->gp;
     la.q.n = t->n;
     la.q.K = K;

@@ -23,6 +23,26 @@ def _dptr(a):
     return ctypes.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
 
 
+def record_columns(base_ptr, stages, record_bytes, on_device):
+    """abi.Columns for `stages` sharing one record per point: the stages'
+    dims are laid out one after another from offset 0."""
+    cols, off = [], 0
+    for st in stages:
+        c = abi.Columns()
+        c.base = base_ptr
+        c.point_stride = record_bytes
+        dims = abi.stage_dims(st)
+        c.ndims = len(dims)
+        c.on_device = on_device
+        for d in range(len(dims)):
+            c.offset[d] = off
+            off += 8
+        cols.append(c)
+    if off > record_bytes:
+        raise ValueError("record too small for the stages' dims")
+    return cols
+
+
 class Context:
     def __init__(self, device: int = 0, hbm_budget: int = 0):
         self.lib = abi.load_library()
@@ -108,6 +128,32 @@ class Context:
             ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code)
         return [o[: len(abi.stage_dims(s))] for o, s in zip(outs, stages)], ex, stats
 
+    def run_columns(self, tile, stages, columns, optimal_knn=None, optimal_radius=None,
+                    aux_on_device=False, exception_capacity=1 << 16, stream=None):
+        """nbg_run with caller-built abi.Columns (e.g. one record per point
+        shared by several stages).  Returns (exceptions, stats)."""
+        ns = len(stages)
+        opts = (abi.StageOpts * max(ns, 1))(*stages)
+        cols = (abi.Columns * max(ns, 1))(*columns)
+        cap = exception_capacity
+        exc = self._exc_buf.get(cap)
+        if exc is None:
+            exc = (abi.RowException * cap)()
+            self._exc_buf = {cap: exc}
+        nexc = ctypes.c_uint32(0)
+        stats = abi.RunStats()
+        kp = None if optimal_knn is None else _dptr(optimal_knn)
+        rp = None if optimal_radius is None else _dptr(optimal_radius)
+        rc = self.lib.nbg_run(self.h, tile.h, opts, ns, cols, kp, rp, int(aux_on_device), exc,
+                              cap, ctypes.byref(nexc), ctypes.byref(stats),
+                              ctypes.c_void_p(stream) if stream else None)
+        self._check(rc)
+        m = min(nexc.value, cap)
+        ex = np.zeros(m, dtype=[("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8)])
+        for j in range(m):
+            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code)
+        return ex, stats
+
     def kd_export(self, tile):
         """The device KD replica: (vind, nodes dict) for parity tests."""
         n = tile.n
@@ -154,6 +200,10 @@ class Tile:
                                      ctypes.byref(h))
         ctx._check(rc)
         self.h = h
+
+    def tune(self, cell_factor=4.0, fixed_cell=0):
+        self.ctx._check(self.ctx.lib.nbg_tile_tune(self.ctx.h, self.h, float(cell_factor),
+                                                   int(fixed_cell)))
 
     def free(self):
         if getattr(self, "h", None) and self.ctx.h:

@@ -160,6 +160,13 @@ int nbg_tile_upload(nbg_context* ctx, const int32_t* x, const int32_t* y,
                     const double offset[3], int32_t on_device, void* stream,
                     nbg_tile** tile);
 int nbg_tile_free(nbg_context* ctx, nbg_tile* tile);
+
+/* Grid tuning of a tile: the cell edge is ceil(cell_factor * r_k), r_k the
+ * radius holding k points at the tile's planar density (default factor 4);
+ * fixed_cell > 0 forces an edge in raw units.  Takes effect at the next run
+ * (the grid is rebuilt).  Used by the autotuner; no counterpart in the
+ * reference (whose KD tree has no tunable). */
+int nbg_tile_tune(nbg_context* ctx, nbg_tile* tile, float cell_factor, int32_t fixed_cell);
 uint64_t nbg_tile_size(const nbg_tile* tile);
 
 /* Run stages over a resident tile.  Stages sharing knn share one fused
@@ -192,11 +199,12 @@ int nbg_neighbor_sets(nbg_context* ctx, nbg_tile* tile, int32_t knn,
  * x/y/z, outputs (on_device must be 1), `unresolved` (capacity n),
  * `exceptions`, `optimal_knn`/`optimal_radius` are device memory owned by the
  * caller; n_unresolved / n_exceptions are host pointers.  All working memory
- * (uniform grid, scan storage, counters: about 19.4 MB) is one fixed device
+ * (grid, scan storage, counters: about 49 MB) is one fixed device
  * array inside this library, present on every GPU that loads it until the
- * process exits; nothing is allocated or freed.  Larger tiles are rejected
- * with NBG_ERR_UNSUPPORTED and a message in err_msg (caller buffer, may be
- * null).
+ * process exits; nothing is allocated or freed.  Larger tiles, and tiles
+ * whose columns span more cells than the fixed table holds (4 per point),
+ * are rejected with NBG_ERR_UNSUPPORTED and a message in err_msg (caller
+ * buffer, may be null).
  *
  * Rows whose neighbour set depends on the reference's tie order (or whose
  * ring search did not finish) need the exact KD replica, whose memory grows

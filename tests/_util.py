@@ -11,7 +11,13 @@ Tolerances (the bar of the parity tests):
     determined sign (the flip test n_z < 0 sees rounding residue); such rows
     are compared up to sign.  sign_eps is 1e-9 against the FP64 oracle and
     1e-6 against the reference's own outputs, whose float narrowing moves
-    NormalZ by up to ~1e-7
+    NormalZ by up to ~1e-7.  With always_up=false the sign is the Eigen
+    chain's; rows whose exact covariance has a zero off-diagonal entry
+    (lattice symmetry) take a branch decided by rounding residue and are
+    compared up to sign; the sign itself is checked against the reference's
+    own outputs (the FP64 oracle's sign is only an alignment).  Rows whose
+    chain sign flips under a 1e-7 relative perturbation of the exact covariance
+    are compared up to sign as well (sign_unstable_rows)
   * curvature and ratio features in [0, 1]: |d| <= 1e-5
   * EigenvalueSum, Omnivariance, Eigenentropy, Density: relative 1e-5 of
     max(|value|, lambda scale)
@@ -59,8 +65,56 @@ def eigen_scale(eig_f64):
     return np.maximum(np.abs(eig_f64).max(axis=0), 1e-300)
 
 
+def symmetric_rows(x, y, z, nbr):
+    """Rows whose exact (integer) neighbourhood covariance has an off-diagonal
+    entry equal to zero: lattice symmetries, where an eigensolver's sign
+    choice is decided by rounding residue."""
+    P = np.stack([np.asarray(v, np.int64) for v in (x, y, z)], 1)
+    d = P[nbr.astype(np.int64)] - P[:, None, :]
+    n = nbr.shape[1]
+    S1 = d.sum(1)
+    S2 = np.einsum("rki,rkj->rij", d, d)
+    M = n * S2 - S1[:, :, None] * S1[:, None, :]
+    return (M[:, 1, 0] == 0) | (M[:, 2, 0] == 0) | (M[:, 2, 1] == 0)
+
+
+def sign_unstable_rows(port, x, y, z, nbr, scale=0.01, trials=8, rel=1e-7, seed=0):
+    """Rows whose Eigen-chain eigenvector sign flips when the exact covariance
+    is perturbed at the level of the reference's float narrowing (relative
+    `rel` of its largest entry): exact lattice ties (equal diagonal entries,
+    rational eigenvalues) send the chain down a branch that rounding residue
+    decides, so the reference's sign there is not a property of the data."""
+    P = np.stack([np.asarray(v, np.int64) for v in (x, y, z)], 1)
+    d = P[nbr.astype(np.int64)] - P[:, None, :]
+    n = nbr.shape[1]
+    S1 = d.sum(1)
+    S2 = np.einsum("rki,rkj->rij", d, d)
+    C = (n * S2 - S1[:, :, None] * S1[:, None, :]) * (scale * scale) / (n * (n - 1))
+    rng = np.random.default_rng(seed)
+    out = np.zeros(len(P), bool)
+    for r in range(len(P)):
+        v0 = port.eigen_chain(C[r])[2][:, 0]
+        sc = np.abs(C[r]).max()
+        for _ in range(trials):
+            E = rng.standard_normal((3, 3)) * rel * sc
+            if np.dot(port.eigen_chain(C[r] + (E + E.T) / 2)[2][:, 0], v0) < 0:
+                out[r] = True
+                break
+    return out
+
+
+def viewpoint_tangent_rows(opts, X, Y, Z, want, eps=1e-6):
+    """Rows whose viewpoint lies in the tangent plane ((vp - p) . n == 0 up to
+    `eps` relative): the reference's orientation test leaves the eigensolver's
+    sign there, which rounding residue decides on lattice inputs."""
+    vp = np.asarray(list(opts.viewpoint), np.float64)
+    d = np.stack([vp[0] - X, vp[1] - Y, vp[2] - Z])
+    dot = (d * want[:3]).sum(0)
+    return np.abs(dot) <= eps * np.abs(d).sum(0)
+
+
 def compare_stage(opts, got, want, want_status, got_status, lam=None, label="", gap_min=1e-4,
-                  tol=TOL, sign_eps=1e-9):
+                  tol=TOL, sign_eps=1e-9, sign_free=None):
     """Asserts `got` (ndims, n) matches `want` within the stated bars.
 
     `lam` is the (3, n) ascending eigenvalue array of the accuracy oracle
@@ -82,8 +136,14 @@ def compare_stage(opts, got, want, want_status, got_status, lam=None, label="", 
     else:
         lscale = lmax
     vec_ok = gap >= gap_min
-    if opts.kind == abi.STAGE_NORMAL and opts.always_up and not opts.has_viewpoint:
-        flat = np.abs(want[2]) < sign_eps
+    if opts.kind == abi.STAGE_NORMAL:
+        flat = np.zeros(n, bool)
+        if opts.always_up and not opts.has_viewpoint:
+            flat = np.abs(want[2]) < sign_eps
+        if sign_free is True:
+            flat = np.ones(n, bool)
+        elif sign_free is not None:
+            flat = flat | sign_free
         if flat.any():
             got = got.copy()
             flip = flat & (np.abs(got[:3] - want[:3]).sum(0) > np.abs(got[:3] + want[:3]).sum(0))
@@ -110,8 +170,11 @@ def compare_stage(opts, got, want, want_status, got_status, lam=None, label="", 
             bar = tol
         err = np.abs(g - w)
         bad = fin & ~(err <= bar)
-        assert not bad.any(), (f"{label}:{name} {bad.sum()} rows over the bar, max err "
-                               f"{err[fin].max():.3e}")
+        if bad.any():
+            rows = np.flatnonzero(ok)[bad][:4]
+            raise AssertionError(f"{label}:{name} {bad.sum()} rows over the bar, max err "
+                                 f"{err[fin].max():.3e}; first rows {rows.tolist()} got "
+                                 f"{g[bad][:4].tolist()} want {w[bad][:4].tolist()}")
 
 
 def status_from_exceptions(n, ex, stage=0):

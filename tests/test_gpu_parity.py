@@ -55,11 +55,22 @@ def test_stages_match_reference_golden(nbg, port, name):
         # accuracy oracle: same neighbour sets, FP64 without narrowing
         want64, st64 = port.tree(X, Y, Z).run_stage(o, mode=1, optimal_knn=kopt,
                                                      optimal_radius=ropt)
+        want_ref = g[sname + "_out"]
+        free64 = free_ref = None
+        if o.kind == abi.STAGE_NORMAL and o.has_viewpoint:
+            free64 = U.viewpoint_tangent_rows(o, X, Y, Z, want64)
+            free_ref = U.viewpoint_tangent_rows(o, X, Y, Z, want_ref)
+        elif o.kind == abi.STAGE_NORMAL and not o.always_up and f"nbr_k{o.knn}" in g:
+            nb = g[f"nbr_k{o.knn}"]
+            free64 = True
+            free_ref = (U.symmetric_rows(g["x"], g["y"], g["z"], nb) |
+                        U.sign_unstable_rows(port, g["x"], g["y"], g["z"], nb))
         U.compare_stage(o, outs[0], want64, g[sname + "_status"], got_status, lam=lam,
-                        label=f"{name}/{sname} vs f64")
+                        label=f"{name}/{sname} vs f64", sign_free=free64)
         # the reference's own outputs, on rows its float narrowing cannot blur
-        U.compare_stage(o, outs[0], g[sname + "_out"], g[sname + "_status"], got_status, lam=lam,
-                        label=f"{name}/{sname} vs reference", gap_min=1e-2, sign_eps=1e-6)
+        U.compare_stage(o, outs[0], want_ref, g[sname + "_status"], got_status, lam=lam,
+                        label=f"{name}/{sname} vs reference", gap_min=1e-2, sign_eps=1e-6,
+                        sign_free=free_ref)
 
 
 def test_kd_replica_matches_reference_tree(nbg, port):
