@@ -107,6 +107,7 @@ class RunStats(ctypes.Structure):
         ("tree_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
         ("kernel_launches", ctypes.c_uint64),
+        ("replay_rows", ctypes.c_uint64),
     ]
 
 

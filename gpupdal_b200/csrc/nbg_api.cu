@@ -95,6 +95,14 @@ static int dev_alloc(Context* ctx, void** p, size_t bytes, uint64_t* account) {
 static void dev_free(Context* ctx, void* p, size_t bytes) { ctx_free(ctx, p, bytes); }
 
 static int ensure_scratch(Context* ctx, uint64_t n, uint64_t ex_cap) {
+    if (ctx->tie_cap < n) {
+        if (ctx->ties) dev_free(ctx, ctx->ties, ctx->tie_cap * sizeof(uint2));
+        ctx->ties = nullptr;
+        ctx->tie_cap = 0;
+        int rc = dev_alloc(ctx, (void**)&ctx->ties, std::max<uint64_t>(n, 1024) * sizeof(uint2), nullptr);
+        if (rc) return rc;
+        ctx->tie_cap = std::max<uint64_t>(n, 1024);
+    }
     if (ctx->exact_cap < n) {
         if (ctx->exact_rows) dev_free(ctx, ctx->exact_rows, ctx->exact_cap * 4);
         ctx->exact_rows = nullptr;
@@ -230,6 +238,7 @@ int nbg_destroy(nbg_context* h) {
     Context* ctx = &h->c;
     cudaSetDevice(ctx->device);
     dev_free(ctx, ctx->exact_rows, ctx->exact_cap * 4);
+    if (ctx->ties) dev_free(ctx, ctx->ties, ctx->tie_cap * sizeof(uint2));
     dev_free(ctx, ctx->ex_rows, ctx->ex_cap * sizeof(nbg_row_exception));
     dev_free(ctx, ctx->counters, 64 * sizeof(uint32_t));
     ctx_trim(ctx);
@@ -511,7 +520,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
 
     cudaEventRecord(ctx->ev[0], stream);
     float grid_ms = 0, query_ms = 0, tree_ms = 0;
-    uint64_t tie_rows = 0, deferred_rows = 0;
+    uint64_t tie_rows = 0, deferred_rows = 0, replay_rows = 0;
     ExceptionSink sink{ctx->ex_rows, ctx->counters + 3, (uint32_t)std::max<uint32_t>(exception_capacity, 1)};
     if (cudaMemsetAsync(ctx->counters, 0, 64 * sizeof(uint32_t), stream)) { cleanup(); return NBG_ERR_CUDA; }
     for (auto& gr : groups) {
@@ -542,7 +551,12 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             for (int k = 0; k < NBG_MAX_DIMS; ++k) d.offset[k] = dcols[s].offset[k];
             if (o.kind == NBG_STAGE_NORMAL && !o.always_up && !o.has_viewpoint) g.sign_exact = 1;
         }
-        if (cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(uint32_t), stream)) { cleanup(); return NBG_ERR_CUDA; }
+        g.resolve_count = ctx->counters + 5;
+        if (cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(uint32_t), stream) ||
+            cudaMemsetAsync(ctx->counters + 4, 0, sizeof(uint32_t), stream)) {
+            cleanup();
+            return NBG_ERR_CUDA;
+        }
         QueryLaunch ql;
         ql.tile = t;
         ql.K = K;
@@ -551,12 +565,14 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         ql.ex = sink;
         ql.exact_rows = ctx->exact_rows;
         ql.counters = ctx->counters;
+        ql.ties = ctx->ties;
+        ql.tie_cap = (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX);
         rc = launch_query(ctx, ql, stream);
         if (rc) { cleanup(); return fail(ctx, rc, std::string("query launch failed: ") +
                                                  cudaGetErrorString(cudaGetLastError())); }
         cudaEventRecord(ctx->ev[3], stream);
-        uint32_t cnt[3] = {0, 0, 0};
-        cudaError_t e = cudaMemcpyAsync(cnt, ctx->counters, 3 * sizeof(uint32_t),
+        uint32_t cnt[5] = {0, 0, 0, 0, 0};
+        cudaError_t e = cudaMemcpyAsync(cnt, ctx->counters, 5 * sizeof(uint32_t),
                                         cudaMemcpyDeviceToHost, stream);
         if (!e) e = cudaStreamSynchronize(stream);
         if (e) { cleanup(); return cuda_fail(ctx, e, "query kernel"); }
@@ -567,9 +583,31 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         grid_ms += ms;
         cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
         query_ms += ms;
-        if (cnt[0]) {
+        const uint32_t nties = (uint32_t)std::min<uint64_t>(cnt[4], ctx->tie_cap);
+        if (cnt[0] || nties) {
             cudaEventRecord(ctx->ev[4], stream);
             rc = kd_ensure(ctx, t, stream);
+            if (!rc && nties) {
+                TieLaunch tl;
+                tl.tile = t;
+                tl.K = K;
+                tl.grp = g;
+                tl.ex = sink;
+                tl.ties = ctx->ties;
+                tl.nties = nties;
+                tl.kd = kd_order(t);
+                tl.exact_rows = ctx->exact_rows;
+                tl.counters = ctx->counters;
+                tl.ids_out = nullptr;
+                rc = launch_ties(ctx, tl, stream);
+                if (!rc) {
+                    e = cudaMemcpyAsync(cnt, ctx->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                        stream);
+                    if (!e) e = cudaStreamSynchronize(stream);
+                    if (e) { cleanup(); return cuda_fail(ctx, e, "tie-order resolver"); }
+                }
+            }
+            replay_rows += cnt[0];
             if (!rc) rc = kd_run_rows(ctx, t, K, g, sink, ctx->exact_rows, cnt[0], stream);
             if (rc) { cleanup(); return rc; }
             cudaEventRecord(ctx->ev[5], stream);
@@ -600,8 +638,9 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             if (e) { cleanup(); return cuda_fail(ctx, e, "output copy"); }
         }
     }
-    uint32_t nex = 0;
+    uint32_t nex = 0, nresolve = 0;
     cudaError_t e = cudaMemcpyAsync(&nex, ctx->counters + 3, 4, cudaMemcpyDeviceToHost, stream);
+    if (!e) e = cudaMemcpyAsync(&nresolve, ctx->counters + 5, 4, cudaMemcpyDeviceToHost, stream);
     if (!e) e = cudaStreamSynchronize(stream);
     if (e) { cleanup(); return cuda_fail(ctx, e, "exception count"); }
     const uint32_t ncopy = std::min(nex, exception_capacity);
@@ -618,6 +657,8 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         stats->points = n * groups.size();
         stats->tie_rows = tie_rows;
         stats->deferred_rows = deferred_rows;
+        stats->resolved_rows = nresolve;
+        stats->replay_rows = replay_rows;
         stats->grid_ms = grid_ms;
         stats->query_ms = query_ms;
         stats->tree_ms = tree_ms;
@@ -656,16 +697,34 @@ extern "C" int nbg_neighbor_sets(nbg_context* h, nbg_tile* th, int32_t knn, uint
         if (rc) return rc;
     }
     cudaMemsetAsync(ctx->counters, 0, 64 * sizeof(uint32_t), stream);
-    rc = launch_neighbor_sets(ctx, t, K, 8, dev_ids, ctx->exact_rows, ctx->counters, stream);
-    uint32_t cnt[3] = {0, 0, 0};
+    rc = launch_neighbor_sets(ctx, t, K, 8, dev_ids, ctx->exact_rows, ctx->counters, ctx->ties,
+                              (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX), stream);
+    uint32_t cnt[5] = {0, 0, 0, 0, 0};
     cudaError_t e = cudaSuccess;
     if (!rc) {
-        e = cudaMemcpyAsync(cnt, ctx->counters, 12, cudaMemcpyDeviceToHost, stream);
+        e = cudaMemcpyAsync(cnt, ctx->counters, 20, cudaMemcpyDeviceToHost, stream);
         if (!e) e = cudaStreamSynchronize(stream);
     }
-    if (!rc && !e && cnt[0]) {
+    const uint32_t nties = (uint32_t)std::min<uint64_t>(cnt[4], ctx->tie_cap);
+    if (!rc && !e && (cnt[0] || nties)) {
         rc = kd_ensure(ctx, t, stream);
-        if (!rc) rc = kd_neighbor_rows(ctx, t, K, ctx->exact_rows, cnt[0], dev_ids, stream);
+        if (!rc && nties) {
+            TieLaunch tl{};
+            tl.tile = t;
+            tl.K = K;
+            tl.ties = ctx->ties;
+            tl.nties = nties;
+            tl.kd = kd_order(t);
+            tl.exact_rows = ctx->exact_rows;
+            tl.counters = ctx->counters;
+            tl.ids_out = dev_ids;
+            rc = launch_ties(ctx, tl, stream);
+            if (!rc) {
+                e = cudaMemcpyAsync(cnt, ctx->counters, 4, cudaMemcpyDeviceToHost, stream);
+                if (!e) e = cudaStreamSynchronize(stream);
+            }
+        }
+        if (!rc && !e) rc = kd_neighbor_rows(ctx, t, K, ctx->exact_rows, cnt[0], dev_ids, stream);
     }
     if (!rc && !e && !ids_on_device) e = cudaMemcpyAsync(ids_out, dev_ids, bytes, cudaMemcpyDeviceToHost, stream);
     if (!e) e = cudaStreamSynchronize(stream);
@@ -674,6 +733,7 @@ extern "C" int nbg_neighbor_sets(nbg_context* h, nbg_tile* th, int32_t knn, uint
         stats->points = n;
         stats->tie_rows = cnt[1];
         stats->deferred_rows = cnt[2];
+        stats->replay_rows = cnt[0];
     }
     if (rc) return rc;
     if (e) return cuda_fail(ctx, e, "neighbour sets");

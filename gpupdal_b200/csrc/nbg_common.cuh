@@ -55,6 +55,20 @@ struct StageGroup {
     StageDev st[NBG_MAX_STAGES];
     const double* optimal_knn;     // device, may be null
     const double* optimal_radius;  // device, may be null
+    uint32_t* resolve_count;       // rows the fast eigensolver handed to the chain (may be null)
+};
+
+// The KD replica's nodes as the tie-order resolver reads them: a child's
+// points are the contiguous range [nb, ne) of the replica's point order, and
+// kpos maps a point id to its position in that order.
+struct KdOrder {
+    const int32_t* c1;
+    const int32_t* c2;
+    const int32_t* feat;
+    const uint32_t* ne;
+    const double* dlo;
+    const double* dhi;
+    const uint32_t* kpos;
 };
 
 // Per-row exception sink.
@@ -411,7 +425,11 @@ __device__ inline void nbg_finish_row(const StageGroup& g, const Transform& tf,
     int ok = 1;
     if (!zero) {
         if (nonfinite) ok = 0;
-        else if (g.sign_exact || !nbg_eigen_fast(C, ev, V)) ok = nbg_eigen_chain(C, ev, V);
+        else if (g.sign_exact) ok = nbg_eigen_chain(C, ev, V);
+        else if (!nbg_eigen_fast(C, ev, V)) {
+            if (g.resolve_count) atomicAdd(g.resolve_count, 1u);
+            ok = nbg_eigen_chain(C, ev, V);
+        }
     }
     double p[3] = {ref_coord(qraw[0], tf.scale[0], tf.offset[0]),
                    ref_coord(qraw[1], tf.scale[1], tf.offset[1]),

@@ -30,7 +30,10 @@ struct Context {
     // per-call scratch (grown on demand)
     uint32_t* exact_rows = nullptr;
     uint64_t exact_cap = 0;
-    uint32_t* counters = nullptr;   // [0] exact rows, [1] tie rows, [2] deferred, [3] exceptions
+    uint2* ties = nullptr;          // tie list of the query kernels
+    uint64_t tie_cap = 0;
+    uint32_t* counters = nullptr;   // [0] exact rows, [1] tie rows, [2] deferred, [3] exceptions,
+                                    // [4] tie list, [5] eigen re-solves
     nbg_row_exception* ex_rows = nullptr;
     uint64_t ex_cap = 0;
     cudaEvent_t ev[8];
@@ -92,8 +95,25 @@ struct QueryLaunch {
     ExceptionSink ex;
     uint32_t* exact_rows;
     uint32_t* counters;
+    uint2* ties = nullptr;  // tie list (null: tie rows join exact_rows)
+    uint32_t tie_cap = 0;
 };
 int launch_query(Context* ctx, const QueryLaunch& q, cudaStream_t stream);
+
+// Tie rows ordered on the KD replica's tree (no search replay).
+struct TieLaunch {
+    const Tile* tile;
+    int K;
+    StageGroup grp;
+    ExceptionSink ex;
+    const uint2* ties;
+    uint32_t nties;
+    KdOrder kd;
+    uint32_t* exact_rows;  // rows the resolver hands to the search replay
+    uint32_t* counters;
+    uint32_t* ids_out;     // neighbour-set export (null in the fused path)
+};
+int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream);
 
 // Exact path: nanoflann replica build (lazy) + DFS for the listed rows.
 int kd_ensure(Context* ctx, Tile* t, cudaStream_t stream);
@@ -101,6 +121,7 @@ int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const Excep
                 const uint32_t* rows, uint32_t nrows, cudaStream_t stream);
 int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
                      uint32_t* ids_out, cudaStream_t stream);
+KdOrder kd_order(const Tile* t);
 void kd_free(Context* ctx, Tile* t);
 uint64_t kd_bytes(uint64_t n);
 int kd_export(Context* ctx, Tile* t, uint32_t* vind, uint32_t* nnodes, int32_t* c1, int32_t* c2,
@@ -109,6 +130,7 @@ int kd_export(Context* ctx, Tile* t, uint32_t* vind, uint32_t* nnodes, int32_t* 
 
 // neighbour-set export of the grid path
 int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
-                         uint32_t* exact_rows, uint32_t* counters, cudaStream_t stream);
+                         uint32_t* exact_rows, uint32_t* counters, uint2* ties, uint32_t tie_cap,
+                         cudaStream_t stream);
 
 }  // namespace nbg

@@ -79,6 +79,7 @@ struct KdReplica {
     int32_t* ry = nullptr;
     int32_t* rz = nullptr;
     uint32_t* rid = nullptr;
+    uint32_t* kpos = nullptr;  // inverse of rid: point id -> position
     uint32_t* mlpos = nullptr;
     uint32_t* mrpos = nullptr;
     // nodes
@@ -469,6 +470,12 @@ __global__ void kd_div_kernel(uint32_t nodes, const int32_t* c1, const int32_t* 
     dhi[node] = ref_coord(bmin[3 * c2[node] + f], tf.scale[f], tf.offset[f]);
 }
 
+__global__ void kd_inverse_kernel(const uint32_t* rid, uint64_t n, uint32_t* kpos) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        kpos[rid[i]] = (uint32_t)i;
+}
+
 // ---------------------------------------------------------------------------
 // search replay
 // ---------------------------------------------------------------------------
@@ -699,7 +706,7 @@ static int kd_grow(Context* ctx, T** p, size_t old_n, size_t new_n, KdReplica* k
     return NBG_OK;
 }
 
-uint64_t kd_bytes(uint64_t n) { return n * 24 + (n / 16 + 1024) * 64; }
+uint64_t kd_bytes(uint64_t n) { return n * 28 + (n / 16 + 1024) * 64; }
 
 void kd_free(Context* ctx, Tile* t) {
     KdReplica* kd = t->kd;
@@ -914,13 +921,32 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
     }
     kd_div_kernel<<<(nn + 127) / 128, 128, 0, st>>>(nn, kd->c1, kd->c2, kd->feat, kd->bmin,
                                                     kd->bmax, tf, kd->dlo, kd->dhi);
-    NBG_LAUNCHED(kd->level_begin.size());
+    if (!kd->kpos) {
+        rc = kd_alloc(ctx, (void**)&kd->kpos, n * 4, kd);
+        if (rc) return rc;
+    }
+    kd_inverse_kernel<<<std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, ctx->sm_count * 8)), 256,
+                        0, st>>>(kd->rid, n, kd->kpos);
+    NBG_LAUNCHED(kd->level_begin.size() + 1);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
         ctx->err = "KD replica extents failed";
         return NBG_ERR_CUDA;
     }
     kd->built = true;
     return NBG_OK;
+}
+
+KdOrder kd_order(const Tile* t) {
+    const KdReplica* kd = t->kd;
+    KdOrder o;
+    o.c1 = kd->c1;
+    o.c2 = kd->c2;
+    o.feat = kd->feat;
+    o.ne = kd->ne;
+    o.dlo = kd->dlo;
+    o.dhi = kd->dhi;
+    o.kpos = kd->kpos;
+    return o;
 }
 
 static KdDev kd_view(const KdReplica* kd) {

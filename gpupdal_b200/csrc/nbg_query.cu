@@ -218,16 +218,35 @@ struct QueryArgs {
     Transform tf;
     ExceptionSink ex;
     uint32_t* exact_rows;
-    uint32_t* counters;  // [0] exact rows, [1] tie rows, [2] incomplete rows
+    uint32_t* counters;  // [0] exact rows, [1] tie rows, [2] incomplete rows, [4] tie list
     uint32_t* ids_out;   // neighbour-set export (null in the fused path)
+    uint2* ties;         // tie list {id, (D_K - 2^23 bias) | R << 24}; null: ties go to exact_rows
+    uint32_t tie_cap;
 };
+
+// A row that cannot finish on the grid: a boundary tie goes to the tie list
+// (its K-th distance and final ring kept for the order resolver), everything
+// else, and ties beyond the list's capacity, to the full search replay.
+__device__ __forceinline__ void defer_row(const QueryArgs& a, uint32_t id, bool tie, uint32_t kk,
+                                          int R) {
+    if (tie && a.ties) {
+        const uint32_t slot = atomicAdd(&a.counters[4], 1u);
+        if (slot < a.tie_cap) {
+            a.ties[slot] = make_uint2(id, (kk - KEY_BASE) | ((uint32_t)R << 24));
+            return;
+        }
+    }
+    const uint32_t slot = atomicAdd(&a.counters[0], 1u);
+    a.exact_rows[slot] = id;
+}
 
 // Pass 1 + completeness/tie decision.  Returns true when the row is exact on
 // the grid path; `R` is the final ring and `kk` the K-th key.
 template <int KS>
 __device__ __forceinline__ bool select_kth(const QueryArgs& a, const GridParams& g,
                                            const QueryCell& qc, const float4 q, int& R,
-                                           uint32_t& kk) {
+                                           uint32_t& kk, bool& tie) {
+    tie = false;
     const int K = a.K;
     const int off = KS - (K + 1);
     TopK<KS> top;
@@ -257,6 +276,7 @@ __device__ __forceinline__ bool select_kth(const QueryArgs& a, const GridParams&
     }
     if (kk1 == kk) {
         atomicAdd(&a.counters[1], 1u);
+        tie = true;
         return false;
     }
     return true;
@@ -278,9 +298,9 @@ __global__ void __launch_bounds__(128) knn_fused_kernel(const QueryArgs a) {
     qc.cz = qc.qz / g.cell;
     int R;
     uint32_t kk;
-    if (!select_kth<KS>(a, g, qc, q, R, kk)) {
-        const uint32_t slot = atomicAdd(&a.counters[0], 1u);
-        a.exact_rows[slot] = id;
+    bool tie;
+    if (!select_kth<KS>(a, g, qc, q, R, kk, tie)) {
+        defer_row(a, id, tie, kk, R);
         return;
     }
     Pass2Fn f2{q.x, q.y, q.z, kk, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -318,9 +338,9 @@ __global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
     qc.cz = qc.qz / g.cell;
     int R;
     uint32_t kk;
-    if (!select_kth<KS>(a, g, qc, q, R, kk)) {
-        const uint32_t slot = atomicAdd(&a.counters[0], 1u);
-        a.exact_rows[slot] = id;
+    bool tie;
+    if (!select_kth<KS>(a, g, qc, q, R, kk, tie)) {
+        defer_row(a, id, tie, kk, R);
         return;
     }
     uint32_t* row = a.ids_out + (uint64_t)id * a.K;
@@ -336,6 +356,213 @@ __global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
         }
         row[t + 1] = v;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Tie-order resolver.
+//
+// In a tie row the points strictly inside the K-th distance D_K are the
+// reference's, and the remaining m = K - less slots go to points at integer
+// distance D_K.  Among those the reference keeps the smallest FP64 distances
+// and, at equal FP64 distance, the ones its depth-first search meets first
+// (nanoflann.hpp:178-205, :1191-1197): while fewer than m of them have been
+// admitted the result set holds fewer than K points within D_K, so its worst
+// distance exceeds D_K and no subtree holding one of them is pruned.  The
+// search meets points of one leaf in the tree's point order and, for points in
+// different leaves, first the side of their lowest common node that the query
+// visits first (nanoflann.hpp:1226-1236: child1 iff (q-divlow)+(q-divhigh) < 0).
+// Ordering that group therefore needs the replica's tree but not its search.
+static constexpr int TIE_CAP = 32;
+
+// True when the reference's search meets replica position pa before pb.
+__device__ __forceinline__ bool kd_meets_first(const KdOrder& kd, const double q[3], uint32_t pa,
+                                               uint32_t pb) {
+    int node = 0;
+    for (int depth = 0; depth < 64; ++depth) {
+        const int a = __ldg(&kd.c1[node]);
+        if (a < 0) break;
+        const uint32_t split = __ldg(&kd.ne[a]);
+        const bool la = pa < split, lb = pb < split;
+        if (la == lb) {
+            node = la ? a : __ldg(&kd.c2[node]);
+            continue;
+        }
+        const double val = q[__ldg(&kd.feat[node])];
+        const bool left_first =
+            __dadd_rn(__dsub_rn(val, __ldg(&kd.dlo[node])), __dsub_rn(val, __ldg(&kd.dhi[node]))) < 0;
+        return la == left_first;
+    }
+    return pa < pb;
+}
+
+struct TieFn {
+    float qx, qy, qz;
+    uint32_t kk;
+    int s1x, s1y, s1z, sxx, syx, syy, szx, szy, szz, less;
+    int gcnt;
+    uint32_t gid[TIE_CAP];
+    int gd[TIE_CAP][3];
+    uint32_t* row;  // neighbour-set export: ids of the strictly closer points
+    int K;
+    __device__ __forceinline__ unsigned long long limit() const {
+        return (unsigned long long)(kk - KEY_BASE);
+    }
+    __device__ __forceinline__ void add(int ix, int iy, int iz) {
+        s1x += ix;
+        s1y += iy;
+        s1z += iz;
+        sxx += ix * ix;
+        syx += iy * ix;
+        syy += iy * iy;
+        szx += iz * ix;
+        szy += iz * iy;
+        szz += iz * iz;
+    }
+    __device__ __forceinline__ void operator()(const float4 p) {
+        const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+        const uint32_t key = dist_key(dx, dy, dz);
+        if (key < kk) {
+            add(small_int(dx), small_int(dy), small_int(dz));
+            if (row && less < K) row[less] = __float_as_uint(p.w);
+            ++less;
+        } else if (key == kk) {
+            if (gcnt < TIE_CAP) {
+                gid[gcnt] = __float_as_uint(p.w);
+                gd[gcnt][0] = small_int(dx);
+                gd[gcnt][1] = small_int(dy);
+                gd[gcnt][2] = small_int(dz);
+            }
+            ++gcnt;
+        }
+    }
+};
+
+struct TieArgs {
+    GridView gv;
+    const GridParams* gp;
+    const int32_t* x;  // raw coordinates in caller order
+    const int32_t* y;
+    const int32_t* z;
+    int K;
+    StageGroup grp;
+    Transform tf;
+    ExceptionSink ex;
+    const uint2* ties;
+    uint32_t nties;
+    KdOrder kd;
+    uint32_t* exact_rows;
+    uint32_t* counters;
+    uint32_t* ids_out;
+};
+
+__global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nties) return;
+    const uint2 e = a.ties[r];
+    const uint32_t id = e.x;
+    const uint32_t kk = KEY_BASE + (e.y & 0xFFFFFFu);
+    const int R = (int)(e.y >> 24);
+    const GridParams g = *a.gp;
+    const int32_t qraw[3] = {__ldg(&a.x[id]), __ldg(&a.y[id]), __ldg(&a.z[id])};
+    QueryCell qc;
+    qc.qx = qraw[0] - g.minx;
+    qc.qy = qraw[1] - g.miny;
+    qc.qz = qraw[2] - g.minz;
+    qc.cx = qc.qx / g.cell;
+    qc.cy = qc.qy / g.cell;
+    qc.cz = qc.qz / g.cell;
+    TieFn f;
+    f.qx = (float)qc.qx;
+    f.qy = (float)qc.qy;
+    f.qz = (float)qc.qz;
+    f.kk = kk;
+    f.s1x = f.s1y = f.s1z = f.sxx = f.syx = f.syy = f.szx = f.szy = f.szz = 0;
+    f.less = 0;
+    f.gcnt = 0;
+    f.row = a.ids_out ? a.ids_out + (uint64_t)id * a.K : nullptr;
+    f.K = a.K;
+    for (int ring = 0; ring <= R; ++ring) scan_shell(a.gv, g, qc, ring, f);
+    const int m = a.K - f.less;
+    if (f.gcnt > TIE_CAP || m <= 0 || m > f.gcnt) {
+        const uint32_t slot = atomicAdd(&a.counters[0], 1u);
+        a.exact_rows[slot] = id;
+        return;
+    }
+    // the reference's FP64 distances of the group (nanoflann's L2 adaptor
+    // sums the squared differences left to right)
+    const double q64[3] = {ref_coord(qraw[0], a.tf.scale[0], a.tf.offset[0]),
+                           ref_coord(qraw[1], a.tf.scale[1], a.tf.offset[1]),
+                           ref_coord(qraw[2], a.tf.scale[2], a.tf.offset[2])};
+    double d64[TIE_CAP];
+    for (int t = 0; t < f.gcnt; ++t) {
+        double acc = 0.0;
+        for (int d = 0; d < 3; ++d) {
+            const double pc = ref_coord(qraw[d] + f.gd[t][d], a.tf.scale[d], a.tf.offset[d]);
+            const double df = __dsub_rn(q64[d], pc);
+            acc = __dadd_rn(acc, __dmul_rn(df, df));
+        }
+        d64[t] = acc;
+    }
+    uint32_t taken = 0;
+    for (int j = 0; j < m; ++j) {
+        int best = -1;
+        for (int t = 0; t < f.gcnt; ++t) {
+            if ((taken >> t) & 1u) continue;
+            if (best < 0 || d64[t] < d64[best] ||
+                (d64[t] == d64[best] &&
+                 kd_meets_first(a.kd, q64, __ldg(&a.kd.kpos[f.gid[t]]), __ldg(&a.kd.kpos[f.gid[best]]))))
+                best = t;
+        }
+        taken |= 1u << best;
+        f.add(f.gd[best][0], f.gd[best][1], f.gd[best][2]);
+        if (f.row) f.row[f.less + j] = f.gid[best];
+    }
+    if (f.row) {
+        uint32_t* row = f.row;
+        for (int s = 1; s < a.K; ++s) {
+            const uint32_t v = row[s];
+            int t = s - 1;
+            while (t >= 0 && row[t] > v) {
+                row[t + 1] = row[t];
+                --t;
+            }
+            row[t + 1] = v;
+        }
+        return;
+    }
+    const long long n = a.K;
+    long long M[6];
+    M[0] = n * f.sxx - (long long)f.s1x * f.s1x;
+    M[1] = n * f.syx - (long long)f.s1y * f.s1x;
+    M[2] = n * f.syy - (long long)f.s1y * f.s1y;
+    M[3] = n * f.szx - (long long)f.s1z * f.s1x;
+    M[4] = n * f.szy - (long long)f.s1z * f.s1y;
+    M[5] = n * f.szz - (long long)f.s1z * f.s1z;
+    nbg_finish_row(a.grp, a.tf, a.ex, id, (int)n, M, qraw);
+}
+
+int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream) {
+    (void)ctx;
+    if (!tl.nties) return NBG_OK;
+    TieArgs a;
+    a.gv = grid_view(tl.tile);
+    a.gp = tl.tile->gp;
+    a.x = tl.tile->x;
+    a.y = tl.tile->y;
+    a.z = tl.tile->z;
+    a.K = tl.K;
+    a.grp = tl.grp;
+    a.tf = tl.tile->tf;
+    a.ex = tl.ex;
+    a.ties = tl.ties;
+    a.nties = tl.nties;
+    a.kd = tl.kd;
+    a.exact_rows = tl.exact_rows;
+    a.counters = tl.counters;
+    a.ids_out = tl.ids_out;
+    knn_tie_kernel<<<(tl.nties + 127) / 128, 128, 0, stream>>>(a);
+    NBG_LAUNCHED(1);
+    return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
 }
 
 static int slots_for(int K) {
@@ -410,13 +637,16 @@ int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
     la.q.exact_rows = ql.exact_rows;
     la.q.counters = ql.counters;
     la.q.ids_out = nullptr;
+    la.q.ties = ql.ties;
+    la.q.tie_cap = ql.tie_cap;
     la.stream = stream;
     la.ids = false;
     return dispatch_slots<KnnLauncher>(ql.K, la);
 }
 
 int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
-                         uint32_t* exact_rows, uint32_t* counters, cudaStream_t stream) {
+                         uint32_t* exact_rows, uint32_t* counters, uint2* ties, uint32_t tie_cap,
+                         cudaStream_t stream) {
     (void)ctx;
     LaunchArgs la{};
     la.q.gv = grid_view(t);
@@ -428,6 +658,8 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
     la.q.exact_rows = exact_rows;
     la.q.counters = counters;
     la.q.ids_out = ids_out;
+    la.q.ties = ties;
+    la.q.tie_cap = tie_cap;
     la.stream = stream;
     la.ids = true;
     return dispatch_slots<KnnLauncher>(K, la);

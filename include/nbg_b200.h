@@ -127,14 +127,19 @@ typedef struct nbg_row_exception {
 /* Per-call counters (filled by nbg_run when non-null). */
 typedef struct nbg_run_stats {
     uint64_t points;          /* queries answered                               */
-    uint64_t tie_rows;        /* rows whose k-th boundary tied (exact KD path)  */
-    uint64_t deferred_rows;   /* rows answered by the wide ring search          */
-    uint64_t resolved_rows;   /* rows re-solved in FP64                         */
+    uint64_t tie_rows;        /* rows whose k-th boundary tied: ordered on the
+                                 KD replica's tree                              */
+    uint64_t deferred_rows;   /* rows the ring search could not finish          */
+    uint64_t resolved_rows;   /* rows whose eigenproblem the FP32 solver handed
+                                 to the FP64 chain (near-degenerate spectra)    */
     double grid_ms;           /* device time of the grid build                  */
     double query_ms;          /* device time of the fused query kernel(s)       */
-    double tree_ms;           /* device time of the KD replica build + DFS      */
+    double tree_ms;           /* device time of the KD replica build, tie
+                                 ordering and search replay                     */
     double total_ms;          /* device time of the whole call                  */
     uint64_t kernel_launches; /* device kernels this library launched in the call */
+    uint64_t replay_rows;     /* rows answered by the full nanoflann search replay
+                                 (deferred rows, tie groups over 32 points)     */
 } nbg_run_stats;
 
 typedef struct nbg_context nbg_context;
