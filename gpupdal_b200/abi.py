@@ -108,6 +108,7 @@ class RunStats(ctypes.Structure):
         ("total_ms", ctypes.c_double),
         ("kernel_launches", ctypes.c_uint64),
         ("replay_rows", ctypes.c_uint64),
+        ("kd_build_ms", ctypes.c_double),
     ]
 
 

@@ -223,8 +223,15 @@ int nbg_create(nbg_context** out, int device, uint64_t hbm_budget_bytes) {
         delete h;
         return NBG_ERR_CUDA;
     }
-    for (int i = 0; i < 8; ++i) cudaEventCreate(&ctx->ev[i]);
+    for (int i = 0; i < 10; ++i) cudaEventCreate(&ctx->ev[i]);
+    for (int i = 0; i < 2; ++i) cudaEventCreateWithFlags(&ctx->xev[i], cudaEventDisableTiming);
     ctx->events = true;
+    int lo_prio = 0, hi_prio = 0;
+    cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+    if (cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, hi_prio) != cudaSuccess) {
+        delete h;
+        return NBG_ERR_CUDA;
+    }
     if (dev_alloc(ctx, (void**)&ctx->counters, 64 * sizeof(uint32_t), nullptr)) {
         delete h;
         return NBG_ERR_OOM;
@@ -242,8 +249,11 @@ int nbg_destroy(nbg_context* h) {
     dev_free(ctx, ctx->ex_rows, ctx->ex_cap * sizeof(nbg_row_exception));
     dev_free(ctx, ctx->counters, 64 * sizeof(uint32_t));
     ctx_trim(ctx);
-    if (ctx->events)
-        for (int i = 0; i < 8; ++i) cudaEventDestroy(ctx->ev[i]);
+    if (ctx->events) {
+        for (int i = 0; i < 10; ++i) cudaEventDestroy(ctx->ev[i]);
+        for (int i = 0; i < 2; ++i) cudaEventDestroy(ctx->xev[i]);
+    }
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     delete h;
     return NBG_OK;
 }
@@ -521,6 +531,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     cudaEventRecord(ctx->ev[0], stream);
     float grid_ms = 0, query_ms = 0, tree_ms = 0;
     uint64_t tie_rows = 0, deferred_rows = 0, replay_rows = 0;
+    float build_ms = 0;
     ExceptionSink sink{ctx->ex_rows, ctx->counters + 3, (uint32_t)std::max<uint32_t>(exception_capacity, 1)};
     if (cudaMemsetAsync(ctx->counters, 0, 64 * sizeof(uint32_t), stream)) { cleanup(); return NBG_ERR_CUDA; }
     for (auto& gr : groups) {
@@ -567,10 +578,25 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         ql.counters = ctx->counters;
         ql.ties = ctx->ties;
         ql.tie_cap = (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX);
+        // the KD replica does not depend on the query: build it on the side
+        // stream while the query kernel runs (tie rows almost always need it)
+        const bool speculative = !(t->kd && kd_built(t)) && n > 100;
+        if (speculative) {
+            cudaEventRecord(ctx->xev[0], stream);
+            cudaStreamWaitEvent(ctx->side, ctx->xev[0], 0);
+        }
         rc = launch_query(ctx, ql, stream);
         if (rc) { cleanup(); return fail(ctx, rc, std::string("query launch failed: ") +
                                                  cudaGetErrorString(cudaGetLastError())); }
         cudaEventRecord(ctx->ev[3], stream);
+        if (speculative) {
+            cudaEventRecord(ctx->ev[8], ctx->side);
+            rc = kd_ensure(ctx, t, ctx->side);
+            if (rc) { cudaStreamSynchronize(stream); cleanup(); return rc; }
+            cudaEventRecord(ctx->ev[9], ctx->side);
+            cudaEventRecord(ctx->xev[1], ctx->side);
+            cudaStreamWaitEvent(stream, ctx->xev[1], 0);
+        }
         uint32_t cnt[5] = {0, 0, 0, 0, 0};
         cudaError_t e = cudaMemcpyAsync(cnt, ctx->counters, 5 * sizeof(uint32_t),
                                         cudaMemcpyDeviceToHost, stream);
@@ -583,6 +609,10 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         grid_ms += ms;
         cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
         query_ms += ms;
+        if (speculative) {
+            cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]);
+            build_ms += ms;
+        }
         const uint32_t nties = (uint32_t)std::min<uint64_t>(cnt[4], ctx->tie_cap);
         if (cnt[0] || nties) {
             cudaEventRecord(ctx->ev[4], stream);
@@ -662,6 +692,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         stats->grid_ms = grid_ms;
         stats->query_ms = query_ms;
         stats->tree_ms = tree_ms;
+        stats->kd_build_ms = build_ms;
         float ms = 0;
         cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[6]);
         stats->total_ms = ms;

@@ -36,8 +36,12 @@ struct Context {
                                     // [4] tie list, [5] eigen re-solves
     nbg_row_exception* ex_rows = nullptr;
     uint64_t ex_cap = 0;
-    cudaEvent_t ev[8];
+    cudaEvent_t ev[10];
     bool events = false;
+    // high-priority side stream: the KD replica build runs there while the
+    // query kernels run on the caller's stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t xev[2];
     // device blocks released by earlier calls, kept for reuse by size
     std::multimap<size_t, void*> cache;
     uint64_t cached = 0;
@@ -122,6 +126,7 @@ int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const Excep
 int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
                      uint32_t* ids_out, cudaStream_t stream);
 KdOrder kd_order(const Tile* t);
+bool kd_built(const Tile* t);
 void kd_free(Context* ctx, Tile* t);
 uint64_t kd_bytes(uint64_t n);
 int kd_export(Context* ctx, Tile* t, uint32_t* vind, uint32_t* nnodes, int32_t* c1, int32_t* c2,

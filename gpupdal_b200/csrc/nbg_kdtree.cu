@@ -936,6 +936,8 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
     return NBG_OK;
 }
 
+bool kd_built(const Tile* t) { return t->kd && t->kd->built; }
+
 KdOrder kd_order(const Tile* t) {
     const KdReplica* kd = t->kd;
     KdOrder o;

@@ -134,12 +134,15 @@ typedef struct nbg_run_stats {
                                  to the FP64 chain (near-degenerate spectra)    */
     double grid_ms;           /* device time of the grid build                  */
     double query_ms;          /* device time of the fused query kernel(s)       */
-    double tree_ms;           /* device time of the KD replica build, tie
-                                 ordering and search replay                     */
+    double tree_ms;           /* device time after the query kernel: KD replica
+                                 build (when not overlapped), tie ordering and
+                                 search replay                                  */
     double total_ms;          /* device time of the whole call                  */
     uint64_t kernel_launches; /* device kernels this library launched in the call */
     uint64_t replay_rows;     /* rows answered by the full nanoflann search replay
                                  (deferred rows, tie groups over 32 points)     */
+    double kd_build_ms;       /* device time of the KD replica build on the side
+                                 stream, overlapped with the query kernel       */
 } nbg_run_stats;
 
 typedef struct nbg_context nbg_context;
