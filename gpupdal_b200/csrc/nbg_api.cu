@@ -95,6 +95,14 @@ static int dev_alloc(Context* ctx, void** p, size_t bytes, uint64_t* account) {
 static void dev_free(Context* ctx, void* p, size_t bytes) { ctx_free(ctx, p, bytes); }
 
 static int ensure_scratch(Context* ctx, uint64_t n, uint64_t ex_cap) {
+    if (ctx->sums_cap < n) {
+        if (ctx->sums) dev_free(ctx, ctx->sums, ctx->sums_cap * sizeof(RowSums));
+        ctx->sums = nullptr;
+        ctx->sums_cap = 0;
+        int rc = dev_alloc(ctx, (void**)&ctx->sums, std::max<uint64_t>(n, 1024) * sizeof(RowSums), nullptr);
+        if (rc) return rc;
+        ctx->sums_cap = std::max<uint64_t>(n, 1024);
+    }
     if (ctx->tie_cap < n) {
         if (ctx->ties) dev_free(ctx, ctx->ties, ctx->tie_cap * sizeof(uint2));
         ctx->ties = nullptr;
@@ -246,6 +254,7 @@ int nbg_destroy(nbg_context* h) {
     cudaSetDevice(ctx->device);
     dev_free(ctx, ctx->exact_rows, ctx->exact_cap * 4);
     if (ctx->ties) dev_free(ctx, ctx->ties, ctx->tie_cap * sizeof(uint2));
+    if (ctx->sums) dev_free(ctx, ctx->sums, ctx->sums_cap * sizeof(RowSums));
     dev_free(ctx, ctx->ex_rows, ctx->ex_cap * sizeof(nbg_row_exception));
     dev_free(ctx, ctx->counters, 64 * sizeof(uint32_t));
     ctx_trim(ctx);
@@ -578,6 +587,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         ql.counters = ctx->counters;
         ql.ties = ctx->ties;
         ql.tie_cap = (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX);
+        ql.sums = ctx->sums;
         // the KD replica does not depend on the query: build it on the side
         // stream while the query kernel runs (tie rows almost always need it)
         const bool speculative = !(t->kd && kd_built(t)) && n > 100;

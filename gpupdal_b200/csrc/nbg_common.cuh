@@ -71,6 +71,14 @@ struct KdOrder {
     const uint32_t* kpos;
 };
 
+// Exact integer neighbourhood sums of one row (offsets from the query, raw
+// units): s = {S1x, S1y, S1z, Sxx, Syx, Syy, Szx, Szy, Szz}; cnt = 0 marks a
+// row the grid path did not finish.
+struct RowSums {
+    int32_t s[9];
+    int32_t cnt;
+};
+
 // Per-row exception sink.
 struct ExceptionSink {
     nbg_row_exception* rows;

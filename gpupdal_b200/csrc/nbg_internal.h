@@ -32,6 +32,8 @@ struct Context {
     uint64_t exact_cap = 0;
     uint2* ties = nullptr;          // tie list of the query kernels
     uint64_t tie_cap = 0;
+    RowSums* sums = nullptr;        // select -> finish hand-over
+    uint64_t sums_cap = 0;
     uint32_t* counters = nullptr;   // [0] exact rows, [1] tie rows, [2] deferred, [3] exceptions,
                                     // [4] tie list, [5] eigen re-solves
     nbg_row_exception* ex_rows = nullptr;
@@ -101,6 +103,7 @@ struct QueryLaunch {
     uint32_t* counters;
     uint2* ties = nullptr;  // tie list (null: tie rows join exact_rows)
     uint32_t tie_cap = 0;
+    RowSums* sums = nullptr;  // split select/finish kernels (null: one fused kernel)
 };
 int launch_query(Context* ctx, const QueryLaunch& q, cudaStream_t stream);
 

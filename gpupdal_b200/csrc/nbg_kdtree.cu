@@ -39,6 +39,12 @@ namespace nbg {
 
 static constexpr int KD_LEAF = 100;
 static constexpr int KD_TILE = 256;
+// Segments of at most this many points are finished, subtree and all, by
+// one warp (kd_warp_build_kernel) instead of level by level.
+static constexpr uint32_t KD_WARP_MAX = 4096;
+static constexpr int KD_WSTACK = 64;
+static constexpr int KD_WARPS = 4;
+static constexpr int KD_RETRY = -100;  // kd_build: redo without warp subtrees
 static constexpr int KD_STACK = 96;
 static constexpr int KD_CAP = 66;
 
@@ -98,6 +104,9 @@ struct KdReplica {
     KdSeg* seg2 = nullptr;
     KdSplit* split = nullptr;
     uint32_t seg_cap = 0;
+    KdSeg* small = nullptr;      // segments left for the warp builder
+    uint32_t* leaves = nullptr;  // leaves made by the level passes (bbox pending)
+    uint32_t leaf_cap = 0;
     // tiles
     uint32_t* nt = nullptr;        // per segment tile count, then prefix (seg_cap+1)
     uint32_t* tile_seg = nullptr;
@@ -106,8 +115,9 @@ struct KdReplica {
     uint32_t tile_cap = 0;
     void* scan_tmp = nullptr;
     size_t scan_bytes = 0;
-    uint32_t* counters = nullptr;  // [0] next segments, [1] nodes, [2] errors
-    std::vector<uint32_t> level_begin;  // node id range per level (host)
+    uint32_t* counters = nullptr;  // [0] next segments, [1] nodes, [2] errors, [3] small
+                                   // segments, [4] leaves
+    uint32_t dl_cap = 0;
     double root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
     bool built = false;
     uint64_t bytes = 0;
@@ -220,24 +230,24 @@ __global__ void kd_seg_minmax_kernel(uint32_t S, const uint32_t* tile_first, con
     }
 }
 
-__global__ void kd_split_kernel(const KdSeg* segs, uint32_t S, KdSplit* sp, Transform tf) {
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= S) return;
-    const KdSeg sg = segs[s];
-    KdSplit p = sp[s];
+// Cut feature and value of a segment from its top-down box (lo, hi) and its
+// points' extents (mn, mx): nanoflann.hpp:779-828 middleSplit_.
+__device__ __forceinline__ void kd_choose_cut(const double lo[3], const double hi[3],
+                                              const int32_t mn_[3], const int32_t mx_[3],
+                                              const Transform& tf, int& cutfeat, double& cutval) {
     const double EPS = 0.00001;
-    double max_span = __dsub_rn(sg.hi[0], sg.lo[0]);
+    double max_span = __dsub_rn(hi[0], lo[0]);
     for (int i = 1; i < 3; ++i) {
-        double span = __dsub_rn(sg.hi[i], sg.lo[i]);
+        double span = __dsub_rn(hi[i], lo[i]);
         if (span > max_span) max_span = span;
     }
     double max_spread = -1;
-    int cutfeat = 0;
+    cutfeat = 0;
     for (int i = 0; i < 3; ++i) {
-        double span = __dsub_rn(sg.hi[i], sg.lo[i]);
+        double span = __dsub_rn(hi[i], lo[i]);
         if (span > __dmul_rn(__dsub_rn(1.0, EPS), max_span)) {
-            double mn = ref_coord(p.mn[i], tf.scale[i], tf.offset[i]);
-            double mx = ref_coord(p.mx[i], tf.scale[i], tf.offset[i]);
+            double mn = ref_coord(mn_[i], tf.scale[i], tf.offset[i]);
+            double mx = ref_coord(mx_[i], tf.scale[i], tf.offset[i]);
             double spread = __dsub_rn(mx, mn);
             if (spread > max_spread) {
                 cutfeat = i;
@@ -245,13 +255,28 @@ __global__ void kd_split_kernel(const KdSeg* segs, uint32_t S, KdSplit* sp, Tran
             }
         }
     }
-    double split_val = __ddiv_rn(__dadd_rn(sg.lo[cutfeat], sg.hi[cutfeat]), 2.0);
-    double mn = ref_coord(p.mn[cutfeat], tf.scale[cutfeat], tf.offset[cutfeat]);
-    double mx = ref_coord(p.mx[cutfeat], tf.scale[cutfeat], tf.offset[cutfeat]);
-    double cutval;
+    double split_val = __ddiv_rn(__dadd_rn(lo[cutfeat], hi[cutfeat]), 2.0);
+    double mn = ref_coord(mn_[cutfeat], tf.scale[cutfeat], tf.offset[cutfeat]);
+    double mx = ref_coord(mx_[cutfeat], tf.scale[cutfeat], tf.offset[cutfeat]);
     if (split_val < mn) cutval = mn;
     else if (split_val > mx) cutval = mx;
     else cutval = split_val;
+}
+
+__global__ void kd_split_kernel(const KdSeg* segs, uint32_t S, KdSplit* sp, Transform tf,
+                                int32_t* bmin, int32_t* bmax) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const KdSeg sg = segs[s];
+    KdSplit p = sp[s];
+    // the node's extents are its points' extents
+    for (int d = 0; d < 3; ++d) {
+        bmin[3 * sg.node + d] = p.mn[d];
+        bmax[3 * sg.node + d] = p.mx[d];
+    }
+    int cutfeat;
+    double cutval;
+    kd_choose_cut(sg.lo, sg.hi, p.mn, p.mx, tf, cutfeat, cutval);
     sp[s].f = cutfeat;
     sp[s].cutval = cutval;
 }
@@ -383,7 +408,9 @@ __global__ void kd_pass2_segs_kernel(const KdSeg* segs, uint32_t S, const KdSpli
 
 __global__ void kd_children_kernel(const KdSeg* segs, uint32_t S, const KdSplit* sp, KdSeg* next,
                                    uint32_t* counters, int32_t* c1, int32_t* c2, int32_t* feat,
-                                   uint32_t* nb, uint32_t* ne, uint32_t node_cap, uint32_t seg_cap) {
+                                   uint32_t* nb, uint32_t* ne, uint32_t node_cap, uint32_t seg_cap,
+                                   KdSeg* small, uint32_t small_max, uint32_t* leaves,
+                                   uint32_t leaf_cap) {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
     const KdSeg sg = segs[s];
@@ -418,7 +445,16 @@ __global__ void kd_children_kernel(const KdSeg* segs, uint32_t S, const KdSplit*
         c1[node] = -1;
         c2[node] = -1;
         feat[node] = 0;
-        if (ch.end - ch.begin > (uint32_t)KD_LEAF) {
+        const uint32_t len = ch.end - ch.begin;
+        if (len <= (uint32_t)KD_LEAF) {
+            const uint32_t slot = atomicAdd(&counters[4], 1u);
+            if (slot < leaf_cap) leaves[slot] = node;
+            else atomicAdd(&counters[2], 1u);
+        } else if (len <= small_max) {
+            const uint32_t slot = atomicAdd(&counters[3], 1u);
+            if (slot < seg_cap) small[slot] = ch;
+            else atomicAdd(&counters[2], 1u);
+        } else {
             const uint32_t slot = atomicAdd(&counters[0], 1u);
             if (slot < seg_cap) next[slot] = ch;
             else atomicAdd(&counters[2], 1u);
@@ -426,37 +462,167 @@ __global__ void kd_children_kernel(const KdSeg* segs, uint32_t S, const KdSplit*
     }
 }
 
-__global__ void kd_node_bbox_kernel(uint32_t first, uint32_t last, const int32_t* c1,
-                                    const int32_t* c2, const uint32_t* nb, const uint32_t* ne,
-                                    const int32_t* rx, const int32_t* ry, const int32_t* rz,
-                                    int32_t* bmin, int32_t* bmax) {
-    uint32_t node = first + blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= last) return;
-    int32_t lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
-    if (c1[node] < 0 && ne[node] <= nb[node]) {
-        // empty leaf: cannot arise from the split rule; keep the empty box
-    } else if (c1[node] < 0) {
-        lo[0] = hi[0] = rx[nb[node]];
-        lo[1] = hi[1] = ry[nb[node]];
-        lo[2] = hi[2] = rz[nb[node]];
-        for (uint32_t i = nb[node] + 1; i < ne[node]; ++i) {
-            lo[0] = min(lo[0], rx[i]);
-            hi[0] = max(hi[0], rx[i]);
-            lo[1] = min(lo[1], ry[i]);
-            hi[1] = max(hi[1], ry[i]);
-            lo[2] = min(lo[2], rz[i]);
-            hi[2] = max(hi[2], rz[i]);
-        }
-    } else {
-        const int a = c1[node], b = c2[node];
+// Extents of [b, e) by one warp (INT32_MAX / INT32_MIN when empty).
+__device__ __forceinline__ void kd_warp_minmax(const int32_t* rx, const int32_t* ry, const int32_t* rz,
+                                               uint32_t b, uint32_t e, int lane, int32_t mn[3],
+                                               int32_t mx[3]) {
+    int32_t v[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, w[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    for (uint32_t i = b + lane; i < e; i += 32) {
+        const int32_t c[3] = {rx[i], ry[i], rz[i]};
+#pragma unroll
         for (int d = 0; d < 3; ++d) {
-            lo[d] = min(bmin[3 * a + d], bmin[3 * b + d]);
-            hi[d] = max(bmax[3 * a + d], bmax[3 * b + d]);
+            v[d] = min(v[d], c[d]);
+            w[d] = max(w[d], c[d]);
         }
     }
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
-        bmin[3 * node + d] = lo[d];
-        bmax[3 * node + d] = hi[d];
+        mn[d] = __reduce_min_sync(0xffffffffu, v[d]);
+        mx[d] = __reduce_max_sync(0xffffffffu, w[d]);
+    }
+}
+
+// Leaves made by the level passes: their extents, one warp per leaf.
+__global__ void kd_leaf_bbox_kernel(const uint32_t* leaves, uint32_t nleaves, const uint32_t* nb,
+                                    const uint32_t* ne, const int32_t* rx, const int32_t* ry,
+                                    const int32_t* rz, int32_t* bmin, int32_t* bmax) {
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= nleaves) return;
+    const uint32_t node = leaves[w];
+    int32_t mn[3], mx[3];
+    kd_warp_minmax(rx, ry, rz, nb[node], ne[node], lane, mn, mx);
+    if (lane < 3) {
+        bmin[3 * node + lane] = mn[lane];
+        bmax[3 * node + lane] = mx[lane];
+    }
+}
+
+// One Hoare pass of nanoflann's planeSplit over [b, e) by one warp: with L
+// the count satisfying the predicate, the t-th element from the left failing
+// it inside [b, b+L) swaps with the t-th element from the right satisfying it
+// inside [b+L, e).  Returns L.  mlpos/mrpos[b ...] are the warp's scratch.
+template <int PASS>
+__device__ uint32_t kd_warp_pass(int32_t* rx, int32_t* ry, int32_t* rz, uint32_t* rid,
+                                 uint32_t* mlpos, uint32_t* mrpos, uint32_t b, uint32_t e, int f,
+                                 double cut, const Transform& tf, int lane) {
+    const int32_t* rc = f == 0 ? rx : (f == 1 ? ry : rz);
+    const double sc = tf.scale[f], of = tf.offset[f];
+    const unsigned lt = (1u << lane) - 1u;
+    uint32_t L = 0;
+    for (uint32_t base = b; base < e; base += 32) {
+        const uint32_t i = base + lane;
+        const bool p = i < e && kd_pred<PASS>(ref_coord(rc[i], sc, of), cut);
+        L += __popc(__ballot_sync(0xffffffffu, p));
+    }
+    uint32_t m = 0;
+    for (uint32_t base = b; base < b + L; base += 32) {
+        const uint32_t i = base + lane;
+        const bool q = i < b + L && !kd_pred<PASS>(ref_coord(rc[i], sc, of), cut);
+        const unsigned mask = __ballot_sync(0xffffffffu, q);
+        if (q) mlpos[b + m + __popc(mask & lt)] = i;
+        m += __popc(mask);
+    }
+    uint32_t r = 0;
+    for (uint32_t base = b + L; base < e; base += 32) {
+        const uint32_t i = base + lane;
+        const bool q = i < e && kd_pred<PASS>(ref_coord(rc[i], sc, of), cut);
+        const unsigned mask = __ballot_sync(0xffffffffu, q);
+        if (q) {
+            const uint32_t k = r + __popc(mask & lt);
+            if (k < m) mrpos[b + (m - 1 - k)] = i;
+        }
+        r += __popc(mask);
+    }
+    __syncwarp();
+    for (uint32_t t = lane; t < m; t += 32) {
+        const uint32_t a = mlpos[b + t], c = mrpos[b + t];
+        const int32_t tx = rx[a], ty = ry[a], tz = rz[a];
+        const uint32_t ti = rid[a];
+        rx[a] = rx[c];
+        ry[a] = ry[c];
+        rz[a] = rz[c];
+        rid[a] = rid[c];
+        rx[c] = tx;
+        ry[c] = ty;
+        rz[c] = tz;
+        rid[c] = ti;
+    }
+    __syncwarp();
+    return L;
+}
+
+// Builds the whole subtree of each listed segment, one warp per segment,
+// depth first with an explicit stack in shared memory.  Same split rules as
+// the level passes; nodes are numbered by an atomic counter.  counters[2]
+// counts capacity or stack overflows (the host then rebuilds level by level).
+__global__ void __launch_bounds__(32 * KD_WARPS) kd_warp_build_kernel(
+    const KdSeg* small, uint32_t nsmall, int32_t* rx, int32_t* ry, int32_t* rz, uint32_t* rid,
+    uint32_t* mlpos, uint32_t* mrpos, int32_t* c1, int32_t* c2, int32_t* feat, uint32_t* nb,
+    uint32_t* ne, int32_t* bmin, int32_t* bmax, uint32_t* counters, uint32_t node_cap,
+    Transform tf) {
+    __shared__ KdSeg stk[KD_WARPS][KD_WSTACK];
+    const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t w = blockIdx.x * KD_WARPS + wl;
+    if (w >= nsmall) return;
+    KdSeg* st = stk[wl];
+    if (lane == 0) st[0] = small[w];
+    int top = 1;
+    __syncwarp();
+    while (top > 0) {
+        const KdSeg sg = st[top - 1];
+        --top;
+        __syncwarp();
+        const uint32_t b = sg.begin, e = sg.end, count = e - b;
+        const int node = sg.node;
+        int32_t mn[3], mx[3];
+        kd_warp_minmax(rx, ry, rz, b, e, lane, mn, mx);
+        if (lane < 3) {
+            bmin[3 * node + lane] = mn[lane];
+            bmax[3 * node + lane] = mx[lane];
+        }
+        if (count <= (uint32_t)KD_LEAF) continue;
+        int f;
+        double cut;
+        kd_choose_cut(sg.lo, sg.hi, mn, mx, tf, f, cut);
+        const uint32_t L = kd_warp_pass<1>(rx, ry, rz, rid, mlpos, mrpos, b, e, f, cut, tf, lane);
+        const uint32_t L2 = kd_warp_pass<2>(rx, ry, rz, rid, mlpos, mrpos, b + L, e, f, cut, tf, lane);
+        const uint32_t lim1 = L, lim2 = L + L2;
+        uint32_t index;
+        if (lim1 > count / 2) index = lim1;
+        else if (lim2 < count / 2) index = lim2;
+        else index = count / 2;
+        uint32_t cid = 0;
+        if (lane == 0) cid = atomicAdd(&counters[1], 2u);
+        cid = __shfl_sync(0xffffffffu, cid, 0);
+        if (cid + 2 > node_cap || top + 2 > KD_WSTACK) {
+            if (lane == 0) atomicAdd(&counters[2], 1u);
+            return;
+        }
+        if (lane == 0) {
+            c1[node] = (int32_t)cid;
+            c2[node] = (int32_t)(cid + 1);
+            feat[node] = f;
+            for (int side = 1; side >= 0; --side) {
+                KdSeg ch = sg;
+                if (side == 0) {
+                    ch.end = b + index;
+                    ch.hi[f] = cut;
+                } else {
+                    ch.begin = b + index;
+                    ch.lo[f] = cut;
+                }
+                ch.node = (int32_t)(cid + side);
+                nb[cid + side] = ch.begin;
+                ne[cid + side] = ch.end;
+                c1[cid + side] = -1;
+                c2[cid + side] = -1;
+                feat[cid + side] = 0;
+                st[top + (1 - side)] = ch;
+            }
+        }
+        top += 2;
+        __syncwarp();
     }
 }
 
@@ -775,47 +941,27 @@ static int kd_pass(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, c
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
 }
 
-int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
-    if (t->kd && t->kd->built) return NBG_OK;
-    if (!t->kd) t->kd = new KdReplica();
+static int kd_grow_nodes(Context* ctx, KdReplica* kd, uint32_t nc, cudaStream_t st) {
+    const uint32_t old = kd->node_cap;
+    if (nc <= old) return NBG_OK;
+    int rc = kd_grow(ctx, &kd->c1, old, nc, kd, st);
+    if (!rc) rc = kd_grow(ctx, &kd->c2, old, nc, kd, st);
+    if (!rc) rc = kd_grow(ctx, &kd->feat, old, nc, kd, st);
+    if (!rc) rc = kd_grow(ctx, &kd->nb, old, nc, kd, st);
+    if (!rc) rc = kd_grow(ctx, &kd->ne, old, nc, kd, st);
+    if (!rc) rc = kd_grow(ctx, &kd->bmin, (size_t)old * 3, (size_t)nc * 3, kd, st);
+    if (!rc) rc = kd_grow(ctx, &kd->bmax, (size_t)old * 3, (size_t)nc * 3, kd, st);
+    if (rc) return rc;
+    kd->node_cap = nc;
+    return NBG_OK;
+}
+
+// One build of the replica; `small_max` = 0 keeps every level on the level
+// passes (the fallback when a warp subtree overflows its stack or the nodes).
+static int kd_build(Context* ctx, Tile* t, uint32_t small_max, cudaStream_t st) {
     KdReplica* kd = t->kd;
     const uint64_t n = t->n;
-    kd->n = n;
     int rc = NBG_OK;
-    if (!kd->rx) {
-        rc = kd_alloc(ctx, (void**)&kd->rx, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->ry, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->rz, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->rid, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->mlpos, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->mrpos, n * 4, kd);
-        kd->seg_cap = (uint32_t)(n / 50 + 64);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[0], kd->seg_cap * sizeof(KdSeg), kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[1], kd->seg_cap * sizeof(KdSeg), kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg2, kd->seg_cap * sizeof(KdSeg), kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->split, kd->seg_cap * sizeof(KdSplit), kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->nt, (kd->seg_cap + 1) * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->counters, 64, kd);
-        size_t b1 = 0;
-        cub::DeviceScan::ExclusiveSum(nullptr, b1, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                      (int)(n / KD_TILE + kd->seg_cap + 2));
-        kd->scan_bytes = b1;
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->scan_tmp, b1, kd);
-        kd->node_cap = 0;
-        if (rc) return rc;
-    }
-    // nodes: initial guess, grown per level as needed
-    const uint32_t want_nodes = (uint32_t)(n / 25 + 64);
-    if (kd->node_cap < want_nodes) {
-        const uint32_t old = kd->node_cap;
-        rc = kd_grow(ctx, &kd->c1, old, want_nodes, kd, st);
-        if (!rc) rc = kd_grow(ctx, &kd->c2, old, want_nodes, kd, st);
-        if (!rc) rc = kd_grow(ctx, &kd->feat, old, want_nodes, kd, st);
-        if (!rc) rc = kd_grow(ctx, &kd->nb, old, want_nodes, kd, st);
-        if (!rc) rc = kd_grow(ctx, &kd->ne, old, want_nodes, kd, st);
-        if (rc) return rc;
-        kd->node_cap = want_nodes;
-    }
     kd_init_kernel<<<std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, ctx->sm_count * 8)), 256, 0,
                      st>>>(t->x, t->y, t->z, n, kd->rx, kd->ry, kd->rz, kd->rid);
     NBG_LAUNCHED(1);
@@ -841,26 +987,26 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
     cudaMemcpyAsync(kd->feat, &zero, 4, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(kd->nb, &zero, 4, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(kd->ne, &rootend, 4, cudaMemcpyHostToDevice, st);
-    kd->node_count = 1;
-    kd->level_begin.assign(1, 0);
+    uint32_t cnt[5] = {0, 1, 0, 0, 0};
     uint32_t S = 0;
-    if (n > (uint64_t)KD_LEAF) {
+    if (n > (uint64_t)KD_LEAF && n > small_max) {
         cudaMemcpyAsync(kd->seg[0], &root, sizeof(KdSeg), cudaMemcpyHostToDevice, st);
         S = 1;
+    } else if (n > (uint64_t)KD_LEAF) {
+        cudaMemcpyAsync(kd->small, &root, sizeof(KdSeg), cudaMemcpyHostToDevice, st);
+        cnt[3] = 1;
+    } else {
+        cudaMemcpyAsync(kd->leaves, &zero, 4, cudaMemcpyHostToDevice, st);
+        cnt[4] = 1;
     }
+    cudaMemcpyAsync(kd->counters, cnt, sizeof(cnt), cudaMemcpyHostToDevice, st);
+    uint32_t node_count = 1;
     int cur = 0;
     while (S > 0) {
         // room for this level's children
-        if (kd->node_count + 2 * S > kd->node_cap) {
-            const uint32_t old = kd->node_cap;
-            const uint32_t nc = std::max<uint32_t>(old * 2, kd->node_count + 2 * S + 64);
-            rc = kd_grow(ctx, &kd->c1, old, nc, kd, st);
-            if (!rc) rc = kd_grow(ctx, &kd->c2, old, nc, kd, st);
-            if (!rc) rc = kd_grow(ctx, &kd->feat, old, nc, kd, st);
-            if (!rc) rc = kd_grow(ctx, &kd->nb, old, nc, kd, st);
-            if (!rc) rc = kd_grow(ctx, &kd->ne, old, nc, kd, st);
+        if (node_count + 2 * S > kd->node_cap) {
+            rc = kd_grow_nodes(ctx, kd, std::max<uint32_t>(kd->node_cap * 2, node_count + 2 * S + 64), st);
             if (rc) return rc;
-            kd->node_cap = nc;
         }
         const KdSeg* segs = kd->seg[cur];
         uint32_t ntiles = 0;
@@ -874,21 +1020,21 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
                                                                       kd->split);
             NBG_LAUNCHED(1);
         }
-        kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, tf);
+        kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, tf, kd->bmin, kd->bmax);
         NBG_LAUNCHED(2 + (ntiles ? 1 : 0));
         rc = kd_pass<1>(ctx, kd, segs, S, tf, st);
         if (rc) return rc;
         kd_pass2_segs_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg2);
         rc = kd_pass<2>(ctx, kd, kd->seg2, S, tf, st);
         if (rc) return rc;
-        uint32_t cnt[3] = {0, kd->node_count, 0};
-        cudaMemcpyAsync(kd->counters, cnt, 12, cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(kd->counters, 0, 4, st);
         NBG_LAUNCHED(2);
         kd_children_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg[cur ^ 1],
                                                             kd->counters, kd->c1, kd->c2, kd->feat,
                                                             kd->nb, kd->ne, kd->node_cap,
-                                                            kd->seg_cap);
-        cudaMemcpyAsync(cnt, kd->counters, 12, cudaMemcpyDeviceToHost, st);
+                                                            kd->seg_cap, kd->small, small_max,
+                                                            kd->leaves, kd->leaf_cap);
+        cudaMemcpyAsync(cnt, kd->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st);
         cudaError_t be = cudaGetLastError();
         if (be == cudaSuccess) be = cudaStreamSynchronize(st);
         if (be != cudaSuccess) {
@@ -899,25 +1045,43 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
             ctx->err = "KD replica build ran out of node or segment capacity";
             return NBG_ERR_UNSUPPORTED;
         }
-        kd->level_begin.push_back(kd->node_count);
-        kd->node_count = cnt[1];
+        node_count = cnt[1];
         S = cnt[0];
         cur ^= 1;
     }
-    kd->level_begin.push_back(kd->node_count);
-    // extents bottom-up, then divlow / divhigh
-    const uint32_t nn = kd->node_count;
-    rc = kd_alloc(ctx, (void**)&kd->bmin, (size_t)nn * 12, kd);
-    if (!rc) rc = kd_alloc(ctx, (void**)&kd->bmax, (size_t)nn * 12, kd);
-    if (!rc) rc = kd_alloc(ctx, (void**)&kd->dlo, (size_t)nn * 8, kd);
-    if (!rc) rc = kd_alloc(ctx, (void**)&kd->dhi, (size_t)nn * 8, kd);
-    if (rc) return rc;
-    for (int lv = (int)kd->level_begin.size() - 2; lv >= 0; --lv) {
-        const uint32_t a = kd->level_begin[lv], b = kd->level_begin[lv + 1];
-        if (b > a)
-            kd_node_bbox_kernel<<<(b - a + 127) / 128, 128, 0, st>>>(a, b, kd->c1, kd->c2, kd->nb,
-                                                                   kd->ne, kd->rx, kd->ry, kd->rz,
-                                                                   kd->bmin, kd->bmax);
+    // subtrees of the small segments, one warp each
+    const uint32_t nsmall = cnt[3], nleaves = cnt[4];
+    if (nsmall) {
+        rc = kd_grow_nodes(ctx, kd, std::max<uint32_t>(kd->node_cap, node_count + (uint32_t)(n / 8) + 1024), st);
+        if (rc) return rc;
+        kd_warp_build_kernel<<<(nsmall + KD_WARPS - 1) / KD_WARPS, 32 * KD_WARPS, 0, st>>>(
+            kd->small, nsmall, kd->rx, kd->ry, kd->rz, kd->rid, kd->mlpos, kd->mrpos, kd->c1, kd->c2,
+            kd->feat, kd->nb, kd->ne, kd->bmin, kd->bmax, kd->counters, kd->node_cap, tf);
+        NBG_LAUNCHED(1);
+    }
+    if (nleaves)
+        kd_leaf_bbox_kernel<<<(nleaves * 32 + 127) / 128, 128, 0, st>>>(
+            kd->leaves, nleaves, kd->nb, kd->ne, kd->rx, kd->ry, kd->rz, kd->bmin, kd->bmax);
+    cudaMemcpyAsync(cnt, kd->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+    cudaError_t we = cudaGetLastError();
+    if (we == cudaSuccess) we = cudaStreamSynchronize(st);
+    if (we != cudaSuccess) {
+        ctx->err = std::string("KD replica subtree build failed: ") + cudaGetErrorString(we);
+        return NBG_ERR_CUDA;
+    }
+    if (cnt[2]) return KD_RETRY;
+    node_count = cnt[1];
+    kd->node_count = node_count;
+    // divlow / divhigh from the children's extents
+    const uint32_t nn = node_count;
+    if (!kd->dlo || kd->dl_cap < nn) {
+        if (kd->dlo) kd_release(ctx, kd, kd->dlo);
+        if (kd->dhi) kd_release(ctx, kd, kd->dhi);
+        kd->dlo = kd->dhi = nullptr;
+        rc = kd_alloc(ctx, (void**)&kd->dlo, (size_t)nn * 8, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->dhi, (size_t)nn * 8, kd);
+        if (rc) return rc;
+        kd->dl_cap = nn;
     }
     kd_div_kernel<<<(nn + 127) / 128, 128, 0, st>>>(nn, kd->c1, kd->c2, kd->feat, kd->bmin,
                                                     kd->bmax, tf, kd->dlo, kd->dhi);
@@ -927,11 +1091,61 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
     }
     kd_inverse_kernel<<<std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, ctx->sm_count * 8)), 256,
                         0, st>>>(kd->rid, n, kd->kpos);
-    NBG_LAUNCHED(kd->level_begin.size() + 1);
+    NBG_LAUNCHED(2 + (nleaves ? 1 : 0));
     if (cudaStreamSynchronize(st) != cudaSuccess) {
         ctx->err = "KD replica extents failed";
         return NBG_ERR_CUDA;
     }
+    return NBG_OK;
+}
+
+int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
+    if (t->kd && t->kd->built) return NBG_OK;
+    if (!t->kd) t->kd = new KdReplica();
+    KdReplica* kd = t->kd;
+    const uint64_t n = t->n;
+    kd->n = n;
+    int rc = NBG_OK;
+    if (!kd->rx) {
+        rc = kd_alloc(ctx, (void**)&kd->rx, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->ry, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->rz, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->rid, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->mlpos, n * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->mrpos, n * 4, kd);
+        kd->seg_cap = (uint32_t)(n / 50 + 64);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[0], kd->seg_cap * sizeof(KdSeg), kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[1], kd->seg_cap * sizeof(KdSeg), kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg2, kd->seg_cap * sizeof(KdSeg), kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->small, kd->seg_cap * sizeof(KdSeg), kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->split, kd->seg_cap * sizeof(KdSplit), kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->nt, (kd->seg_cap + 1) * 4, kd);
+        kd->leaf_cap = (uint32_t)(n / 16 + 1024);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->leaves, (size_t)kd->leaf_cap * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->counters, 64, kd);
+        size_t b1 = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, b1, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                      (int)(n / KD_TILE + kd->seg_cap + 2));
+        kd->scan_bytes = b1;
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->scan_tmp, b1, kd);
+        kd->node_cap = 0;
+        if (rc) return rc;
+    }
+    // nodes: initial guess, grown as needed
+    rc = kd_grow_nodes(ctx, kd, (uint32_t)(n / 25 + 64), st);
+    if (rc) return rc;
+    rc = kd_build(ctx, t, KD_WARP_MAX, st);
+    if (rc == KD_RETRY) {
+        // a warp subtree overflowed its stack or the node arrays: redo the
+        // whole build with the level passes only
+        rc = kd_grow_nodes(ctx, kd, (uint32_t)std::min<uint64_t>(2 * n + 64, UINT32_MAX), st);
+        if (!rc) rc = kd_build(ctx, t, 0, st);
+        if (rc == KD_RETRY) {
+            ctx->err = "KD replica build ran out of node capacity";
+            rc = NBG_ERR_UNSUPPORTED;
+        }
+    }
+    if (rc) return rc;
     kd->built = true;
     return NBG_OK;
 }

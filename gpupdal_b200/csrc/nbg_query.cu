@@ -222,6 +222,7 @@ struct QueryArgs {
     uint32_t* ids_out;   // neighbour-set export (null in the fused path)
     uint2* ties;         // tie list {id, (D_K - 2^23 bias) | R << 24}; null: ties go to exact_rows
     uint32_t tie_cap;
+    RowSums* sums;       // split form: per sorted position, read by knn_finish_kernel
 };
 
 // A row that cannot finish on the grid: a boundary tie goes to the tie list
@@ -319,6 +320,75 @@ __global__ void __launch_bounds__(128) knn_fused_kernel(const QueryArgs a) {
     M[4] = n * f2.szy - (long long)f2.s1z * f2.s1y;
     M[5] = n * f2.szz - (long long)f2.s1z * f2.s1z;
     const int32_t qraw[3] = {qc.qx + g.minx, qc.qy + g.miny, qc.qz + g.minz};
+    nbg_finish_row(a.grp, a.tf, a.ex, id, (int)n, M, qraw);
+}
+
+// Split form, pass 1 + pass 2: the row's exact neighbourhood sums, in sorted
+// order (cnt = 0 marks a row handed to the exact path).
+template <int KS>
+__global__ void __launch_bounds__(128) knn_select_kernel(const QueryArgs a) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const GridParams g = *a.gp;
+    const float4 q = __ldg(&a.gv.sorted[i]);
+    const uint32_t id = __float_as_uint(q.w);
+    QueryCell qc;
+    qc.qx = __float2int_rz(q.x);
+    qc.qy = __float2int_rz(q.y);
+    qc.qz = __float2int_rz(q.z);
+    qc.cx = qc.qx / g.cell;
+    qc.cy = qc.qy / g.cell;
+    qc.cz = qc.qz / g.cell;
+    int R;
+    uint32_t kk;
+    bool tie;
+    RowSums out;
+    out.cnt = 0;
+    if (!select_kth<KS>(a, g, qc, q, R, kk, tie)) {
+        defer_row(a, id, tie, kk, R);
+        a.sums[i] = out;
+        return;
+    }
+    Pass2Fn f2{q.x, q.y, q.z, kk, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int r = 0; r <= R; ++r) scan_shell(a.gv, g, qc, r, f2);
+    if (f2.cnt != a.K) {
+        defer_row(a, id, false, kk, R);
+        a.sums[i] = out;
+        return;
+    }
+    out.s[0] = f2.s1x;
+    out.s[1] = f2.s1y;
+    out.s[2] = f2.s1z;
+    out.s[3] = f2.sxx;
+    out.s[4] = f2.syx;
+    out.s[5] = f2.syy;
+    out.s[6] = f2.szx;
+    out.s[7] = f2.szy;
+    out.s[8] = f2.szz;
+    out.cnt = f2.cnt;
+    a.sums[i] = out;
+}
+
+// Split form, finish: covariance, eigensolve and stage projections of the
+// rows the select kernel completed.  Uniform work per thread.
+__global__ void __launch_bounds__(128) knn_finish_kernel(const QueryArgs a) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const RowSums r = a.sums[i];
+    if (r.cnt == 0) return;
+    const GridParams* gp = a.gp;
+    const float4 q = __ldg(&a.gv.sorted[i]);
+    const uint32_t id = __float_as_uint(q.w);
+    const long long n = r.cnt;
+    long long M[6];
+    M[0] = n * r.s[3] - (long long)r.s[0] * r.s[0];
+    M[1] = n * r.s[4] - (long long)r.s[1] * r.s[0];
+    M[2] = n * r.s[5] - (long long)r.s[1] * r.s[1];
+    M[3] = n * r.s[6] - (long long)r.s[2] * r.s[0];
+    M[4] = n * r.s[7] - (long long)r.s[2] * r.s[1];
+    M[5] = n * r.s[8] - (long long)r.s[2] * r.s[2];
+    const int32_t qraw[3] = {__float2int_rz(q.x) + __ldg(&gp->minx), __float2int_rz(q.y) + __ldg(&gp->miny),
+                             __float2int_rz(q.z) + __ldg(&gp->minz)};
     nbg_finish_row(a.grp, a.tf, a.ex, id, (int)n, M, qraw);
 }
 
@@ -606,11 +676,17 @@ struct KnnLauncher {
         const int threads = 128;
         const uint64_t blocks = (la.q.n + threads - 1) / threads;
         if (blocks == 0) return NBG_OK;
-        if (la.ids)
+        if (la.ids) {
             knn_ids_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
-        else
+            NBG_LAUNCHED(1);
+        } else if (la.q.sums) {
+            knn_select_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
+            knn_finish_kernel<<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
+            NBG_LAUNCHED(2);
+        } else {
             knn_fused_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
-        NBG_LAUNCHED(1);
+            NBG_LAUNCHED(1);
+        }
         return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
     }
 };
@@ -639,6 +715,7 @@ int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
     la.q.ids_out = nullptr;
     la.q.ties = ql.ties;
     la.q.tie_cap = ql.tie_cap;
+    la.q.sums = ql.sums;
     la.stream = stream;
     la.ids = false;
     return dispatch_slots<KnnLauncher>(ql.K, la);
@@ -660,6 +737,7 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
     la.q.ids_out = ids_out;
     la.q.ties = ties;
     la.q.tie_cap = tie_cap;
+    la.q.sums = nullptr;
     la.stream = stream;
     la.ids = true;
     return dispatch_slots<KnnLauncher>(K, la);
