@@ -112,6 +112,40 @@ class RunStats(ctypes.Structure):
     ]
 
 
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("x", ctypes.c_void_p),
+        ("y", ctypes.c_void_p),
+        ("z", ctypes.c_void_p),
+        ("n", ctypes.c_uint64),
+        ("scale", ctypes.c_double * 3),
+        ("offset", ctypes.c_double * 3),
+        ("on_device", ctypes.c_int32),
+        ("n_stages", ctypes.c_int32),
+        ("stages", ctypes.POINTER(StageOpts)),
+        ("outputs", ctypes.POINTER(Columns)),
+        ("optimal_knn", ctypes.c_void_p),
+        ("optimal_radius", ctypes.c_void_p),
+        ("aux_on_device", ctypes.c_int32),
+        ("exception_capacity", ctypes.c_uint32),
+        ("exceptions", ctypes.c_void_p),
+        ("user_tag", ctypes.c_uint64),
+    ]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("n_exceptions", ctypes.c_uint32),
+        ("user_tag", ctypes.c_uint64),
+        ("submit_us", ctypes.c_double),
+        ("start_us", ctypes.c_double),
+        ("end_us", ctypes.c_double),
+        ("est_bytes", ctypes.c_uint64),
+        ("stats", RunStats),
+    ]
+
+
 def stage_dims(opts: StageOpts) -> list:
     """Output dimension names of one stage, in the library's order."""
     if opts.kind == STAGE_NORMAL:
@@ -190,5 +224,17 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_stage_noalloc.restype = ctypes.c_int
     lib.nbg_debug_kd_export.argtypes = [vp, vp] + [vp] * 9 + [ctypes.c_uint32]
     lib.nbg_debug_kd_export.restype = ctypes.c_int
+    lib.nbg_server_create.argtypes = [ctypes.POINTER(vp), i32, i32, u64]
+    lib.nbg_server_create.restype = ctypes.c_int
+    lib.nbg_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]
+    lib.nbg_server_submit.restype = ctypes.c_int
+    lib.nbg_server_wait.argtypes = [vp, ctypes.c_uint64, i32, ctypes.POINTER(RequestResult)]
+    lib.nbg_server_wait.restype = ctypes.c_int
+    lib.nbg_request_bytes.argtypes = [ctypes.POINTER(Request)]
+    lib.nbg_request_bytes.restype = u64
+    lib.nbg_server_last_error.argtypes = [vp]
+    lib.nbg_server_last_error.restype = ctypes.c_char_p
+    lib.nbg_server_destroy.argtypes = [vp]
+    lib.nbg_server_destroy.restype = ctypes.c_int
     _LIB = lib
     return lib

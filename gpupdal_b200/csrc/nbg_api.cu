@@ -45,6 +45,16 @@ std::atomic<uint64_t> g_launches{0};
 
 static size_t round_bytes(size_t bytes) { return bytes == 0 ? 256 : ((bytes + 255) / 256) * 256; }
 
+// Size class of a request: 256-byte granules up to 64 KiB, then eighth-octave
+// steps (at most 12.5% over the request).
+static size_t size_class(size_t bytes) {
+    bytes = round_bytes(bytes);
+    if (bytes <= (64u << 10)) return bytes;
+    size_t p = (size_t)1 << (63 - __builtin_clzll((unsigned long long)bytes));
+    const size_t step = p / 8;
+    return ((bytes + step - 1) / step) * step;
+}
+
 void ctx_trim(Context* ctx) {
     for (auto& kv : ctx->cache) cudaFree(kv.second);
     ctx->used -= std::min<uint64_t>(ctx->used, ctx->cached);
@@ -52,13 +62,17 @@ void ctx_trim(Context* ctx) {
     ctx->cached = 0;
 }
 
+// Device allocation through the context's cache: the smallest cached block
+// of at least the request's size class and at most twice it is reused, so
+// calls of varying sizes (a request stream) recycle their blocks.
 int ctx_alloc(Context* ctx, void** p, size_t bytes) {
-    bytes = round_bytes(bytes);
-    auto it = ctx->cache.find(bytes);
-    if (it != ctx->cache.end()) {
+    bytes = size_class(bytes);
+    auto it = ctx->cache.lower_bound(bytes);
+    if (it != ctx->cache.end() && it->first <= 2 * bytes) {
         *p = it->second;
+        ctx->live[*p] = it->first;
+        ctx->cached -= it->first;
         ctx->cache.erase(it);
-        ctx->cached -= bytes;
         return NBG_OK;
     }
     if (ctx->budget && ctx->used + bytes > ctx->budget) ctx_trim(ctx);
@@ -76,12 +90,19 @@ int ctx_alloc(Context* ctx, void** p, size_t bytes) {
         }
     }
     ctx->used += bytes;
+    ctx->live[*p] = bytes;
     return NBG_OK;
 }
 
 void ctx_free(Context* ctx, void* p, size_t bytes) {
     if (!p) return;
-    bytes = round_bytes(bytes);
+    auto it = ctx->live.find(p);
+    if (it != ctx->live.end()) {
+        bytes = it->second;
+        ctx->live.erase(it);
+    } else {
+        bytes = size_class(bytes);
+    }
     ctx->cache.emplace(bytes, p);
     ctx->cached += bytes;
 }

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <map>
 #include <mutex>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -47,11 +48,13 @@ struct Context {
     // device blocks released by earlier calls, kept for reuse by size
     std::multimap<size_t, void*> cache;
     uint64_t cached = 0;
+    std::unordered_map<void*, size_t> live;  // block sizes of handed-out blocks
 };
 
-// Device allocation through the context: reuses a cached block of the same
-// size, honours the HBM budget (cached blocks are released first when the
-// budget would be exceeded).  Returns NBG_OK, NBG_ERR_BUDGET or NBG_ERR_OOM.
+// Device allocation through the context: reuses a cached block of the
+// request's size class (up to twice its size), honours the HBM budget (cached
+// blocks are released first when the budget would be exceeded).  Returns
+// NBG_OK, NBG_ERR_BUDGET or NBG_ERR_OOM.
 int ctx_alloc(Context* ctx, void** p, size_t bytes);
 void ctx_free(Context* ctx, void* p, size_t bytes);
 void ctx_trim(Context* ctx);

@@ -215,3 +215,115 @@ class Tile:
             self.free()
         except Exception:
             pass
+
+
+class Server:
+    """The served form (nbg_server_*): requests are queued FIFO and admitted
+    onto `slots` workers while the HBM budget holds their footprint; admitted
+    requests overlap on the device.
+
+    submit() takes one tile's raw coordinates and its stages and returns a
+    ticket; wait() returns (outputs, exceptions, result) once it finished."""
+
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget: int = 0):
+        self.lib = abi.load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.nbg_server_create(ctypes.byref(h), int(device), int(slots), int(hbm_budget))
+        if rc != abi.NBG_OK:
+            raise NbgError(rc, "nbg_server_create failed")
+        self.h = h
+        self.device = device
+        self._pending = {}
+
+    def submit(self, x, y, z, stages, scale=(0.01, 0.01, 0.01), offset=(0.0, 0.0, 0.0),
+               optimal_knn=None, optimal_radius=None, out=None, device_out=False,
+               exception_capacity=None, tag=0):
+        on_device = not isinstance(x, np.ndarray)
+        if not on_device:
+            x, y, z = (np.ascontiguousarray(v, dtype=np.int32) for v in (x, y, z))
+        n = int(len(x))
+        ns = len(stages)
+        opts = (abi.StageOpts * ns)(*stages)
+        cols = (abi.Columns * ns)()
+        outs = []
+        for i, st in enumerate(stages):
+            nd = len(abi.stage_dims(st))
+            if out is not None:
+                buf = out[i]
+            elif device_out:
+                import torch
+                buf = torch.zeros((max(nd, 1), n), dtype=torch.float64, device=f"cuda:{self.device}")
+            else:
+                buf = np.zeros((max(nd, 1), n), dtype=np.float64)
+            outs.append(buf)
+            c = cols[i]
+            c.base = _dptr(buf).value
+            c.point_stride = 8
+            c.ndims = nd
+            c.on_device = 1 if device_out else 2
+            for d in range(nd):
+                c.offset[d] = d * n * 8
+        cap = exception_capacity if exception_capacity is not None else max(1024, n)
+        exc = (abi.RowException * cap)()
+        aux = []
+        if optimal_knn is not None:
+            aux = [np.ascontiguousarray(optimal_knn, dtype=np.float64),
+                   np.ascontiguousarray(optimal_radius, dtype=np.float64)]
+        r = abi.Request()
+        r.x, r.y, r.z = _dptr(x).value, _dptr(y).value, _dptr(z).value
+        r.n = n
+        for k in range(3):
+            r.scale[k] = scale[k]
+            r.offset[k] = offset[k]
+        r.on_device = int(on_device)
+        r.n_stages = ns
+        r.stages = opts
+        r.outputs = cols
+        r.optimal_knn = aux[0].ctypes.data if aux else None
+        r.optimal_radius = aux[1].ctypes.data if aux else None
+        r.aux_on_device = 0
+        r.exception_capacity = cap
+        r.exceptions = ctypes.addressof(exc)
+        r.user_tag = int(tag)
+        t = ctypes.c_uint64(0)
+        rc = self.lib.nbg_server_submit(self.h, ctypes.byref(r), ctypes.byref(t))
+        if rc != abi.NBG_OK:
+            raise NbgError(rc, self.lib.nbg_server_last_error(self.h).decode())
+        # everything the worker reads stays referenced until wait()
+        self._pending[t.value] = (x, y, z, opts, cols, outs, exc, aux, stages, r)
+        return t.value
+
+    def request_bytes(self, n, stages):
+        r = abi.Request()
+        r.n = int(n)
+        r.n_stages = len(stages)
+        cols = (abi.Columns * len(stages))()
+        for i, st in enumerate(stages):
+            cols[i].ndims = len(abi.stage_dims(st))
+        r.outputs = cols
+        return int(self.lib.nbg_request_bytes(ctypes.byref(r)))
+
+    def wait(self, ticket, timeout_ms=-1):
+        res = abi.RequestResult()
+        rc = self.lib.nbg_server_wait(self.h, int(ticket), int(timeout_ms), ctypes.byref(res))
+        if rc != abi.NBG_OK:
+            raise NbgError(rc, "nbg_server_wait")
+        x, y, z, opts, cols, outs, exc, aux, stages, r = self._pending.pop(ticket)
+        if res.status != abi.NBG_OK:
+            raise NbgError(res.status, self.lib.nbg_server_last_error(self.h).decode())
+        m = min(res.n_exceptions, len(exc))
+        ex = np.zeros(m, dtype=[("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8)])
+        for j in range(m):
+            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code)
+        return [o[: len(abi.stage_dims(s))] for o, s in zip(outs, stages)], ex, res
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nbg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -197,6 +197,65 @@ int nbg_neighbor_sets(nbg_context* ctx, nbg_tile* tile, int32_t knn,
                       uint32_t* ids_out, int32_t ids_on_device,
                       nbg_run_stats* stats, void* stream);
 
+/* Served form ------------------------------------------------------------
+ * A request loop over one device: requests (one tile + its stages each) are
+ * queued FIFO and admitted while a slot is free and the HBM budget holds the
+ * request's estimated footprint; each slot is a host worker with its own
+ * context and stream, so admitted requests overlap on the device (continuous
+ * batching: a request that arrives while others run starts as soon as a slot
+ * and memory free up).  The reference has no counterpart (its stages run one
+ * view at a time, pdal/Stage.hpp:419-497); each request does exactly what
+ * nbg_tile_upload + nbg_run + nbg_tile_free do, so results are the same
+ * alone and in any mix.  The caller's buffers must stay valid until the
+ * request completes. */
+typedef struct nbg_request {
+    const int32_t* x;            /* raw coordinates, caller order           */
+    const int32_t* y;
+    const int32_t* z;
+    uint64_t n;
+    double scale[3];
+    double offset[3];
+    int32_t on_device;           /* x/y/z are device pointers               */
+    int32_t n_stages;
+    const nbg_stage_opts* stages;
+    const nbg_columns* outputs;  /* one per stage, as nbg_run               */
+    const double* optimal_knn;   /* may be null                             */
+    const double* optimal_radius;
+    int32_t aux_on_device;
+    uint32_t exception_capacity;
+    nbg_row_exception* exceptions;
+    uint64_t user_tag;
+} nbg_request;
+
+typedef struct nbg_request_result {
+    int32_t status;              /* NBG_OK or the run's error code          */
+    uint32_t n_exceptions;
+    uint64_t user_tag;
+    double submit_us;            /* host clock, microseconds since creation */
+    double start_us;             /* admitted to a slot                      */
+    double end_us;               /* results in the caller's buffers         */
+    uint64_t est_bytes;          /* footprint the admission charged         */
+    nbg_run_stats stats;
+} nbg_request_result;
+
+typedef struct nbg_server nbg_server;
+
+/* slots: concurrent requests (host workers); hbm_budget_bytes 0 = no limit */
+int nbg_server_create(nbg_server** server, int32_t device, int32_t slots,
+                      uint64_t hbm_budget_bytes);
+/* Queues a request; *ticket identifies it.  NBG_ERR_BUDGET when the request
+ * alone exceeds the budget. */
+int nbg_server_submit(nbg_server* server, const nbg_request* request, uint64_t* ticket);
+/* Waits up to timeout_ms (< 0: no limit) for a request; NBG_ERR_TIMEOUT if
+ * it has not finished.  A finished request's result is returned once. */
+int nbg_server_wait(nbg_server* server, uint64_t ticket, int32_t timeout_ms,
+                    nbg_request_result* result);
+/* Estimated device footprint of a request (what admission charges). */
+uint64_t nbg_request_bytes(const nbg_request* request);
+const char* nbg_server_last_error(const nbg_server* server);
+/* Waits for every queued request, then stops the workers. */
+int nbg_server_destroy(nbg_server* server);
+
 /* No-allocation entry point.  This function has no counterpart in the
  * reference; it exists for callers that cannot allocate device memory when
  * they need results: code running inside another framework's allocator or

@@ -49,6 +49,9 @@ int main(void) {
   printf("%zu %zu %zu %zu\n", offsetof(nbg_stage_opts, viewpoint),
          offsetof(nbg_stage_opts, feature_mask), offsetof(nbg_columns, offset),
          offsetof(nbg_run_stats, grid_ms));
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(nbg_request), sizeof(nbg_request_result),
+         offsetof(nbg_request, stages), offsetof(nbg_request, user_tag),
+         offsetof(nbg_request_result, stats), offsetof(nbg_run_stats, kd_build_ms));
   return 0;
 }
 """
@@ -64,6 +67,10 @@ int main(void) {
                      ctypes.sizeof(abi.RowException), ctypes.sizeof(abi.RunStats)]
     assert offs == [abi.StageOpts.viewpoint.offset, abi.StageOpts.feature_mask.offset,
                     abi.Columns.offset.offset, abi.RunStats.grid_ms.offset]
+    served = [int(v) for v in lines[2].split()]
+    assert served == [ctypes.sizeof(abi.Request), ctypes.sizeof(abi.RequestResult),
+                      abi.Request.stages.offset, abi.Request.user_tag.offset,
+                      abi.RequestResult.stats.offset, abi.RunStats.kd_build_ms.offset]
 
 
 def test_loader_fails_loudly_without_the_library(tmp_path):
