@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--knn", type=int, default=16)
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--served-requests", type=int, default=64)
+    ap.add_argument("--served-rate", type=float, default=20.0)
+    ap.add_argument("--served-slots", type=int, default=4)
+    ap.add_argument("--no-served", action="store_true")
     return ap.parse_args()
 
 
@@ -153,6 +157,39 @@ def cpu_reference(x, y, z, knn, sample, kind=None):
                                     f"{side / 100:.0f} m) of the same tile: KD build + "
                                     f"eigenvalues + normal, {threads} threads",
             "seconds": dt}
+
+
+def served_leg(ctx, args):
+    """The served stream (bounded sample): sequential plain per-tile calls
+    against the request loop, all requests at once (capacity) and at Poisson
+    arrivals (latency)."""
+    from gpupdal_b200 import served
+    from gpupdal_b200.native import Server
+    reqs = served.make_stream(args.served_requests, seed=1000)
+    pts = sum(len(r["x"]) for r in reqs)
+    served.run_plain(ctx, reqs[:4])  # warm the plain context's caches
+    plain_s = sum(served.run_plain(ctx, reqs))
+    srv = Server(0, slots=args.served_slots, hbm_budget=120 * 10**9)
+    try:
+        served.run_served(srv, reqs[:8])  # warm-up: worker contexts' caches
+        cap_s, cap_lat, _ = served.run_served(srv, reqs)
+        rate_s, lat, res = served.run_served(srv, reqs, rate=args.served_rate, seed=1)
+    finally:
+        srv.close()
+    lat_ms = np.sort(np.array(lat) * 1e3)
+    return {
+        "stream": (f"{len(reqs)} requests, sizes log-uniform 10k-8M of the mixture (subsamples of "
+                   "one 8M cloud, seed 1000), knn in {8,16,32,64}, normal/eigenvalues/"
+                   "covariancefeatures(all) in equal shares; host buffers in and out"),
+        "points": pts,
+        "plain_mpts_s": pts / plain_s / 1e6,
+        "served_mpts_s": pts / cap_s / 1e6,
+        "served_vs_plain": plain_s / cap_s,
+        "slots": args.served_slots, "hbm_budget_gb": 120,
+        "rate_req_s": args.served_rate,
+        "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+        "rate_mpts_s": pts / rate_s / 1e6,
+    }
 
 
 def dist_setup():
@@ -296,10 +333,12 @@ def main():
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None,
-                     "kernel": "knn_fused_kernel", "peak_source": peak_kind,
+                     "kernel": "knn_select_kernel+knn_finish_kernel", "peak_source": peak_kind,
                      "bytes_per_point": BYTES_PER_POINT},
         "clocks": clk,
     }
+    if ws == 1 and not args.no_served:
+        line["served"] = served_leg(ctx, args)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(x, y, z, args.knn, args.cpu_sample)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <new>
 #include <string>
 #include <vector>
@@ -105,6 +106,108 @@ void ctx_free(Context* ctx, void* p, size_t bytes) {
     }
     ctx->cache.emplace(bytes, p);
     ctx->cached += bytes;
+}
+
+// ---------------------------------------------------------------------------
+// host copies
+static constexpr size_t kBounce = (size_t)32 << 20;
+
+static bool host_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+static int bounce_init(Context* ctx) {
+    if (ctx->bounce_ready) return NBG_OK;
+    for (int i = 0; i < 2; ++i) {
+        if (cudaHostAlloc((void**)&ctx->bounce[i], kBounce, cudaHostAllocDefault) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->bev[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, NBG_ERR_OOM, "pinned bounce buffer");
+        }
+    }
+    ctx->bounce_ready = true;
+    return NBG_OK;
+}
+
+// memcpy with up to 4 host threads for large blocks
+static void par_memcpy(void* dst, const void* src, size_t bytes) {
+    const size_t per = (size_t)8 << 20;
+    const int nt = (int)std::min<size_t>(4, (bytes + per - 1) / per);
+    if (nt <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t part = (bytes + nt - 1) / nt;
+    for (int i = 1; i < nt; ++i) {
+        const size_t off = part * i;
+        if (off >= bytes) break;
+        th.emplace_back([=] { std::memcpy((char*)dst + off, (const char*)src + off,
+                                          std::min(part, bytes - off)); });
+    }
+    std::memcpy(dst, src, std::min(part, bytes));
+    for (auto& t : th) t.join();
+}
+
+int host_to_device(Context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    if (!bytes) return NBG_OK;
+    if (bytes < ((size_t)1 << 20) || host_pinned(src)) {
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
+        return e ? cuda_fail(ctx, e, "host to device copy") : NBG_OK;
+    }
+    int rc = bounce_init(ctx);
+    if (rc) return rc;
+    const size_t nch = (bytes + kBounce - 1) / kBounce;
+    for (size_t k = 0; k < nch; ++k) {
+        const int b = (int)(k & 1);
+        const size_t off = k * kBounce, len = std::min(kBounce, bytes - off);
+        // the copy that last read this buffer must be done
+        if (cudaEventSynchronize(ctx->bev[b]) != cudaSuccess) return cuda_fail(ctx, cudaGetLastError(), "bounce");
+        par_memcpy(ctx->bounce[b], (const char*)src + off, len);
+        cudaError_t e = cudaMemcpyAsync((char*)dst + off, ctx->bounce[b], len, cudaMemcpyHostToDevice, stream);
+        if (!e) e = cudaEventRecord(ctx->bev[b], stream);
+        if (e) return cuda_fail(ctx, e, "host to device copy");
+    }
+    return NBG_OK;
+}
+
+int device_to_host(Context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    if (!bytes) return NBG_OK;
+    if (bytes < ((size_t)1 << 20) || host_pinned(dst)) {
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream);
+        if (!e) e = cudaStreamSynchronize(stream);
+        return e ? cuda_fail(ctx, e, "device to host copy") : NBG_OK;
+    }
+    int rc = bounce_init(ctx);
+    if (rc) return rc;
+    const size_t nch = (bytes + kBounce - 1) / kBounce;
+    auto issue = [&](size_t k) -> cudaError_t {
+        const int b = (int)(k & 1);
+        const size_t off = k * kBounce, len = std::min(kBounce, bytes - off);
+        cudaError_t e = cudaMemcpyAsync(ctx->bounce[b], (const char*)src + off, len,
+                                        cudaMemcpyDeviceToHost, stream);
+        if (!e) e = cudaEventRecord(ctx->bev[b], stream);
+        return e;
+    };
+    // previous users of the buffers (host-to-device chunks) must be done
+    for (int b = 0; b < 2; ++b)
+        if (cudaEventSynchronize(ctx->bev[b]) != cudaSuccess) return cuda_fail(ctx, cudaGetLastError(), "bounce");
+    cudaError_t e = issue(0);
+    for (size_t k = 0; k < nch && !e; ++k) {
+        if (k + 1 < nch) e = issue(k + 1);
+        if (e) break;
+        const int b = (int)(k & 1);
+        e = cudaEventSynchronize(ctx->bev[b]);
+        if (e) break;
+        const size_t off = k * kBounce, len = std::min(kBounce, bytes - off);
+        par_memcpy((char*)dst + off, ctx->bounce[b], len);
+    }
+    return e ? cuda_fail(ctx, e, "device to host copy") : NBG_OK;
 }
 
 static int dev_alloc(Context* ctx, void** p, size_t bytes, uint64_t* account) {
@@ -284,6 +387,12 @@ int nbg_destroy(nbg_context* h) {
         for (int i = 0; i < 2; ++i) cudaEventDestroy(ctx->xev[i]);
     }
     if (ctx->side) cudaStreamDestroy(ctx->side);
+    if (ctx->bounce_ready) {
+        for (int i = 0; i < 2; ++i) {
+            cudaFreeHost(ctx->bounce[i]);
+            cudaEventDestroy(ctx->bev[i]);
+        }
+    }
     delete h;
     return NBG_OK;
 }
@@ -343,14 +452,21 @@ int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const in
         return rc;
     }
     if (n) {
-        cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-        cudaError_t e = cudaMemcpyAsync(t->x, x, n * 4, kind, stream);
-        if (!e) e = cudaMemcpyAsync(t->y, y, n * 4, kind, stream);
-        if (!e) e = cudaMemcpyAsync(t->z, z, n * 4, kind, stream);
-        if (e) {
+        int urc = NBG_OK;
+        if (on_device) {
+            cudaError_t e = cudaMemcpyAsync(t->x, x, n * 4, cudaMemcpyDeviceToDevice, stream);
+            if (!e) e = cudaMemcpyAsync(t->y, y, n * 4, cudaMemcpyDeviceToDevice, stream);
+            if (!e) e = cudaMemcpyAsync(t->z, z, n * 4, cudaMemcpyDeviceToDevice, stream);
+            if (e) urc = cuda_fail(ctx, e, "coordinate upload");
+        } else {
+            urc = host_to_device(ctx, t->x, x, n * 4, stream);
+            if (!urc) urc = host_to_device(ctx, t->y, y, n * 4, stream);
+            if (!urc) urc = host_to_device(ctx, t->z, z, n * 4, stream);
+        }
+        if (urc) {
             tile_release(ctx, t);
             delete th;
-            return cuda_fail(ctx, e, "coordinate upload");
+            return urc;
         }
     }
     *out = th;
@@ -520,14 +636,15 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             // rows the reference skips keep the caller's values
             for (int d = 0; d < outputs[s].ndims; ++d) {
                 const nbg_columns& u = outputs[s];
-                cudaError_t e;
-                if (u.point_stride == 8)
-                    e = cudaMemcpyAsync(hout[s].dev + (size_t)d * n * 8, (char*)u.base + u.offset[d],
-                                        n * 8, cudaMemcpyHostToDevice, stream);
-                else
-                    e = cudaMemcpy2DAsync(hout[s].dev + (size_t)d * n * 8, 8,
-                                          (char*)u.base + u.offset[d], u.point_stride, 8, n,
-                                          cudaMemcpyHostToDevice, stream);
+                if (u.point_stride == 8) {
+                    rc = host_to_device(ctx, hout[s].dev + (size_t)d * n * 8,
+                                        (char*)u.base + u.offset[d], n * 8, stream);
+                    if (rc) { cleanup(); return rc; }
+                    continue;
+                }
+                cudaError_t e = cudaMemcpy2DAsync(hout[s].dev + (size_t)d * n * 8, 8,
+                                                  (char*)u.base + u.offset[d], u.point_stride, 8, n,
+                                                  cudaMemcpyHostToDevice, stream);
                 if (e) { cleanup(); return cuda_fail(ctx, e, "output staging"); }
             }
         }
@@ -538,8 +655,9 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         rc = dev_alloc(ctx, (void**)&aux_dev[0], n * 8, nullptr);
         if (!rc) rc = dev_alloc(ctx, (void**)&aux_dev[1], n * 8, nullptr);
         if (rc) { cleanup(); return rc; }
-        cudaMemcpyAsync(aux_dev[0], optimal_knn, n * 8, cudaMemcpyHostToDevice, stream);
-        cudaMemcpyAsync(aux_dev[1], optimal_radius, n * 8, cudaMemcpyHostToDevice, stream);
+        rc = host_to_device(ctx, aux_dev[0], optimal_knn, n * 8, stream);
+        if (!rc) rc = host_to_device(ctx, aux_dev[1], optimal_radius, n * 8, stream);
+        if (rc) { cleanup(); return rc; }
         kopt = aux_dev[0];
         ropt = aux_dev[1];
     }
@@ -680,22 +798,22 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     }
     // results back to host layouts
     if (packed) {
-        cudaError_t e = cudaMemcpyAsync(outputs[0].base, packed_dev, packed_bytes,
-                                        cudaMemcpyDeviceToHost, stream);
-        if (e) { cleanup(); return cuda_fail(ctx, e, "output copy"); }
+        rc = device_to_host(ctx, outputs[0].base, packed_dev, packed_bytes, stream);
+        if (rc) { cleanup(); return rc; }
     }
     for (int s = 0; s < n_stages; ++s) {
         if (!hout[s].dev) continue;
         const nbg_columns& u = outputs[s];
         for (int d = 0; d < u.ndims; ++d) {
-            cudaError_t e;
-            if (u.point_stride == 8)
-                e = cudaMemcpyAsync((char*)u.base + u.offset[d], hout[s].dev + (size_t)d * n * 8, n * 8,
-                                    cudaMemcpyDeviceToHost, stream);
-            else
-                e = cudaMemcpy2DAsync((char*)u.base + u.offset[d], u.point_stride,
-                                      hout[s].dev + (size_t)d * n * 8, 8, 8, n,
-                                      cudaMemcpyDeviceToHost, stream);
+            if (u.point_stride == 8) {
+                rc = device_to_host(ctx, (char*)u.base + u.offset[d], hout[s].dev + (size_t)d * n * 8,
+                                    n * 8, stream);
+                if (rc) { cleanup(); return rc; }
+                continue;
+            }
+            cudaError_t e = cudaMemcpy2DAsync((char*)u.base + u.offset[d], u.point_stride,
+                                              hout[s].dev + (size_t)d * n * 8, 8, 8, n,
+                                              cudaMemcpyDeviceToHost, stream);
             if (e) { cleanup(); return cuda_fail(ctx, e, "output copy"); }
         }
     }
@@ -788,7 +906,7 @@ extern "C" int nbg_neighbor_sets(nbg_context* h, nbg_tile* th, int32_t knn, uint
         }
         if (!rc && !e) rc = kd_neighbor_rows(ctx, t, K, ctx->exact_rows, cnt[0], dev_ids, stream);
     }
-    if (!rc && !e && !ids_on_device) e = cudaMemcpyAsync(ids_out, dev_ids, bytes, cudaMemcpyDeviceToHost, stream);
+    if (!rc && !e && !ids_on_device) rc = device_to_host(ctx, ids_out, dev_ids, bytes, stream);
     if (!e) e = cudaStreamSynchronize(stream);
     if (!ids_on_device) dev_free(ctx, dev_ids, bytes);
     if (stats) {

@@ -49,7 +49,20 @@ struct Context {
     std::multimap<size_t, void*> cache;
     uint64_t cached = 0;
     std::unordered_map<void*, size_t> live;  // block sizes of handed-out blocks
+    // pinned bounce buffers for copies to and from pageable host memory
+    char* bounce[2] = {nullptr, nullptr};
+    cudaEvent_t bev[2];
+    bool bounce_ready = false;
 };
+
+// Copies between device memory and host memory.  Pinned (or registered) host
+// memory is copied directly; pageable host memory goes through the
+// context's pinned bounce buffers in 32 MiB chunks, the device copy of one
+// chunk overlapping the host-side memcpy (several threads) of the previous.
+// Both return once the host side is complete (d2h) or the source may be
+// reused (h2d).
+int host_to_device(Context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t stream);
+int device_to_host(Context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t stream);
 
 // Device allocation through the context: reuses a cached block of the
 // request's size class (up to twice its size), honours the HBM budget (cached
