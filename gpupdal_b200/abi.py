@@ -112,6 +112,23 @@ class RunStats(ctypes.Structure):
     ]
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [
+        ("tile", ctypes.c_void_p),
+        ("n_stages", ctypes.c_int32),
+        ("exception_capacity", ctypes.c_uint32),
+        ("stages", ctypes.POINTER(StageOpts)),
+        ("outputs", ctypes.POINTER(Columns)),
+        ("optimal_knn", ctypes.c_void_p),
+        ("optimal_radius", ctypes.c_void_p),
+        ("exceptions", ctypes.c_void_p),
+        ("n_exceptions", ctypes.POINTER(ctypes.c_uint32)),
+    ]
+
+
+BATCH_GRAPH = 1
+
+
 class Request(ctypes.Structure):
     _fields_ = [
         ("x", ctypes.c_void_p),
@@ -224,6 +241,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_stage_noalloc.restype = ctypes.c_int
     lib.nbg_debug_kd_export.argtypes = [vp, vp] + [vp] * 9 + [ctypes.c_uint32]
     lib.nbg_debug_kd_export.restype = ctypes.c_int
+    lib.nbg_run_batch.argtypes = [vp, ctypes.POINTER(BatchItem), i32, ctypes.c_uint32,
+                                  ctypes.POINTER(RunStats), vp]
+    lib.nbg_run_batch.restype = ctypes.c_int
     lib.nbg_server_create.argtypes = [ctypes.POINTER(vp), i32, i32, u64]
     lib.nbg_server_create.restype = ctypes.c_int
     lib.nbg_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]

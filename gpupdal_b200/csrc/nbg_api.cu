@@ -18,16 +18,10 @@
 
 #include "nbg_internal.h"
 
-struct nbg_context {
-    nbg::Context c;
-};
-struct nbg_tile {
-    nbg::Tile t;
-};
 
 namespace nbg {
 
-static int fail(Context* c, int code, const std::string& msg) {
+int fail(Context* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
 }
@@ -218,7 +212,7 @@ static int dev_alloc(Context* ctx, void** p, size_t bytes, uint64_t* account) {
 
 static void dev_free(Context* ctx, void* p, size_t bytes) { ctx_free(ctx, p, bytes); }
 
-static int ensure_scratch(Context* ctx, uint64_t n, uint64_t ex_cap) {
+int ensure_scratch(Context* ctx, uint64_t n, uint64_t ex_cap) {
     if (ctx->sums_cap < n) {
         if (ctx->sums) dev_free(ctx, ctx->sums, ctx->sums_cap * sizeof(RowSums));
         ctx->sums = nullptr;
@@ -386,6 +380,7 @@ int nbg_destroy(nbg_context* h) {
         for (int i = 0; i < 10; ++i) cudaEventDestroy(ctx->ev[i]);
         for (int i = 0; i < 2; ++i) cudaEventDestroy(ctx->xev[i]);
     }
+    batch_release(ctx);
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->bounce_ready) {
         for (int i = 0; i < 2; ++i) {
@@ -513,6 +508,43 @@ static int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
     return NBG_OK;
 }
 
+int validate_stages(Context* ctx, const nbg_stage_opts* stages, int n_stages,
+                    const nbg_columns* outputs, bool* need_aux) {
+    *need_aux = false;
+    for (int s = 0; s < n_stages; ++s) {
+        const nbg_stage_opts& o = stages[s];
+        if (o.kind < 1 || o.kind > 3) return fail(ctx, NBG_ERR_INVALID, "unknown stage kind");
+        if (o.knn < 0 || o.knn > 64)
+            return fail(ctx, NBG_ERR_INVALID, "knn must be in [0, 64]");
+        if (o.kind != NBG_STAGE_NORMAL && o.stride != 1 && o.stride != 0)
+            return fail(ctx, NBG_ERR_UNSUPPORTED, "stride > 1 is not supported");
+        if (o.kind == NBG_STAGE_COVARIANCEFEATURES && o.optimized)
+            return fail(ctx, NBG_ERR_UNSUPPORTED, "optimized is not supported");
+        if (o.kind == NBG_STAGE_COVARIANCEFEATURES &&
+            (o.mode < NBG_MODE_RAW || o.mode > NBG_MODE_NORMALIZED))
+            return fail(ctx, NBG_ERR_INVALID, "invalid mode");
+        if (outputs[s].ndims != ndims_of(o))
+            return fail(ctx, NBG_ERR_INVALID, "output ndims does not match the stage");
+        if (o.kind == NBG_STAGE_COVARIANCEFEATURES && (o.feature_mask & NBG_FEAT_DENSITY))
+            *need_aux = true;
+    }
+    return NBG_OK;
+}
+
+void fill_stage(StageDev& d, const nbg_stage_opts& o, const nbg_columns& c) {
+    d.kind = o.kind;
+    d.always_up = o.always_up;
+    d.has_viewpoint = o.has_viewpoint;
+    d.normalize = o.normalize;
+    for (int k = 0; k < 3; ++k) d.viewpoint[k] = o.viewpoint[k];
+    d.feature_mask = o.feature_mask & NBG_FEAT_ALL;
+    d.mode = o.mode;
+    d.ndims = c.ndims;
+    d.base = (char*)c.base;
+    d.point_stride = c.point_stride;
+    for (int k = 0; k < NBG_MAX_DIMS; ++k) d.offset[k] = c.offset[k];
+}
+
 struct HostOut {
     const nbg_columns* user;
     char* dev = nullptr;  // device staging (host outputs only)
@@ -538,23 +570,8 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     if (n_stages < 0 || n_stages > NBG_MAX_STAGES || (n_stages && (!stages || !outputs)))
         return fail(ctx, NBG_ERR_INVALID, "bad stage array");
     bool need_aux = false;
-    for (int s = 0; s < n_stages; ++s) {
-        const nbg_stage_opts& o = stages[s];
-        if (o.kind < 1 || o.kind > 3) return fail(ctx, NBG_ERR_INVALID, "unknown stage kind");
-        if (o.knn < 0 || o.knn > 64)
-            return fail(ctx, NBG_ERR_INVALID, "knn must be in [0, 64]");
-        if (o.kind != NBG_STAGE_NORMAL && o.stride != 1 && o.stride != 0)
-            return fail(ctx, NBG_ERR_UNSUPPORTED, "stride > 1 is not supported");
-        if (o.kind == NBG_STAGE_COVARIANCEFEATURES && o.optimized)
-            return fail(ctx, NBG_ERR_UNSUPPORTED, "optimized is not supported");
-        if (o.kind == NBG_STAGE_COVARIANCEFEATURES &&
-            (o.mode < NBG_MODE_RAW || o.mode > NBG_MODE_NORMALIZED))
-            return fail(ctx, NBG_ERR_INVALID, "invalid mode");
-        if (outputs[s].ndims != ndims_of(o))
-            return fail(ctx, NBG_ERR_INVALID, "output ndims does not match the stage");
-        if (o.kind == NBG_STAGE_COVARIANCEFEATURES && (o.feature_mask & NBG_FEAT_DENSITY))
-            need_aux = true;
-    }
+    int vrc = validate_stages(ctx, stages, n_stages, outputs, &need_aux);
+    if (vrc) return vrc;
     if (need_aux && (!optimal_knn || !optimal_radius))
         return fail(ctx, NBG_ERR_INVALID, "Density needs OptimalKNN and OptimalRadius");
     const uint64_t n = t->n;
@@ -695,19 +712,8 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         for (int i = 0; i < g.nstages; ++i) {
             const int s = gr[i];
             const nbg_stage_opts& o = stages[s];
-            StageDev& d = g.st[i];
             g.stage_index[i] = s;
-            d.kind = o.kind;
-            d.always_up = o.always_up;
-            d.has_viewpoint = o.has_viewpoint;
-            d.normalize = o.normalize;
-            for (int k = 0; k < 3; ++k) d.viewpoint[k] = o.viewpoint[k];
-            d.feature_mask = o.feature_mask & NBG_FEAT_ALL;
-            d.mode = o.mode;
-            d.ndims = dcols[s].ndims;
-            d.base = (char*)dcols[s].base;
-            d.point_stride = dcols[s].point_stride;
-            for (int k = 0; k < NBG_MAX_DIMS; ++k) d.offset[k] = dcols[s].offset[k];
+            fill_stage(g.st[i], o, dcols[s]);
             if (o.kind == NBG_STAGE_NORMAL && !o.always_up && !o.has_viewpoint) g.sign_exact = 1;
         }
         g.resolve_count = ctx->counters + 5;

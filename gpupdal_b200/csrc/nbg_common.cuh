@@ -92,6 +92,31 @@ struct Transform {
     double offset[3];
 };
 
+// Arguments of the query kernels for one tile and one stage group.
+struct QueryArgs {
+    GridView gv;
+    const GridParams* gp;
+    uint64_t n;
+    int K;
+    int rmax;
+    StageGroup grp;
+    Transform tf;
+    ExceptionSink ex;
+    uint32_t* exact_rows;
+    uint32_t* counters;  // [0] exact rows, [1] tie rows, [2] incomplete rows, [4] tie list
+    uint32_t* ids_out;   // neighbour-set export (null in the fused path)
+    uint2* ties;         // tie list {id, (D_K - 2^23 bias) | R << 24}; null: ties go to exact_rows
+    uint32_t tie_cap;
+    RowSums* sums;       // split form: per sorted position, read by knn_finish_kernel
+};
+
+// One tile of a batch: its query arguments and the first work item (block of
+// queries) it owns in the batch's queue.
+struct BatchJob {
+    QueryArgs q;
+    uint64_t first;
+};
+
 // ---------------------------------------------------------------------------
 // The reference's coordinate, fl(fl(raw*scale) + offset), with no contraction.
 __device__ __forceinline__ double ref_coord(int32_t raw, double s, double o) {

@@ -151,11 +151,14 @@ __global__ void col_base_kernel(const GridParams* __restrict__ gpp, const uint32
     }
 }
 
+// Table entry of every point and the per-entry histogram.  An entry at or
+// beyond `entries` (a table too small for this grid: only the build that does
+// not read the table size first can see one) sets bit 2 of cap_hit and is
+// dropped; the caller rebuilds such a grid.
 __global__ void cell_count_kernel(const int32_t* __restrict__ x, const int32_t* __restrict__ y,
-                                  const int32_t* __restrict__ z, uint64_t n,
-                                  const GridParams* __restrict__ gpp,
+                                  const int32_t* __restrict__ z, uint64_t n, GridParams* gpp,
                                   const int4* __restrict__ colinfo, uint32_t* __restrict__ keys,
-                                  uint32_t* __restrict__ counts) {
+                                  uint32_t* __restrict__ counts, uint64_t entries) {
     const GridParams g = *gpp;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
@@ -164,6 +167,11 @@ __global__ void cell_count_kernel(const int32_t* __restrict__ x, const int32_t* 
         const int cz = (int)((uint32_t)(z[i] - g.minz) / (uint32_t)g.cell);
         const int4 ci = colinfo[cy * (uint32_t)g.gx + cx];
         const uint32_t key = (uint32_t)ci.x + (uint32_t)(cz - ci.y);
+        if ((uint64_t)key >= entries) {
+            keys[i] = 0xFFFFFFFFu;
+            atomicOr(&gpp->cap_hit, 2u);
+            continue;
+        }
         keys[i] = key;
         atomicAdd(&counts[key], 1u);
     }
@@ -177,6 +185,7 @@ __global__ void cell_scatter_kernel(const int32_t* __restrict__ x, const int32_t
     const GridParams g = *gpp;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
+        if (keys[i] == 0xFFFFFFFFu) continue;
         const uint32_t pos = atomicAdd(&cursor[keys[i]], 1u);
         float4 r;
         r.x = (float)(x[i] - g.minx);
@@ -234,7 +243,7 @@ int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
     if (cudaMemsetAsync(t->cstart, 0, ((size_t)T + 1) * sizeof(uint32_t), stream))
         return NBG_ERR_CUDA;
     cell_count_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->colinfo, t->keys,
-                                              t->cstart);
+                                              t->cstart, (uint64_t)T + 1);
     tmp = t->grid_tmp_bytes;
     if (cub::DeviceScan::ExclusiveSum(t->grid_tmp, tmp, t->cstart, t->cstart, (int)(T + 1),
                                       stream))
@@ -246,6 +255,46 @@ int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
                                                 t->sorted);
     // bbox (2), config, col init, zrange, extent, scan (2), bases, count, scan (2), scatter
     NBG_LAUNCHED(13);
+    return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+}
+
+// The same build without reading the table size on the host (no
+// synchronisation, so it can be captured in a CUDA graph): the histogram and
+// its scan cover the whole table capacity.  A grid whose table would not fit
+// sets bit 2 of cap_hit; the caller rebuilds it with build_grid.
+int build_grid_async(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
+    const uint64_t n = t->n;
+    const int sms = ctx->sm_count;
+    const int nb = grid_blocks(n, 256, sms);
+    const uint64_t entries = t->table_cap - 1;  // cstart needs entries + 1 slots
+    bbox_init_kernel<<<1, 32, 0, stream>>>(t->bbox);
+    bbox_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->bbox);
+    grid_config_kernel<<<1, 1, 0, stream>>>(t->bbox, n, k1, t->cell_factor, t->cols_cap,
+                                            t->fixed_cell, t->gp);
+    const int cb = grid_blocks(t->cols_cap + 1, 256, sms);
+    col_init_kernel<<<cb, 256, 0, stream>>>((uint32_t)t->cols_cap, t->colinfo);
+    col_zrange_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->colinfo);
+    col_extent_kernel<<<cb, 256, 0, stream>>>(t->gp, t->colinfo, t->ext);
+    size_t tmp = t->grid_tmp_bytes;
+    if (cub::DeviceScan::ExclusiveSum(t->grid_tmp, tmp, t->ext, t->ext, (int)(t->cols_cap + 1),
+                                      stream))
+        return NBG_ERR_CUDA;
+    col_base_kernel<<<cb, 256, 0, stream>>>(t->gp, t->ext, t->colinfo, t->table_dev);
+    if (cudaMemsetAsync(t->cstart, 0, (size_t)(entries + 1) * sizeof(uint32_t), stream))
+        return NBG_ERR_CUDA;
+    cell_count_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->colinfo, t->keys,
+                                              t->cstart, entries);
+    tmp = t->grid_tmp_bytes;
+    if (cub::DeviceScan::ExclusiveSum(t->grid_tmp, tmp, t->cstart, t->cstart, (int)(entries + 1),
+                                      stream))
+        return NBG_ERR_CUDA;
+    if (cudaMemcpyAsync(t->cursor, t->cstart, (size_t)(entries + 1) * sizeof(uint32_t),
+                        cudaMemcpyDeviceToDevice, stream))
+        return NBG_ERR_CUDA;
+    cell_scatter_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->keys, t->cursor,
+                                                t->sorted);
+    NBG_LAUNCHED(13);
+    t->table_size = entries;
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
 }
 

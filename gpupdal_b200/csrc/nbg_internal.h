@@ -105,6 +105,12 @@ struct Tile {
 };
 
 int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream);
+int build_grid_async(Context* ctx, Tile* t, int k1, cudaStream_t stream);
+int fail(Context* c, int code, const std::string& msg);
+int validate_stages(Context* ctx, const nbg_stage_opts* stages, int n_stages,
+                    const nbg_columns* outputs, bool* need_aux);
+void fill_stage(StageDev& d, const nbg_stage_opts& o, const nbg_columns& c);
+int ensure_scratch(Context* ctx, uint64_t n, uint64_t ex_cap);
 size_t grid_temp_bytes(uint64_t items);
 int grid_grow_table(Context* ctx, Tile* t, uint64_t entries);
 GridView grid_view(const Tile* t);
@@ -157,4 +163,15 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
                          uint32_t* exact_rows, uint32_t* counters, uint2* ties, uint32_t tie_cap,
                          cudaStream_t stream);
 
+// Batched form: the context's batch scratch and cached graph (nbg_batch.cu).
+void batch_release(Context* ctx);
+
 }  // namespace nbg
+
+// The C ABI's opaque handles.
+struct nbg_context {
+    nbg::Context c;
+};
+struct nbg_tile {
+    nbg::Tile t;
+};

@@ -22,6 +22,8 @@
 // Distinct integer distances order points exactly as the reference's FP64
 // distances do (the FP64 rounding error is far below one raw unit^2), so a
 // row with no boundary tie has exactly the reference's neighbour set.
+#include <algorithm>
+
 #include "nbg_common.cuh"
 #include "nbg_internal.h"
 
@@ -208,22 +210,6 @@ struct CollectFn {
     }
 };
 
-struct QueryArgs {
-    GridView gv;
-    const GridParams* gp;
-    uint64_t n;
-    int K;
-    int rmax;
-    StageGroup grp;
-    Transform tf;
-    ExceptionSink ex;
-    uint32_t* exact_rows;
-    uint32_t* counters;  // [0] exact rows, [1] tie rows, [2] incomplete rows, [4] tie list
-    uint32_t* ids_out;   // neighbour-set export (null in the fused path)
-    uint2* ties;         // tie list {id, (D_K - 2^23 bias) | R << 24}; null: ties go to exact_rows
-    uint32_t tie_cap;
-    RowSums* sums;       // split form: per sorted position, read by knn_finish_kernel
-};
 
 // A row that cannot finish on the grid: a boundary tie goes to the tie list
 // (its K-th distance and final ring kept for the order resolver), everything
@@ -326,9 +312,7 @@ __global__ void __launch_bounds__(128) knn_fused_kernel(const QueryArgs a) {
 // Split form, pass 1 + pass 2: the row's exact neighbourhood sums, in sorted
 // order (cnt = 0 marks a row handed to the exact path).
 template <int KS>
-__global__ void __launch_bounds__(128) knn_select_kernel(const QueryArgs a) {
-    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
+__device__ __forceinline__ void select_row(const QueryArgs& a, const uint64_t i) {
     const GridParams g = *a.gp;
     const float4 q = __ldg(&a.gv.sorted[i]);
     const uint32_t id = __float_as_uint(q.w);
@@ -369,11 +353,15 @@ __global__ void __launch_bounds__(128) knn_select_kernel(const QueryArgs a) {
     a.sums[i] = out;
 }
 
+template <int KS>
+__global__ void __launch_bounds__(128) knn_select_kernel(const QueryArgs a) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < a.n) select_row<KS>(a, i);
+}
+
 // Split form, finish: covariance, eigensolve and stage projections of the
 // rows the select kernel completed.  Uniform work per thread.
-__global__ void __launch_bounds__(128) knn_finish_kernel(const QueryArgs a) {
-    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
+__device__ __forceinline__ void finish_row(const QueryArgs& a, const uint64_t i) {
     const RowSums r = a.sums[i];
     if (r.cnt == 0) return;
     const GridParams* gp = a.gp;
@@ -391,6 +379,91 @@ __global__ void __launch_bounds__(128) knn_finish_kernel(const QueryArgs a) {
                              __float2int_rz(q.z) + __ldg(&gp->minz)};
     nbg_finish_row(a.grp, a.tf, a.ex, id, (int)n, M, qraw);
 }
+
+__global__ void __launch_bounds__(128) knn_finish_kernel(const QueryArgs a) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < a.n) finish_row(a, i);
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: persistent kernels draining one device work queue of
+// (tile, block of 128 queries) items, tiles of any size in one launch.  A
+// block takes the next item with one atomic, finds its tile by binary search
+// over the jobs' first items, and answers the item's queries exactly as the
+// per-tile kernels do.
+__device__ __forceinline__ bool next_item(const BatchJob* __restrict__ jobs, int njobs,
+                                          uint64_t items, unsigned long long* head,
+                                          uint64_t& item, int& job) {
+    __shared__ unsigned long long s_item;
+    __shared__ int s_job;
+    if (threadIdx.x == 0) {
+        const unsigned long long it = atomicAdd(head, 1ull);
+        int lo = 0, hi = njobs;
+        if (it < items) {
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (jobs[mid].first <= it) lo = mid;
+                else hi = mid;
+            }
+        }
+        s_item = it;
+        s_job = lo;
+    }
+    __syncthreads();
+    item = s_item;
+    job = s_job;
+    __syncthreads();
+    return item < items;
+}
+
+template <int KS>
+__global__ void __launch_bounds__(128) knn_select_queue_kernel(const BatchJob* __restrict__ jobs,
+                                                               int njobs, uint64_t items,
+                                                               unsigned long long* head) {
+    uint64_t item;
+    int j;
+    while (next_item(jobs, njobs, items, head, item, j)) {
+        const QueryArgs& a = jobs[j].q;
+        const uint64_t i = (item - jobs[j].first) * 128u + threadIdx.x;
+        if (i < a.n) select_row<KS>(a, i);
+    }
+}
+
+__global__ void __launch_bounds__(128) knn_finish_queue_kernel(const BatchJob* __restrict__ jobs,
+                                                               int njobs, uint64_t items,
+                                                               unsigned long long* head) {
+    uint64_t item;
+    int j;
+    while (next_item(jobs, njobs, items, head, item, j)) {
+        const QueryArgs& a = jobs[j].q;
+        const uint64_t i = (item - jobs[j].first) * 128u + threadIdx.x;
+        if (i < a.n) finish_row(a, i);
+    }
+}
+
+struct QueueArgs {
+    const BatchJob* jobs;
+    int njobs;
+    uint64_t items;
+    unsigned long long* head;
+    int sms;
+    cudaStream_t stream;
+};
+
+template <int KS>
+struct QueueLauncher {
+    using Args = QueueArgs;
+    static int run(const QueueArgs& q) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_select_queue_kernel<KS>, 128, 0);
+        const uint64_t grid = std::min<uint64_t>(q.items, (uint64_t)q.sms * std::max(per_sm, 1));
+        if (!grid) return NBG_OK;
+        knn_select_queue_kernel<KS><<<(unsigned)grid, 128, 0, q.stream>>>(q.jobs, q.njobs, q.items,
+                                                                           q.head);
+        NBG_LAUNCHED(1);
+        return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+    }
+};
 
 template <int KS>
 __global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
@@ -741,6 +814,24 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
     la.stream = stream;
     la.ids = true;
     return dispatch_slots<KnnLauncher>(K, la);
+}
+
+int slots_for_k(int K) { return slots_for(K); }
+
+int launch_select_queue(Context* ctx, int K, const BatchJob* jobs, int njobs, uint64_t items,
+                        unsigned long long* head, cudaStream_t stream) {
+    return dispatch_slots<QueueLauncher>(K, QueueArgs{jobs, njobs, items, head, ctx->sm_count, stream});
+}
+
+int launch_finish_queue(Context* ctx, const BatchJob* jobs, int njobs, uint64_t items,
+                        unsigned long long* head, cudaStream_t stream) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_finish_queue_kernel, 128, 0);
+    const uint64_t grid = std::min<uint64_t>(items, (uint64_t)ctx->sm_count * std::max(per_sm, 1));
+    if (!grid) return NBG_OK;
+    knn_finish_queue_kernel<<<(unsigned)grid, 128, 0, stream>>>(jobs, njobs, items, head);
+    NBG_LAUNCHED(1);
+    return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
 }
 
 }  // namespace nbg

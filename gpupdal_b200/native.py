@@ -154,6 +154,48 @@ class Context:
             ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code)
         return ex, stats
 
+    def run_batch(self, tiles, stages, outputs, optimal=None, graph=True,
+                  exception_capacity=1 << 16, stream=None):
+        """nbg_run_batch over `tiles` (list of Tile); stages[i] is the stage
+        list of tile i, outputs[i] its device abi.Columns list, optimal[i]
+        an (OptimalKNN, OptimalRadius) pair of device tensors or None.
+        Returns (exceptions per tile, stats)."""
+        m = len(tiles)
+        arr = (abi.BatchItem * max(m, 1))()
+        keep = []
+        nex = (ctypes.c_uint32 * max(m, 1))()
+        excs = []
+        for i, t in enumerate(tiles):
+            opts = (abi.StageOpts * len(stages[i]))(*stages[i])
+            cols = (abi.Columns * len(stages[i]))(*outputs[i])
+            exc = (abi.RowException * exception_capacity)()
+            keep += [opts, cols]
+            excs.append(exc)
+            it = arr[i]
+            it.tile = t.h.value
+            it.n_stages = len(stages[i])
+            it.exception_capacity = exception_capacity
+            it.stages = opts
+            it.outputs = cols
+            if optimal is not None and optimal[i] is not None:
+                it.optimal_knn = _dptr(optimal[i][0]).value
+                it.optimal_radius = _dptr(optimal[i][1]).value
+            it.exceptions = ctypes.addressof(exc)
+            it.n_exceptions = ctypes.cast(ctypes.addressof(nex) + 4 * i,
+                                          ctypes.POINTER(ctypes.c_uint32))
+        stats = abi.RunStats()
+        rc = self.lib.nbg_run_batch(self.h, arr, m, abi.BATCH_GRAPH if graph else 0,
+                                    ctypes.byref(stats), ctypes.c_void_p(stream) if stream else None)
+        self._check(rc)
+        out = []
+        for i in range(m):
+            k = min(nex[i], exception_capacity)
+            ex = np.zeros(k, dtype=[("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8)])
+            for j in range(k):
+                ex[j] = (excs[i][j].point_id, excs[i][j].stage, excs[i][j].code)
+            out.append(ex)
+        return out, stats
+
     def kd_export(self, tile):
         """The device KD replica: (vind, nodes dict) for parity tests."""
         n = tile.n

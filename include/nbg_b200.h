@@ -197,6 +197,32 @@ int nbg_neighbor_sets(nbg_context* ctx, nbg_tile* tile, int32_t knn,
                       uint32_t* ids_out, int32_t ids_on_device,
                       nbg_run_stats* stats, void* stream);
 
+/* Batched form -----------------------------------------------------------
+ * Many tiles of uneven size and knn in one call: the tiles' grids are built,
+ * then one persistent kernel per neighbour-count class drains a device work
+ * queue of (tile, 128-query block) items and one more finishes every row,
+ * all captured in a CUDA graph (replayed while the batch's shape is
+ * unchanged); the KD replicas for tie rows are built on a side stream while
+ * the queue drains.  Each item's results equal those of nbg_run on that
+ * tile.  Outputs, OptimalKNN/OptimalRadius and the tiles are device-resident;
+ * the stages of one item share one knn; a tile appears at most once. */
+typedef struct nbg_batch_item {
+    nbg_tile* tile;
+    int32_t n_stages;
+    uint32_t exception_capacity;
+    const nbg_stage_opts* stages;
+    const nbg_columns* outputs;       /* on_device = 1                       */
+    const double* optimal_knn;        /* device, may be null                 */
+    const double* optimal_radius;
+    nbg_row_exception* exceptions;    /* host, exception_capacity entries    */
+    uint32_t* n_exceptions;           /* host, may be null                   */
+} nbg_batch_item;
+
+#define NBG_BATCH_GRAPH 1u            /* capture the queue launches in a graph */
+
+int nbg_run_batch(nbg_context* ctx, const nbg_batch_item* items, int32_t n_items,
+                  uint32_t flags, nbg_run_stats* stats, void* stream);
+
 /* Served form ------------------------------------------------------------
  * A request loop over one device: requests (one tile + its stages each) are
  * queued FIFO and admitted while a slot is free and the HBM budget holds the
