@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--served-rate", type=float, default=20.0)
     ap.add_argument("--served-slots", type=int, default=4)
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--batch-tiles", type=int, default=256)
+    ap.add_argument("--no-batched", action="store_true")
     return ap.parse_args()
 
 
@@ -157,6 +159,47 @@ def cpu_reference(x, y, z, knn, sample, kind=None):
                                     f"{side / 100:.0f} m) of the same tile: KD build + "
                                     f"eigenvalues + normal, {threads} threads",
             "seconds": dt}
+
+
+def batched_leg(ctx, args):
+    """The batched tile set: plain per-tile launches against one
+    nbg_run_batch (graph-captured queue), with fixed and autotuned cells."""
+    import torch
+    from gpupdal_b200 import batched
+    tset = batched.make_set(args.batch_tiles, seed=100)
+    pts = sum(t["n"] for t in tset)
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = [fn() for _ in range(steps)]
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, out
+
+    steps = max(1, min(args.steps, 3))
+    batched.step_plain(ctx, tset)
+    plain_ms, _ = timed(lambda: batched.step_plain(ctx, tset), steps)
+    batched.step_batched(ctx, tset)
+    fixed_ms, st_fixed = timed(lambda: batched.step_batched(ctx, tset), steps)
+    batched.step_batched(ctx, tset, autotune=True)  # tunes each size/knn class once
+    tuned_ms, st_tuned = timed(lambda: batched.step_batched(ctx, tset, autotune=True), steps)
+    sizes = np.array([t["n"] for t in tset])
+    return {
+        "set": (f"{len(tset)} tiles, sizes log-normal (median 200k, sigma 1.0) clipped to "
+                f"[20k, 4M] ({int(sizes.min())}-{int(sizes.max())}), subsamples of one 8M "
+                "mixture cloud (seed 100), knn in {8,16,32}, normal + covariancefeatures(all); "
+                "device-resident inputs and outputs, tiles re-uploaded every step"),
+        "points": int(pts),
+        "plain_mpts_s": pts / plain_ms / 1e3,
+        "batched_mpts_s": pts / fixed_ms / 1e3,
+        "batched_autotuned_mpts_s": pts / tuned_ms / 1e3,
+        "batched_vs_plain": plain_ms / fixed_ms,
+        "graph": True,
+        "query_ms": st_fixed[-1].query_ms, "kd_build_ms": st_fixed[-1].kd_build_ms,
+        "tree_ms": st_fixed[-1].tree_ms, "grid_ms": st_fixed[-1].grid_ms,
+    }
 
 
 def served_leg(ctx, args):
@@ -337,6 +380,8 @@ def main():
                      "bytes_per_point": BYTES_PER_POINT},
         "clocks": clk,
     }
+    if ws == 1 and not args.no_batched:
+        line["batched"] = batched_leg(ctx, args)
     if ws == 1 and not args.no_served:
         line["served"] = served_leg(ctx, args)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

@@ -127,6 +127,7 @@ class BatchItem(ctypes.Structure):
 
 
 BATCH_GRAPH = 1
+BATCH_AUTOTUNE = 2
 
 
 class Request(ctypes.Structure):
@@ -224,6 +225,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_tile_free.restype = ctypes.c_int
     lib.nbg_tile_tune.argtypes = [vp, vp, ctypes.c_float, i32]
     lib.nbg_tile_tune.restype = ctypes.c_int
+    lib.nbg_tile_autotune.argtypes = [vp, vp, i32, ctypes.POINTER(ctypes.c_float), i32, i32,
+                                      ctypes.POINTER(ctypes.c_float), vp]
+    lib.nbg_tile_autotune.restype = ctypes.c_int
     lib.nbg_tile_size.argtypes = [vp]
     lib.nbg_tile_size.restype = u64
     lib.nbg_run.argtypes = [vp, vp, ctypes.POINTER(StageOpts), i32, ctypes.POINTER(Columns),

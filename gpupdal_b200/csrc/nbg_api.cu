@@ -21,6 +21,8 @@
 
 namespace nbg {
 
+int slots_for_k(int K);
+
 int fail(Context* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
@@ -857,6 +859,102 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     if (nex > exception_capacity)
         return fail(ctx, NBG_ERR_EXCEPTIONS, "row-exception list overflowed");
     return NBG_OK;
+}
+
+namespace nbg {
+
+int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, int32_t n_candidates,
+                  bool use_cache, float* chosen, cudaStream_t stream) {
+    if (knn < 0 || knn > 64) return fail(ctx, NBG_ERR_INVALID, "knn must be in [0, 64]");
+    static const float defaults[] = {1.0f, 1.5f, 2.0f, 3.0f, 4.0f, 6.0f};
+    if (!candidates || n_candidates <= 0) {
+        candidates = defaults;
+        n_candidates = (int32_t)(sizeof(defaults) / sizeof(defaults[0]));
+    }
+    const uint64_t n = t->n;
+    if (n == 0) return NBG_OK;
+    const int K = (int)std::min<uint64_t>(n, (uint64_t)knn + 1);
+    int lg = 0;
+    while ((1ull << (lg + 1)) <= n) ++lg;
+    const std::pair<int, int> key(lg, slots_for_k(K));
+    auto hit = ctx->tuned.find(key);
+    if (use_cache && hit != ctx->tuned.end()) {
+        if (t->cell_factor != hit->second) {
+            t->cell_factor = hit->second;
+            t->fixed_cell = 0;
+            t->grid_valid = false;
+        }
+        if (chosen) *chosen = hit->second;
+        return NBG_OK;
+    }
+    int rc = ensure_scratch(ctx, n, 1);
+    if (rc) return rc;
+    const uint64_t rows_total = (n + 127) / 128;
+    const unsigned blocks = (unsigned)std::min<uint64_t>(rows_total, 512);
+    const uint64_t stride = std::max<uint64_t>(128, (n / blocks) / 128 * 128);
+    const double scale = (double)n / ((double)blocks * 128.0);
+    uint32_t* cnt_dev = ctx->counters + 32;  // scratch block, not the call counters
+    float best = candidates[0];
+    double best_ms = 1e300;
+    for (int c = 0; c < n_candidates; ++c) {
+        const float cf = candidates[c];
+        if (!(cf > 0.0f) || cf > 64.0f) return fail(ctx, NBG_ERR_INVALID, "bad cell factor");
+        t->cell_factor = cf;
+        t->fixed_cell = 0;
+        t->grid_valid = false;
+        cudaEventRecord(ctx->ev[0], stream);
+        rc = ensure_grid(ctx, t, K, stream);
+        if (rc) return rc;
+        cudaEventRecord(ctx->ev[1], stream);
+        QueryLaunch ql;
+        ql.tile = t;
+        ql.K = K;
+        ql.rmax = 8;
+        ql.grp = StageGroup{};
+        ql.ex = ExceptionSink{ctx->ex_rows, cnt_dev + 3, 1};
+        ql.exact_rows = ctx->exact_rows;
+        ql.counters = cnt_dev;
+        ql.ties = ctx->ties;
+        ql.tie_cap = (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX);
+        ql.sums = ctx->sums;
+        cudaMemsetAsync(cnt_dev, 0, 8 * sizeof(uint32_t), stream);
+        cudaEventRecord(ctx->ev[2], stream);
+        rc = launch_select_sample(ctx, ql, stride, blocks, stream);
+        if (rc) return fail(ctx, rc, "autotune sample launch");
+        cudaEventRecord(ctx->ev[3], stream);
+        uint32_t cnt[3] = {0, 0, 0};
+        NBG_TRY(cudaMemcpyAsync(cnt, cnt_dev, sizeof(cnt), cudaMemcpyDeviceToHost, stream), "autotune");
+        NBG_TRY(cudaStreamSynchronize(stream), "autotune");
+        float build_ms = 0, sample_ms = 0;
+        cudaEventElapsedTime(&build_ms, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&sample_ms, ctx->ev[2], ctx->ev[3]);
+        // rows the ring search cannot finish go to the search replay: charge
+        // each an estimated 20 us of replay
+        const double deferred = (double)cnt[0] * scale;
+        const double est = build_ms + sample_ms * scale + deferred * 0.02;
+        if (est < best_ms) {
+            best_ms = est;
+            best = cf;
+        }
+    }
+    t->cell_factor = best;
+    t->grid_valid = false;
+    ctx->tuned[key] = best;
+    if (chosen) *chosen = best;
+    return NBG_OK;
+}
+
+}  // namespace nbg
+
+extern "C" int nbg_tile_autotune(nbg_context* h, nbg_tile* th, int32_t knn, const float* candidates,
+                                 int32_t n_candidates, int32_t use_cache, float* chosen,
+                                 void* stream_v) {
+    if (!h || !th) return NBG_ERR_INVALID;
+    Context* ctx = &h->c;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return tile_autotune(ctx, &th->t, knn, candidates, n_candidates, use_cache != 0, chosen,
+                         (cudaStream_t)stream_v);
 }
 
 extern "C" int nbg_neighbor_sets(nbg_context* h, nbg_tile* th, int32_t knn, uint32_t* ids_out,

@@ -8,7 +8,8 @@
 //              finish kernel then takes every item of every class.  The head
 //              resets and the launches are captured in a CUDA graph, replayed
 //              while the batch's job arrays and counts are unchanged.
-// 3. replicas  a host thread builds the tiles' KD replicas on the context's
+// 3. replicas  a host thread builds the tiles' KD replicas, all as one forest
+//              (one level-synchronous build for every tile), on the context's
 //              side stream while the queue drains (they depend only on the
 //              coordinates)
 // 4. exact     per tile: the tie-order resolver, then the search replay for
@@ -184,6 +185,14 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
         if (rc) return rc;
         B->ex = ex_total;
     }
+    // ---- cell factors from the autotuner (measured once per size/knn class)
+    if (flags & NBG_BATCH_AUTOTUNE) {
+        for (int i : live) {
+            rc = tile_autotune(ctx, &items[i].tile->t, items[i].stages[0].knn, nullptr, 0, true,
+                               nullptr, st);
+            if (rc) return rc;
+        }
+    }
     // ---- grids (no host synchronisation), then one read of every shape
     cudaEventRecord(B->ev[0], user);
     cudaStreamWaitEvent(st, B->ev[0], 0);
@@ -350,10 +359,7 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
         kd_thread = std::thread([&] {
             cudaSetDevice(ctx->device);
             cudaEventRecord(ctx->ev[8], ctx->side);
-            for (Tile* t : kd_tiles) {
-                kd_rc = kd_ensure(ctx, t, ctx->side);
-                if (kd_rc) break;
-            }
+            kd_rc = kd_ensure_many(ctx, kd_tiles.data(), (int)kd_tiles.size(), ctx->side);
             cudaEventRecord(ctx->ev[9], ctx->side);
             cudaStreamSynchronize(ctx->side);
             cudaEventElapsedTime(&kd_ms, ctx->ev[8], ctx->ev[9]);

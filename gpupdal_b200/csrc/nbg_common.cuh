@@ -60,7 +60,7 @@ struct StageGroup {
 
 // The KD replica's nodes as the tie-order resolver reads them: a child's
 // points are the contiguous range [nb, ne) of the replica's point order, and
-// kpos maps a point id to its position in that order.
+// kpos[base + id] is the position of point id in that order.
 struct KdOrder {
     const int32_t* c1;
     const int32_t* c2;
@@ -68,7 +68,9 @@ struct KdOrder {
     const uint32_t* ne;
     const double* dlo;
     const double* dhi;
-    const uint32_t* kpos;
+    const uint32_t* kpos;  // indexed base + point id
+    int32_t root;          // the tile's root node
+    uint64_t base;         // the tile's first position
 };
 
 // Exact integer neighbourhood sums of one row (offsets from the query, raw

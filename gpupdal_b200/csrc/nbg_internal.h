@@ -49,6 +49,8 @@ struct Context {
     std::multimap<size_t, void*> cache;
     uint64_t cached = 0;
     std::unordered_map<void*, size_t> live;  // block sizes of handed-out blocks
+    // autotuner: chosen cell factor per (log2 points, neighbour slots) class
+    std::map<std::pair<int, int>, float> tuned;
     // pinned bounce buffers for copies to and from pageable host memory
     char* bounce[2] = {nullptr, nullptr};
     cudaEvent_t bev[2];
@@ -128,6 +130,9 @@ struct QueryLaunch {
     RowSums* sums = nullptr;  // split select/finish kernels (null: one fused kernel)
 };
 int launch_query(Context* ctx, const QueryLaunch& q, cudaStream_t stream);
+// Select pass over a sample of `blocks` blocks of 128 rows, `stride` rows apart.
+int launch_select_sample(Context* ctx, const QueryLaunch& q, uint64_t stride, unsigned blocks,
+                         cudaStream_t stream);
 
 // Tie rows ordered on the KD replica's tree (no search replay).
 struct TieLaunch {
@@ -146,6 +151,8 @@ int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream);
 
 // Exact path: nanoflann replica build (lazy) + DFS for the listed rows.
 int kd_ensure(Context* ctx, Tile* t, cudaStream_t stream);
+// One forest holding the replicas of every listed tile that has none.
+int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t stream);
 int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const ExceptionSink& ex,
                 const uint32_t* rows, uint32_t nrows, cudaStream_t stream);
 int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
@@ -162,6 +169,10 @@ int kd_export(Context* ctx, Tile* t, uint32_t* vind, uint32_t* nnodes, int32_t* 
 int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
                          uint32_t* exact_rows, uint32_t* counters, uint2* ties, uint32_t tie_cap,
                          cudaStream_t stream);
+
+// Autotuner (nbg_tile_autotune without the context lock).
+int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, int32_t n_candidates,
+                  bool use_cache, float* chosen, cudaStream_t stream);
 
 // Batched form: the context's batch scratch and cached graph (nbg_batch.cu).
 void batch_release(Context* ctx);

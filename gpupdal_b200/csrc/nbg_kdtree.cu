@@ -76,16 +76,28 @@ struct KdDev {
     const uint32_t* ne;
     const double* dlo;
     const double* dhi;
+    int32_t root;  // the tree's root node
     double root_lo[3], root_hi[3];
 };
 
-struct KdReplica {
+// Storage of one or more replicas built together (a forest): the trees'
+// points are concatenated (tree k owns positions [base[k], base[k] + npts[k])),
+// their nodes share the node arrays, and tree k's root is node k.  Segments
+// carry their tree in KdSeg::pad, nodes in ntree[].
+struct KdForest {
     uint64_t n = 0;
+    int ntrees = 0;
+    std::vector<uint64_t> base, npts;
+    std::vector<Transform> tfh;
+    std::vector<double> rootbox;  // 6 per tree: lo[3], hi[3]
+    Transform* tfs = nullptr;     // device, per tree
+    int32_t* ntree = nullptr;     // device, per node
+    int refs = 0;
     int32_t* rx = nullptr;
     int32_t* ry = nullptr;
     int32_t* rz = nullptr;
     uint32_t* rid = nullptr;
-    uint32_t* kpos = nullptr;  // inverse of rid: point id -> position
+    uint32_t* kpos = nullptr;  // base + point id -> position (inverse of rid per tree)
     uint32_t* mlpos = nullptr;
     uint32_t* mrpos = nullptr;
     // nodes
@@ -118,10 +130,15 @@ struct KdReplica {
     uint32_t* counters = nullptr;  // [0] next segments, [1] nodes, [2] errors, [3] small
                                    // segments, [4] leaves
     uint32_t dl_cap = 0;
-    double root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
-    bool built = false;
     uint64_t bytes = 0;
     std::vector<std::pair<void*, size_t>> blocks;  // device blocks owned
+};
+
+// A tile's view of its replica: the forest and the tile's tree in it.
+struct KdReplica {
+    KdForest* f = nullptr;
+    int tree = 0;
+    bool built = false;
 };
 
 // ---------------------------------------------------------------------------
@@ -263,11 +280,12 @@ __device__ __forceinline__ void kd_choose_cut(const double lo[3], const double h
     else cutval = split_val;
 }
 
-__global__ void kd_split_kernel(const KdSeg* segs, uint32_t S, KdSplit* sp, Transform tf,
+__global__ void kd_split_kernel(const KdSeg* segs, uint32_t S, KdSplit* sp, const Transform* tfs,
                                 int32_t* bmin, int32_t* bmax) {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
     const KdSeg sg = segs[s];
+    const Transform tf = tfs[sg.pad];
     KdSplit p = sp[s];
     // the node's extents are its points' extents
     for (int d = 0; d < 3; ++d) {
@@ -297,10 +315,11 @@ __global__ void __launch_bounds__(KD_TILE) kd_count_kernel(const KdSeg* segs, co
                                                            const uint32_t* tile_seg,
                                                            const KdSplit* sp, const int32_t* rx,
                                                            const int32_t* ry, const int32_t* rz,
-                                                           Transform tf, uint32_t* tile_cnt) {
+                                                           const Transform* tfs, uint32_t* tile_cnt) {
     const uint32_t t = blockIdx.x;
     const uint32_t s = tile_seg[t];
     const KdSeg sg = segs[s];
+    const Transform& tf = tfs[sg.pad];
     const int f = sp[s].f;
     const double cut = sp[s].cutval;
     const uint32_t i = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
@@ -314,10 +333,11 @@ __global__ void __launch_bounds__(KD_TILE) kd_count_kernel(const KdSeg* segs, co
 template <int PASS>
 __global__ void kd_seg_count_kernel(const KdSeg* segs, uint32_t S, const uint32_t* tile_first,
                                     const uint32_t* tile_pref, KdSplit* sp, const int32_t* rx,
-                                    const int32_t* ry, const int32_t* rz, Transform tf) {
+                                    const int32_t* ry, const int32_t* rz, const Transform* tfs) {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
     const KdSeg sg = segs[s];
+    const Transform& tf = tfs[sg.pad];
     const uint32_t first = tile_first[s], nt = tile_first[s + 1] - first;
     const uint32_t len = sg.end - sg.begin;
     const int f = sp[s].f;
@@ -346,13 +366,14 @@ __global__ void __launch_bounds__(KD_TILE) kd_classify_kernel(const KdSeg* segs,
                                                               const uint32_t* tile_pref,
                                                               const KdSplit* sp, const int32_t* rx,
                                                               const int32_t* ry, const int32_t* rz,
-                                                              Transform tf, uint32_t* mlpos,
+                                                              const Transform* tfs, uint32_t* mlpos,
                                                               uint32_t* mrpos) {
     typedef cub::BlockScan<uint32_t, KD_TILE> Scan;
     __shared__ typename Scan::TempStorage tmp;
     const uint32_t t = blockIdx.x;
     const uint32_t s = tile_seg[t];
     const KdSeg sg = segs[s];
+    const Transform& tf = tfs[sg.pad];
     const int f = sp[s].f;
     const double cut = sp[s].cutval;
     const uint32_t L = PASS == 1 ? sp[s].L : sp[s].L2;
@@ -410,7 +431,7 @@ __global__ void kd_children_kernel(const KdSeg* segs, uint32_t S, const KdSplit*
                                    uint32_t* counters, int32_t* c1, int32_t* c2, int32_t* feat,
                                    uint32_t* nb, uint32_t* ne, uint32_t node_cap, uint32_t seg_cap,
                                    KdSeg* small, uint32_t small_max, uint32_t* leaves,
-                                   uint32_t leaf_cap) {
+                                   uint32_t leaf_cap, int32_t* ntree) {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
     const KdSeg sg = segs[s];
@@ -445,6 +466,7 @@ __global__ void kd_children_kernel(const KdSeg* segs, uint32_t S, const KdSplit*
         c1[node] = -1;
         c2[node] = -1;
         feat[node] = 0;
+        ntree[node] = sg.pad;
         const uint32_t len = ch.end - ch.begin;
         if (len <= (uint32_t)KD_LEAF) {
             const uint32_t slot = atomicAdd(&counters[4], 1u);
@@ -560,7 +582,7 @@ __global__ void __launch_bounds__(32 * KD_WARPS) kd_warp_build_kernel(
     const KdSeg* small, uint32_t nsmall, int32_t* rx, int32_t* ry, int32_t* rz, uint32_t* rid,
     uint32_t* mlpos, uint32_t* mrpos, int32_t* c1, int32_t* c2, int32_t* feat, uint32_t* nb,
     uint32_t* ne, int32_t* bmin, int32_t* bmax, uint32_t* counters, uint32_t node_cap,
-    Transform tf) {
+    const Transform* tfs, int32_t* ntree) {
     __shared__ KdSeg stk[KD_WARPS][KD_WSTACK];
     const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t w = blockIdx.x * KD_WARPS + wl;
@@ -582,6 +604,7 @@ __global__ void __launch_bounds__(32 * KD_WARPS) kd_warp_build_kernel(
             bmax[3 * node + lane] = mx[lane];
         }
         if (count <= (uint32_t)KD_LEAF) continue;
+        const Transform tf = tfs[sg.pad];
         int f;
         double cut;
         kd_choose_cut(sg.lo, sg.hi, mn, mx, tf, f, cut);
@@ -618,6 +641,7 @@ __global__ void __launch_bounds__(32 * KD_WARPS) kd_warp_build_kernel(
                 c1[cid + side] = -1;
                 c2[cid + side] = -1;
                 feat[cid + side] = 0;
+                ntree[cid + side] = sg.pad;
                 st[top + (1 - side)] = ch;
             }
         }
@@ -628,18 +652,20 @@ __global__ void __launch_bounds__(32 * KD_WARPS) kd_warp_build_kernel(
 
 __global__ void kd_div_kernel(uint32_t nodes, const int32_t* c1, const int32_t* c2,
                               const int32_t* feat, const int32_t* bmin, const int32_t* bmax,
-                              Transform tf, double* dlo, double* dhi) {
+                              const Transform* tfs, const int32_t* ntree, double* dlo, double* dhi) {
     uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= nodes || c1[node] < 0) return;
     const int f = feat[node];
+    const Transform& tf = tfs[ntree[node]];
     dlo[node] = ref_coord(bmax[3 * c1[node] + f], tf.scale[f], tf.offset[f]);
     dhi[node] = ref_coord(bmin[3 * c2[node] + f], tf.scale[f], tf.offset[f]);
 }
 
-__global__ void kd_inverse_kernel(const uint32_t* rid, uint64_t n, uint32_t* kpos) {
+// kpos[base + id] = position of point id of the tree starting at base.
+__global__ void kd_inverse_kernel(const uint32_t* rid, uint64_t base, uint64_t n, uint32_t* kpos) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x)
-        kpos[rid[i]] = (uint32_t)i;
+        kpos[base + rid[base + i]] = (uint32_t)(base + i);
 }
 
 // ---------------------------------------------------------------------------
@@ -702,7 +728,7 @@ __device__ bool kd_search(const KdDev& kd, const Transform& tf, const double q[3
     }
     KdFrame st[KD_STACK];
     int top = 0;
-    st[0].node = 0;
+    st[0].node = kd.root;
     st[0].mind = distsq;
     st[0].phase = 0;
     while (top >= 0) {
@@ -840,7 +866,7 @@ __global__ void kd_scatter_ids_kernel(const uint32_t* __restrict__ rows, uint32_
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-static int kd_alloc(Context* ctx, void** p, size_t bytes, KdReplica* kd) {
+static int kd_alloc(Context* ctx, void** p, size_t bytes, KdForest* kd) {
     int rc = ctx_alloc(ctx, p, bytes);
     if (rc) return rc;
     kd->bytes += bytes;
@@ -848,7 +874,7 @@ static int kd_alloc(Context* ctx, void** p, size_t bytes, KdReplica* kd) {
     return NBG_OK;
 }
 
-static void kd_release(Context* ctx, KdReplica* kd, void* p) {
+static void kd_release(Context* ctx, KdForest* kd, void* p) {
     for (size_t i = 0; i < kd->blocks.size(); ++i)
         if (kd->blocks[i].first == p) {
             ctx_free(ctx, p, kd->blocks[i].second);
@@ -859,7 +885,7 @@ static void kd_release(Context* ctx, KdReplica* kd, void* p) {
 }
 
 template <class T>
-static int kd_grow(Context* ctx, T** p, size_t old_n, size_t new_n, KdReplica* kd, cudaStream_t st) {
+static int kd_grow(Context* ctx, T** p, size_t old_n, size_t new_n, KdForest* kd, cudaStream_t st) {
     T* q = nullptr;
     int rc = kd_alloc(ctx, (void**)&q, new_n * sizeof(T), kd);
     if (rc) return rc;
@@ -872,18 +898,24 @@ static int kd_grow(Context* ctx, T** p, size_t old_n, size_t new_n, KdReplica* k
     return NBG_OK;
 }
 
-uint64_t kd_bytes(uint64_t n) { return n * 28 + (n / 16 + 1024) * 64; }
+uint64_t kd_bytes(uint64_t n) { return n * 28 + (n / 16 + 1024) * 68; }
+
+static void kd_forest_free(Context* ctx, KdForest* f) {
+    for (auto& b : f->blocks) ctx_free(ctx, b.first, b.second);
+    delete f;
+}
 
 void kd_free(Context* ctx, Tile* t) {
     KdReplica* kd = t->kd;
     if (!kd) return;
-    for (auto& b : kd->blocks) ctx_free(ctx, b.first, b.second);
+    KdForest* f = kd->f;
     delete kd;
     t->kd = nullptr;
+    if (f && --f->refs <= 0) kd_forest_free(ctx, f);
 }
 
 // Builds the tile list of `S` segments; returns the number of tiles.
-static int kd_tiles(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, uint32_t* ntiles,
+static int kd_tiles(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, uint32_t* ntiles,
                     cudaStream_t st) {
     kd_seg_tiles_kernel<<<(S + 1 + 255) / 256, 256, 0, st>>>(segs, S, kd->nt);
     size_t tb = kd->scan_bytes;
@@ -914,24 +946,25 @@ static int kd_tiles(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, 
 }
 
 template <int PASS>
-static int kd_pass(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, const Transform& tf,
-                   cudaStream_t st) {
+static int kd_pass(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, cudaStream_t st) {
     uint32_t ntiles = 0;
     int rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
     if (rc) return rc;
     if (ntiles) {
         kd_count_kernel<PASS><<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->split,
-                                                          kd->rx, kd->ry, kd->rz, tf, kd->tile_cnt);
+                                                          kd->rx, kd->ry, kd->rz, kd->tfs,
+                                                          kd->tile_cnt);
     }
     cudaMemsetAsync(kd->tile_cnt + ntiles, 0, 4, st);
     size_t tb = kd->scan_bytes;
     cub::DeviceScan::ExclusiveSum(kd->scan_tmp, tb, kd->tile_cnt, kd->tile_cnt, (int)(ntiles + 1), st);
     kd_seg_count_kernel<PASS><<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->nt, kd->tile_cnt,
-                                                               kd->split, kd->rx, kd->ry, kd->rz, tf);
+                                                               kd->split, kd->rx, kd->ry, kd->rz,
+                                                               kd->tfs);
     if (ntiles) {
         kd_classify_kernel<PASS><<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg,
                                                              kd->tile_cnt, kd->split, kd->rx,
-                                                             kd->ry, kd->rz, tf, kd->mlpos,
+                                                             kd->ry, kd->rz, kd->tfs, kd->mlpos,
                                                              kd->mrpos);
         kd_swap_kernel<PASS><<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->split,
                                                          kd->mlpos, kd->mrpos, kd->rx, kd->ry,
@@ -941,7 +974,7 @@ static int kd_pass(Context* ctx, KdReplica* kd, const KdSeg* segs, uint32_t S, c
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
 }
 
-static int kd_grow_nodes(Context* ctx, KdReplica* kd, uint32_t nc, cudaStream_t st) {
+static int kd_grow_nodes(Context* ctx, KdForest* kd, uint32_t nc, cudaStream_t st) {
     const uint32_t old = kd->node_cap;
     if (nc <= old) return NBG_OK;
     int rc = kd_grow(ctx, &kd->c1, old, nc, kd, st);
@@ -949,6 +982,7 @@ static int kd_grow_nodes(Context* ctx, KdReplica* kd, uint32_t nc, cudaStream_t 
     if (!rc) rc = kd_grow(ctx, &kd->feat, old, nc, kd, st);
     if (!rc) rc = kd_grow(ctx, &kd->nb, old, nc, kd, st);
     if (!rc) rc = kd_grow(ctx, &kd->ne, old, nc, kd, st);
+    if (!rc) rc = kd_grow(ctx, &kd->ntree, old, nc, kd, st);
     if (!rc) rc = kd_grow(ctx, &kd->bmin, (size_t)old * 3, (size_t)nc * 3, kd, st);
     if (!rc) rc = kd_grow(ctx, &kd->bmax, (size_t)old * 3, (size_t)nc * 3, kd, st);
     if (rc) return rc;
@@ -956,51 +990,74 @@ static int kd_grow_nodes(Context* ctx, KdReplica* kd, uint32_t nc, cudaStream_t 
     return NBG_OK;
 }
 
-// One build of the replica; `small_max` = 0 keeps every level on the level
-// passes (the fallback when a warp subtree overflows its stack or the nodes).
-static int kd_build(Context* ctx, Tile* t, uint32_t small_max, cudaStream_t st) {
-    KdReplica* kd = t->kd;
-    const uint64_t n = t->n;
+static unsigned grid_for(const Context* ctx, uint64_t n) {
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, ctx->sm_count * 8));
+}
+
+// One build of the forest over `tiles`; `small_max` = 0 keeps every level on
+// the level passes (the fallback when a warp subtree overflows its stack or
+// the node arrays).
+static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t small_max,
+                    cudaStream_t st) {
+    const int T = kd->ntrees;
     int rc = NBG_OK;
-    kd_init_kernel<<<std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, ctx->sm_count * 8)), 256, 0,
-                     st>>>(t->x, t->y, t->z, n, kd->rx, kd->ry, kd->rz, kd->rid);
-    NBG_LAUNCHED(1);
-    // root: actual bbox, as calculateBounds
-    const GridParams& g = t->host_gp;
-    const Transform& tf = t->tf;
-    KdSeg root;
-    root.begin = 0;
-    root.end = (uint32_t)n;
-    root.node = 0;
-    root.pad = 0;
-    int32_t mn[3] = {g.minx, g.miny, g.minz}, mx[3] = {g.maxx, g.maxy, g.maxz};
-    for (int d = 0; d < 3; ++d) {
-        root.lo[d] = (double)mn[d] * tf.scale[d] + tf.offset[d];
-        root.hi[d] = (double)mx[d] * tf.scale[d] + tf.offset[d];
-        kd->root_lo[d] = root.lo[d];
-        kd->root_hi[d] = root.hi[d];
+    std::vector<KdSeg> level0, small0;
+    std::vector<uint32_t> leaves0;
+    std::vector<int32_t> c_init(T, -1), f_init(T, 0), tree_init(T);
+    std::vector<uint32_t> nb_init(T), ne_init(T);
+    for (int k = 0; k < T; ++k) {
+        const Tile* t = tiles[k];
+        const uint64_t b = kd->base[k], n = kd->npts[k];
+        kd_init_kernel<<<grid_for(ctx, n), 256, 0, st>>>(t->x, t->y, t->z, n, kd->rx + b, kd->ry + b,
+                                                         kd->rz + b, kd->rid + b);
+        // root: the tile's actual bounding box, as calculateBounds
+        const GridParams& g = t->host_gp;
+        KdSeg root;
+        root.begin = (uint32_t)b;
+        root.end = (uint32_t)(b + n);
+        root.node = k;
+        root.pad = k;
+        const int32_t mn[3] = {g.minx, g.miny, g.minz}, mx[3] = {g.maxx, g.maxy, g.maxz};
+        for (int d = 0; d < 3; ++d) {
+            root.lo[d] = (double)mn[d] * t->tf.scale[d] + t->tf.offset[d];
+            root.hi[d] = (double)mx[d] * t->tf.scale[d] + t->tf.offset[d];
+            kd->rootbox[6 * k + d] = root.lo[d];
+            kd->rootbox[6 * k + 3 + d] = root.hi[d];
+        }
+        tree_init[k] = k;
+        nb_init[k] = root.begin;
+        ne_init[k] = root.end;
+        if (n > (uint64_t)KD_LEAF && n > small_max) level0.push_back(root);
+        else if (n > (uint64_t)KD_LEAF) small0.push_back(root);
+        else leaves0.push_back((uint32_t)k);
     }
-    int32_t neg = -1;
-    uint32_t zero = 0, rootend = (uint32_t)n;
-    cudaMemcpyAsync(kd->c1, &neg, 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(kd->c2, &neg, 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(kd->feat, &zero, 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(kd->nb, &zero, 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(kd->ne, &rootend, 4, cudaMemcpyHostToDevice, st);
-    uint32_t cnt[5] = {0, 1, 0, 0, 0};
-    uint32_t S = 0;
-    if (n > (uint64_t)KD_LEAF && n > small_max) {
-        cudaMemcpyAsync(kd->seg[0], &root, sizeof(KdSeg), cudaMemcpyHostToDevice, st);
-        S = 1;
-    } else if (n > (uint64_t)KD_LEAF) {
-        cudaMemcpyAsync(kd->small, &root, sizeof(KdSeg), cudaMemcpyHostToDevice, st);
-        cnt[3] = 1;
-    } else {
-        cudaMemcpyAsync(kd->leaves, &zero, 4, cudaMemcpyHostToDevice, st);
-        cnt[4] = 1;
+    NBG_LAUNCHED(T);
+    if (level0.size() > kd->seg_cap || small0.size() > kd->seg_cap || leaves0.size() > kd->leaf_cap) {
+        ctx->err = "KD replica: too many trees for the segment lists";
+        return NBG_ERR_UNSUPPORTED;
     }
+    // root nodes 0..T-1 (host arrays outlive the copies: the stream is synchronised below)
+    cudaMemcpyAsync(kd->c1, c_init.data(), T * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->c2, c_init.data(), T * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->feat, f_init.data(), T * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->nb, nb_init.data(), T * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->ne, ne_init.data(), T * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->ntree, tree_init.data(), T * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kd->tfs, kd->tfh.data(), T * sizeof(Transform), cudaMemcpyHostToDevice, st);
+    if (!level0.empty())
+        cudaMemcpyAsync(kd->seg[0], level0.data(), level0.size() * sizeof(KdSeg), cudaMemcpyHostToDevice, st);
+    if (!small0.empty())
+        cudaMemcpyAsync(kd->small, small0.data(), small0.size() * sizeof(KdSeg), cudaMemcpyHostToDevice, st);
+    if (!leaves0.empty())
+        cudaMemcpyAsync(kd->leaves, leaves0.data(), leaves0.size() * 4, cudaMemcpyHostToDevice, st);
+    uint32_t cnt[5] = {0, (uint32_t)T, 0, (uint32_t)small0.size(), (uint32_t)leaves0.size()};
     cudaMemcpyAsync(kd->counters, cnt, sizeof(cnt), cudaMemcpyHostToDevice, st);
-    uint32_t node_count = 1;
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        ctx->err = "KD replica init failed";
+        return NBG_ERR_CUDA;
+    }
+    uint32_t node_count = (uint32_t)T;
+    uint32_t S = (uint32_t)level0.size();
     int cur = 0;
     while (S > 0) {
         // room for this level's children
@@ -1020,12 +1077,12 @@ static int kd_build(Context* ctx, Tile* t, uint32_t small_max, cudaStream_t st) 
                                                                       kd->split);
             NBG_LAUNCHED(1);
         }
-        kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, tf, kd->bmin, kd->bmax);
+        kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->tfs, kd->bmin, kd->bmax);
         NBG_LAUNCHED(2 + (ntiles ? 1 : 0));
-        rc = kd_pass<1>(ctx, kd, segs, S, tf, st);
+        rc = kd_pass<1>(ctx, kd, segs, S, st);
         if (rc) return rc;
         kd_pass2_segs_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg2);
-        rc = kd_pass<2>(ctx, kd, kd->seg2, S, tf, st);
+        rc = kd_pass<2>(ctx, kd, kd->seg2, S, st);
         if (rc) return rc;
         cudaMemsetAsync(kd->counters, 0, 4, st);
         NBG_LAUNCHED(2);
@@ -1033,7 +1090,7 @@ static int kd_build(Context* ctx, Tile* t, uint32_t small_max, cudaStream_t st) 
                                                             kd->counters, kd->c1, kd->c2, kd->feat,
                                                             kd->nb, kd->ne, kd->node_cap,
                                                             kd->seg_cap, kd->small, small_max,
-                                                            kd->leaves, kd->leaf_cap);
+                                                            kd->leaves, kd->leaf_cap, kd->ntree);
         cudaMemcpyAsync(cnt, kd->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st);
         cudaError_t be = cudaGetLastError();
         if (be == cudaSuccess) be = cudaStreamSynchronize(st);
@@ -1051,12 +1108,14 @@ static int kd_build(Context* ctx, Tile* t, uint32_t small_max, cudaStream_t st) 
     }
     // subtrees of the small segments, one warp each
     const uint32_t nsmall = cnt[3], nleaves = cnt[4];
+    const uint64_t n = kd->n;
     if (nsmall) {
         rc = kd_grow_nodes(ctx, kd, std::max<uint32_t>(kd->node_cap, node_count + (uint32_t)(n / 8) + 1024), st);
         if (rc) return rc;
         kd_warp_build_kernel<<<(nsmall + KD_WARPS - 1) / KD_WARPS, 32 * KD_WARPS, 0, st>>>(
             kd->small, nsmall, kd->rx, kd->ry, kd->rz, kd->rid, kd->mlpos, kd->mrpos, kd->c1, kd->c2,
-            kd->feat, kd->nb, kd->ne, kd->bmin, kd->bmax, kd->counters, kd->node_cap, tf);
+            kd->feat, kd->nb, kd->ne, kd->bmin, kd->bmax, kd->counters, kd->node_cap, kd->tfs,
+            kd->ntree);
         NBG_LAUNCHED(1);
     }
     if (nleaves)
@@ -1084,14 +1143,15 @@ static int kd_build(Context* ctx, Tile* t, uint32_t small_max, cudaStream_t st) 
         kd->dl_cap = nn;
     }
     kd_div_kernel<<<(nn + 127) / 128, 128, 0, st>>>(nn, kd->c1, kd->c2, kd->feat, kd->bmin,
-                                                    kd->bmax, tf, kd->dlo, kd->dhi);
+                                                    kd->bmax, kd->tfs, kd->ntree, kd->dlo, kd->dhi);
     if (!kd->kpos) {
         rc = kd_alloc(ctx, (void**)&kd->kpos, n * 4, kd);
         if (rc) return rc;
     }
-    kd_inverse_kernel<<<std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, ctx->sm_count * 8)), 256,
-                        0, st>>>(kd->rid, n, kd->kpos);
-    NBG_LAUNCHED(2 + (nleaves ? 1 : 0));
+    for (int k = 0; k < T; ++k)
+        kd_inverse_kernel<<<grid_for(ctx, kd->npts[k]), 256, 0, st>>>(kd->rid, kd->base[k],
+                                                                      kd->npts[k], kd->kpos);
+    NBG_LAUNCHED(1 + T + (nleaves ? 1 : 0));
     if (cudaStreamSynchronize(st) != cudaSuccess) {
         ctx->err = "KD replica extents failed";
         return NBG_ERR_CUDA;
@@ -1099,61 +1159,90 @@ static int kd_build(Context* ctx, Tile* t, uint32_t small_max, cudaStream_t st) 
     return NBG_OK;
 }
 
-int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
-    if (t->kd && t->kd->built) return NBG_OK;
-    if (!t->kd) t->kd = new KdReplica();
-    KdReplica* kd = t->kd;
-    const uint64_t n = t->n;
-    kd->n = n;
-    int rc = NBG_OK;
-    if (!kd->rx) {
-        rc = kd_alloc(ctx, (void**)&kd->rx, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->ry, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->rz, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->rid, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->mlpos, n * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->mrpos, n * 4, kd);
-        kd->seg_cap = (uint32_t)(n / 50 + 64);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[0], kd->seg_cap * sizeof(KdSeg), kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[1], kd->seg_cap * sizeof(KdSeg), kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg2, kd->seg_cap * sizeof(KdSeg), kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->small, kd->seg_cap * sizeof(KdSeg), kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->split, kd->seg_cap * sizeof(KdSplit), kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->nt, (kd->seg_cap + 1) * 4, kd);
-        kd->leaf_cap = (uint32_t)(n / 16 + 1024);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->leaves, (size_t)kd->leaf_cap * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->counters, 64, kd);
-        size_t b1 = 0;
-        cub::DeviceScan::ExclusiveSum(nullptr, b1, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                      (int)(n / KD_TILE + kd->seg_cap + 2));
-        kd->scan_bytes = b1;
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->scan_tmp, b1, kd);
-        kd->node_cap = 0;
-        if (rc) return rc;
+// Builds one forest holding the replicas of every listed tile that has none.
+int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t st) {
+    std::vector<Tile*> todo;
+    for (int i = 0; i < count; ++i)
+        if (!(tiles[i]->kd && tiles[i]->kd->built) && tiles[i]->n > 0) todo.push_back(tiles[i]);
+    if (todo.empty()) return NBG_OK;
+    for (Tile* t : todo) kd_free(ctx, t);
+    KdForest* kd = new KdForest();
+    kd->ntrees = (int)todo.size();
+    uint64_t n = 0;
+    for (Tile* t : todo) {
+        kd->base.push_back(n);
+        kd->npts.push_back(t->n);
+        kd->tfh.push_back(t->tf);
+        n += t->n;
     }
-    // nodes: initial guess, grown as needed
-    rc = kd_grow_nodes(ctx, kd, (uint32_t)(n / 25 + 64), st);
-    if (rc) return rc;
-    rc = kd_build(ctx, t, KD_WARP_MAX, st);
-    if (rc == KD_RETRY) {
-        // a warp subtree overflowed its stack or the node arrays: redo the
-        // whole build with the level passes only
-        rc = kd_grow_nodes(ctx, kd, (uint32_t)std::min<uint64_t>(2 * n + 64, UINT32_MAX), st);
-        if (!rc) rc = kd_build(ctx, t, 0, st);
+    if (n >= (1ull << 32) - 1) {
+        delete kd;
+        ctx->err = "KD replica: more than 2^32 points in one forest";
+        return NBG_ERR_UNSUPPORTED;
+    }
+    kd->n = n;
+    kd->rootbox.assign(6 * (size_t)kd->ntrees, 0.0);
+    const int T = kd->ntrees;
+    int rc = kd_alloc(ctx, (void**)&kd->rx, n * 4, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->ry, n * 4, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->rz, n * 4, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->rid, n * 4, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->mlpos, n * 4, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->mrpos, n * 4, kd);
+    kd->seg_cap = (uint32_t)(n / 50 + 64 + T);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[0], kd->seg_cap * sizeof(KdSeg), kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg[1], kd->seg_cap * sizeof(KdSeg), kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg2, kd->seg_cap * sizeof(KdSeg), kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->small, kd->seg_cap * sizeof(KdSeg), kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->split, kd->seg_cap * sizeof(KdSplit), kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->nt, (kd->seg_cap + 1) * 4, kd);
+    kd->leaf_cap = (uint32_t)(n / 16 + 1024 + T);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->leaves, (size_t)kd->leaf_cap * 4, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->counters, 64, kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->tfs, (size_t)T * sizeof(Transform), kd);
+    size_t b1 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b1, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (int)(n / KD_TILE + kd->seg_cap + 2));
+    kd->scan_bytes = b1;
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->scan_tmp, b1, kd);
+    if (!rc) rc = kd_grow_nodes(ctx, kd, (uint32_t)(n / 25 + 64 + 2 * (uint64_t)T), st);
+    if (!rc) {
+        rc = kd_build(ctx, kd, todo.data(), KD_WARP_MAX, st);
         if (rc == KD_RETRY) {
-            ctx->err = "KD replica build ran out of node capacity";
-            rc = NBG_ERR_UNSUPPORTED;
+            // a warp subtree overflowed its stack or the node arrays: redo the
+            // whole build with the level passes only
+            rc = kd_grow_nodes(ctx, kd, (uint32_t)std::min<uint64_t>(2 * n + 64 + 2 * (uint64_t)T, UINT32_MAX), st);
+            if (!rc) rc = kd_build(ctx, kd, todo.data(), 0, st);
+            if (rc == KD_RETRY) {
+                ctx->err = "KD replica build ran out of node capacity";
+                rc = NBG_ERR_UNSUPPORTED;
+            }
         }
     }
-    if (rc) return rc;
-    kd->built = true;
+    if (rc) {
+        kd_forest_free(ctx, kd);
+        return rc;
+    }
+    for (int k = 0; k < T; ++k) {
+        KdReplica* v = new KdReplica();
+        v->f = kd;
+        v->tree = k;
+        v->built = true;
+        todo[k]->kd = v;
+    }
+    kd->refs = T;
     return NBG_OK;
+}
+
+int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
+    Tile* one[1] = {t};
+    return kd_ensure_many(ctx, one, 1, st);
 }
 
 bool kd_built(const Tile* t) { return t->kd && t->kd->built; }
 
 KdOrder kd_order(const Tile* t) {
-    const KdReplica* kd = t->kd;
+    const KdForest* kd = t->kd->f;
     KdOrder o;
     o.c1 = kd->c1;
     o.c2 = kd->c2;
@@ -1162,10 +1251,14 @@ KdOrder kd_order(const Tile* t) {
     o.dlo = kd->dlo;
     o.dhi = kd->dhi;
     o.kpos = kd->kpos;
+    o.root = t->kd->tree;
+    o.base = kd->base[t->kd->tree];
     return o;
 }
 
-static KdDev kd_view(const KdReplica* kd) {
+static KdDev kd_view(const Tile* t) {
+    const KdForest* kd = t->kd->f;
+    const int k = t->kd->tree;
     KdDev v;
     v.rx = kd->rx;
     v.ry = kd->ry;
@@ -1178,9 +1271,10 @@ static KdDev kd_view(const KdReplica* kd) {
     v.ne = kd->ne;
     v.dlo = kd->dlo;
     v.dhi = kd->dhi;
+    v.root = k;
     for (int d = 0; d < 3; ++d) {
-        v.root_lo[d] = kd->root_lo[d];
-        v.root_hi[d] = kd->root_hi[d];
+        v.root_lo[d] = kd->rootbox[6 * k + d];
+        v.root_hi[d] = kd->rootbox[6 * k + 3 + d];
     }
     return v;
 }
@@ -1189,7 +1283,7 @@ static KdDev kd_view(const KdReplica* kd) {
 static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
                           uint32_t** nbr, uint32_t** counts, cudaStream_t st) {
     if (K > KD_CAP) return NBG_ERR_INVALID;
-    KdReplica* kd = t->kd;
+    KdForest* kd = t->kd->f;
     *nbr = nullptr;
     *counts = nullptr;
     int arc = ctx_alloc(ctx, (void**)nbr, (size_t)nrows * K * 4);
@@ -1201,7 +1295,7 @@ static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, ui
         return arc;
     }
     cudaMemsetAsync(kd->counters + 2, 0, 4, st);
-    kd_search_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(kd_view(kd), t->tf, t->x, t->y, t->z,
+    kd_search_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(kd_view(t), t->tf, t->x, t->y, t->z,
                                                           rows, nrows, K, *nbr, *counts,
                                                           kd->counters + 2);
     NBG_LAUNCHED(1);
@@ -1262,27 +1356,53 @@ int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_
     return rc;
 }
 
-// Test hook: copies the replica's point order (ids) and node arrays out.
+// Test hook: copies the tile's replica out (point order as ids, and its
+// tree's nodes renumbered in breadth-first order from its root, ranges
+// relative to the tile).
 int kd_export(Context* ctx, Tile* t, uint32_t* vind, uint32_t* nnodes, int32_t* c1, int32_t* c2,
               int32_t* feat, double* dlo, double* dhi, uint32_t* nb, uint32_t* ne, uint32_t cap,
               cudaStream_t st) {
     int rc = kd_ensure(ctx, t, st);
     if (rc) return rc;
-    KdReplica* kd = t->kd;
-    *nnodes = kd->node_count;
-    cudaMemcpyAsync(vind, kd->rid, t->n * 4, cudaMemcpyDeviceToHost, st);
-    const uint32_t m = std::min(cap, kd->node_count);
-    if (m) {
-        cudaMemcpyAsync(c1, kd->c1, m * 4, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(c2, kd->c2, m * 4, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(feat, kd->feat, m * 4, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(dlo, kd->dlo, m * 8, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(dhi, kd->dhi, m * 8, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(nb, kd->nb, m * 4, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(ne, kd->ne, m * 4, cudaMemcpyDeviceToHost, st);
+    const KdForest* kd = t->kd->f;
+    const int k = t->kd->tree;
+    const uint64_t base = kd->base[k];
+    const uint32_t nn = kd->node_count;
+    std::vector<int32_t> hc1(nn), hc2(nn), hf(nn);
+    std::vector<uint32_t> hnb(nn), hne(nn);
+    std::vector<double> hlo(nn), hhi(nn);
+    cudaMemcpyAsync(vind, kd->rid + base, t->n * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hc1.data(), kd->c1, nn * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hc2.data(), kd->c2, nn * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hf.data(), kd->feat, nn * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hlo.data(), kd->dlo, nn * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hhi.data(), kd->dhi, nn * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hnb.data(), kd->nb, nn * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hne.data(), kd->ne, nn * 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return NBG_ERR_CUDA;
+    std::vector<int32_t> order{(int32_t)k};
+    for (size_t q = 0; q < order.size(); ++q) {
+        const int32_t v = order[q];
+        if (hc1[v] >= 0) {
+            order.push_back(hc1[v]);
+            order.push_back(hc2[v]);
+        }
     }
-    return cudaStreamSynchronize(st) == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+    std::vector<int32_t> newid(nn, -1);
+    for (size_t q = 0; q < order.size(); ++q) newid[order[q]] = (int32_t)q;
+    *nnodes = (uint32_t)order.size();
+    const uint32_t m = std::min<uint32_t>(cap, (uint32_t)order.size());
+    for (uint32_t q = 0; q < m; ++q) {
+        const int32_t v = order[q];
+        c1[q] = hc1[v] >= 0 ? newid[hc1[v]] : -1;
+        c2[q] = hc2[v] >= 0 ? newid[hc2[v]] : -1;
+        feat[q] = hf[v];
+        dlo[q] = hlo[v];
+        dhi[q] = hhi[v];
+        nb[q] = (uint32_t)(hnb[v] - base);
+        ne[q] = (uint32_t)(hne[v] - base);
+    }
+    return NBG_OK;
 }
 
 }  // namespace nbg
-

@@ -380,6 +380,13 @@ __device__ __forceinline__ void finish_row(const QueryArgs& a, const uint64_t i)
     nbg_finish_row(a.grp, a.tf, a.ex, id, (int)n, M, qraw);
 }
 
+// Autotuning sample: block b answers rows [b*stride, b*stride + 128).
+template <int KS>
+__global__ void __launch_bounds__(128) knn_select_sample_kernel(const QueryArgs a, uint64_t stride) {
+    const uint64_t i = blockIdx.x * stride + threadIdx.x;
+    if (i < a.n) select_row<KS>(a, i);
+}
+
 __global__ void __launch_bounds__(128) knn_finish_kernel(const QueryArgs a) {
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i < a.n) finish_row(a, i);
@@ -520,7 +527,7 @@ static constexpr int TIE_CAP = 32;
 // True when the reference's search meets replica position pa before pb.
 __device__ __forceinline__ bool kd_meets_first(const KdOrder& kd, const double q[3], uint32_t pa,
                                                uint32_t pb) {
-    int node = 0;
+    int node = kd.root;
     for (int depth = 0; depth < 64; ++depth) {
         const int a = __ldg(&kd.c1[node]);
         if (a < 0) break;
@@ -653,7 +660,8 @@ __global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
             if ((taken >> t) & 1u) continue;
             if (best < 0 || d64[t] < d64[best] ||
                 (d64[t] == d64[best] &&
-                 kd_meets_first(a.kd, q64, __ldg(&a.kd.kpos[f.gid[t]]), __ldg(&a.kd.kpos[f.gid[best]]))))
+                 kd_meets_first(a.kd, q64, __ldg(&a.kd.kpos[a.kd.base + f.gid[t]]),
+                                __ldg(&a.kd.kpos[a.kd.base + f.gid[best]]))))
                 best = t;
         }
         taken |= 1u << best;
@@ -817,6 +825,47 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
 }
 
 int slots_for_k(int K) { return slots_for(K); }
+
+struct SampleArgs {
+    QueryArgs q;
+    uint64_t stride;
+    unsigned blocks;
+    cudaStream_t stream;
+};
+
+template <int KS>
+struct SampleLauncher {
+    using Args = SampleArgs;
+    static int run(const SampleArgs& s) {
+        if (!s.blocks) return NBG_OK;
+        knn_select_sample_kernel<KS><<<s.blocks, 128, 0, s.stream>>>(s.q, s.stride);
+        NBG_LAUNCHED(1);
+        return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+    }
+};
+
+int launch_select_sample(Context* ctx, const QueryLaunch& ql, uint64_t stride, unsigned blocks,
+                         cudaStream_t stream) {
+    (void)ctx;
+    SampleArgs s{};
+    s.q.gv = grid_view(ql.tile);
+    s.q.gp = ql.tile->gp;
+    s.q.n = ql.tile->n;
+    s.q.K = ql.K;
+    s.q.rmax = ql.rmax;
+    s.q.grp = ql.grp;
+    s.q.tf = ql.tile->tf;
+    s.q.ex = ql.ex;
+    s.q.exact_rows = ql.exact_rows;
+    s.q.counters = ql.counters;
+    s.q.ties = ql.ties;
+    s.q.tie_cap = ql.tie_cap;
+    s.q.sums = ql.sums;
+    s.stride = stride;
+    s.blocks = blocks;
+    s.stream = stream;
+    return dispatch_slots<SampleLauncher>(ql.K, s);
+}
 
 int launch_select_queue(Context* ctx, int K, const BatchJob* jobs, int njobs, uint64_t items,
                         unsigned long long* head, cudaStream_t stream) {

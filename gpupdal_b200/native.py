@@ -154,7 +154,7 @@ class Context:
             ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code)
         return ex, stats
 
-    def run_batch(self, tiles, stages, outputs, optimal=None, graph=True,
+    def run_batch(self, tiles, stages, outputs, optimal=None, graph=True, autotune=False,
                   exception_capacity=1 << 16, stream=None):
         """nbg_run_batch over `tiles` (list of Tile); stages[i] is the stage
         list of tile i, outputs[i] its device abi.Columns list, optimal[i]
@@ -184,7 +184,8 @@ class Context:
             it.n_exceptions = ctypes.cast(ctypes.addressof(nex) + 4 * i,
                                           ctypes.POINTER(ctypes.c_uint32))
         stats = abi.RunStats()
-        rc = self.lib.nbg_run_batch(self.h, arr, m, abi.BATCH_GRAPH if graph else 0,
+        flags = (abi.BATCH_GRAPH if graph else 0) | (abi.BATCH_AUTOTUNE if autotune else 0)
+        rc = self.lib.nbg_run_batch(self.h, arr, m, flags,
                                     ctypes.byref(stats), ctypes.c_void_p(stream) if stream else None)
         self._check(rc)
         out = []
@@ -246,6 +247,18 @@ class Tile:
     def tune(self, cell_factor=4.0, fixed_cell=0):
         self.ctx._check(self.ctx.lib.nbg_tile_tune(self.ctx.h, self.h, float(cell_factor),
                                                    int(fixed_cell)))
+
+    def autotune(self, knn, candidates=None, use_cache=False):
+        """Cell factor chosen by the library's autotuner (applied to the tile)."""
+        cand = None
+        cnt = 0
+        if candidates is not None:
+            cand = (ctypes.c_float * len(candidates))(*candidates)
+            cnt = len(candidates)
+        out = ctypes.c_float(0)
+        self.ctx._check(self.ctx.lib.nbg_tile_autotune(self.ctx.h, self.h, int(knn), cand, cnt,
+                                                       int(use_cache), ctypes.byref(out), None))
+        return out.value
 
     def free(self):
         if getattr(self, "h", None) and self.ctx.h:

@@ -94,7 +94,9 @@ typedef struct nbg_stage_opts {
     int32_t always_up;     /* normal: flip so that NormalZ >= 0              */
     int32_t has_viewpoint; /* normal: orient towards viewpoint[]             */
     double viewpoint[3];
-    int32_t refine;        /* normal: accepted, output-neutral (see DESIGN)  */
+    int32_t refine;        /* normal: accepted; output-neutral in the
+                              reference (NormalFilter.cpp:184-286 refines a
+                              copy of the normal)                            */
     int32_t normalize;     /* eigenvalues: divide by their sum               */
     uint32_t feature_mask; /* covariancefeatures: NBG_FEAT_* bits            */
     int32_t mode;          /* covariancefeatures: NBG_MODE_*                 */
@@ -175,6 +177,14 @@ int nbg_tile_free(nbg_context* ctx, nbg_tile* tile);
  * (the grid is rebuilt).  Used by the autotuner; no counterpart in the
  * reference (whose KD tree has no tunable). */
 int nbg_tile_tune(nbg_context* ctx, nbg_tile* tile, float cell_factor, int32_t fixed_cell);
+/* Autotuner: builds the tile's grid with each candidate cell factor (null:
+ * 1, 1.5, 2, 3, 4, 6), times the select pass on a 65,536-row sample spread
+ * over the tile, and keeps the factor with the least estimated grid + query
+ * time (rows the ring search would defer charged at 20 us each).  The choice
+ * is cached per (log2 points, neighbour slots) class of the context; with
+ * use_cache a cached class is applied without measuring. */
+int nbg_tile_autotune(nbg_context* ctx, nbg_tile* tile, int32_t knn, const float* candidates,
+                      int32_t n_candidates, int32_t use_cache, float* chosen, void* stream);
 uint64_t nbg_tile_size(const nbg_tile* tile);
 
 /* Run stages over a resident tile.  Stages sharing knn share one fused
@@ -219,6 +229,8 @@ typedef struct nbg_batch_item {
 } nbg_batch_item;
 
 #define NBG_BATCH_GRAPH 1u            /* capture the queue launches in a graph */
+#define NBG_BATCH_AUTOTUNE 2u         /* cell factor per tile from the autotuner
+                                         (cached per size/knn class)          */
 
 int nbg_run_batch(nbg_context* ctx, const nbg_batch_item* items, int32_t n_items,
                   uint32_t flags, nbg_run_stats* stats, void* stream);
