@@ -38,6 +38,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mpts/s k=16 normals+eigen, served vs plain @<=1e-5 rel err; p50/p99 latency"
 BYTES_PER_POINT = 20 + 8 * 7 + 1  # sorted xyz+id, id permutation, 7 f64 outputs, status
+# DRAM bytes per point of knn_select_kernel + knn_finish_kernel (read + write) from one
+# ncu capture of the same workload at 4M points: (178.4 + 691.4) MB / 4e6
+TRAFFIC_PER_POINT = 217.5
 
 
 def parse():
@@ -236,14 +239,29 @@ def served_leg(ctx, args):
 
 
 def dist_setup():
+    """One process per GPU (torchrun env); NCCL on GPUs, gloo without (host-logic tests)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
-        import torch.distributed as dist
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
+
+
+def rank_max(v, ws):
+    """Max of a float over the ranks (the timing rule: slowest rank)."""
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def run_reference(args, ws, rank):
@@ -320,12 +338,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(v):
-        if ws == 1:
-            return v
-        import torch.distributed as dist
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(v, ws)
 
     def timed(fn, steps):
         stats = []
@@ -375,7 +388,9 @@ def main():
                 "d2h_bytes_per_step": 8 * sum(nd) * n},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
+                     "frac": achieved / hbm, "traffic": TRAFFIC_PER_POINT * n,
+                     "traffic_source": "ncu dram bytes of select+finish on the 4M-point tile, "
+                                       "scaled per point",
                      "kernel": "knn_select_kernel+knn_finish_kernel", "peak_source": peak_kind,
                      "bytes_per_point": BYTES_PER_POINT},
         "clocks": clk,
