@@ -38,7 +38,11 @@
 namespace nbg {
 
 static constexpr int KD_LEAF = 100;
-static constexpr int KD_TILE = 256;
+// Level passes: tiles of KD_TILE elements, KD_THREADS threads of KD_ITEMS
+// elements each (segments on the level passes hold more than 4096 points).
+static constexpr int KD_TILE = 1024;
+static constexpr int KD_THREADS = 256;
+static constexpr int KD_ITEMS = KD_TILE / KD_THREADS;
 // Segments of at most this many points are finished, subtree and all, by
 // one warp (kd_warp_build_kernel) instead of level by level.
 static constexpr uint32_t KD_WARP_MAX = 4096;
@@ -57,7 +61,7 @@ struct KdSeg {
 
 struct KdSplit {
     int32_t f;
-    int32_t pad;
+    uint32_t eq;  // points equal to the cut value (pass 2 has work only when > 0)
     double cutval;
     uint32_t L, m;    // pass 1: count below, misplaced pairs
     uint32_t L2, m2;  // pass 2 on [L, n)
@@ -115,6 +119,8 @@ struct KdForest {
     KdSeg* seg[2] = {nullptr, nullptr};
     KdSeg* seg2 = nullptr;
     KdSplit* split = nullptr;
+    KdSplit* split2 = nullptr;     // pass-2 segments' split records
+    uint32_t* seg2_from = nullptr; // pass-2 segment -> its level segment
     uint32_t seg_cap = 0;
     KdSeg* small = nullptr;      // segments left for the warp builder
     uint32_t* leaves = nullptr;  // leaves made by the level passes (bbox pending)
@@ -122,13 +128,13 @@ struct KdForest {
     // tiles
     uint32_t* nt = nullptr;        // per segment tile count, then prefix (seg_cap+1)
     uint32_t* tile_seg = nullptr;
-    uint32_t* tile_cnt = nullptr;  // per tile count, then prefix (tile_cap+1)
+    unsigned long long* tile_cnt = nullptr;  // per tile counts (lt | eq << 32), then prefix
     int32_t* tile_mm = nullptr;    // per tile extents (6 ints)
     uint32_t tile_cap = 0;
     void* scan_tmp = nullptr;
     size_t scan_bytes = 0;
     uint32_t* counters = nullptr;  // [0] next segments, [1] nodes, [2] errors, [3] small
-                                   // segments, [4] leaves
+                                   // segments, [4] leaves, [5] pass-2 segments
     uint32_t dl_cap = 0;
     uint64_t bytes = 0;
     std::vector<std::pair<void*, size_t>> blocks;  // device blocks owned
@@ -185,20 +191,27 @@ __global__ void kd_minmax_init_kernel(KdSplit* sp, uint32_t S) {
 }
 
 // Per-tile extents (block reduction) into tile_mm[6*t]: min x,y,z, max x,y,z.
-__global__ void __launch_bounds__(KD_TILE) kd_minmax_kernel(const KdSeg* segs, const uint32_t* tile_first,
-                                                            const uint32_t* tile_seg,
-                                                            const int32_t* rx, const int32_t* ry,
-                                                            const int32_t* rz, int32_t* tile_mm) {
-    __shared__ int32_t red[KD_TILE / 32][6];
+__global__ void __launch_bounds__(KD_THREADS) kd_minmax_kernel(const KdSeg* segs, const uint32_t* tile_first,
+                                                               const uint32_t* tile_seg,
+                                                               const int32_t* rx, const int32_t* ry,
+                                                               const int32_t* rz, int32_t* tile_mm) {
+    __shared__ int32_t red[KD_THREADS / 32][6];
     const uint32_t t = blockIdx.x;
     const uint32_t s = tile_seg[t];
     const KdSeg sg = segs[s];
-    const uint32_t i = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
+    const uint32_t i0 = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
     int32_t v[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, w[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
-    if (i < sg.end) {
-        v[0] = w[0] = rx[i];
-        v[1] = w[1] = ry[i];
-        v[2] = w[2] = rz[i];
+#pragma unroll
+    for (int k = 0; k < KD_ITEMS; ++k) {
+        const uint32_t i = i0 + k * KD_THREADS;
+        if (i < sg.end) {
+            const int32_t c[3] = {rx[i], ry[i], rz[i]};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                v[d] = min(v[d], c[d]);
+                w[d] = max(w[d], c[d]);
+            }
+        }
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -215,20 +228,20 @@ __global__ void __launch_bounds__(KD_TILE) kd_minmax_kernel(const KdSeg* segs, c
     __syncthreads();
     if (threadIdx.x < 6) {
         int32_t r = red[0][threadIdx.x];
-        for (int k = 1; k < KD_TILE / 32; ++k)
+        for (int k = 1; k < KD_THREADS / 32; ++k)
             r = threadIdx.x < 3 ? min(r, red[k][threadIdx.x]) : max(r, red[k][threadIdx.x]);
         tile_mm[6 * (size_t)t + threadIdx.x] = r;
     }
 }
 
-// One warp per segment folds its tiles' extents.
-__global__ void kd_seg_minmax_kernel(uint32_t S, const uint32_t* tile_first, const int32_t* tile_mm,
-                                     KdSplit* sp) {
-    const uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+// One block per segment folds its tiles' extents.
+__global__ void __launch_bounds__(KD_THREADS) kd_seg_minmax_kernel(uint32_t S, const uint32_t* tile_first,
+                                                                   const int32_t* tile_mm, KdSplit* sp) {
+    __shared__ int32_t red[KD_THREADS / 32][6];
+    const uint32_t s = blockIdx.x;
     if (s >= S) return;
     int32_t v[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, w[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
-    for (uint32_t t = tile_first[s] + lane; t < tile_first[s + 1]; t += 32) {
+    for (uint32_t t = tile_first[s] + threadIdx.x; t < tile_first[s + 1]; t += KD_THREADS) {
         for (int d = 0; d < 3; ++d) {
             v[d] = min(v[d], tile_mm[6 * (size_t)t + d]);
             w[d] = max(w[d], tile_mm[6 * (size_t)t + 3 + d]);
@@ -239,11 +252,20 @@ __global__ void kd_seg_minmax_kernel(uint32_t S, const uint32_t* tile_first, con
         v[d] = __reduce_min_sync(0xffffffffu, v[d]);
         w[d] = __reduce_max_sync(0xffffffffu, w[d]);
     }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (lane == 0) {
         for (int d = 0; d < 3; ++d) {
-            sp[s].mn[d] = v[d];
-            sp[s].mx[d] = w[d];
+            red[warp][d] = v[d];
+            red[warp][3 + d] = w[d];
         }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        int32_t r = red[0][threadIdx.x];
+        for (int k = 1; k < KD_THREADS / 32; ++k)
+            r = threadIdx.x < 3 ? min(r, red[k][threadIdx.x]) : max(r, red[k][threadIdx.x]);
+        if (threadIdx.x < 3) sp[s].mn[threadIdx.x] = r;
+        else sp[s].mx[threadIdx.x - 3] = r;
     }
 }
 
@@ -310,31 +332,53 @@ __device__ __forceinline__ bool kd_pred(double v, double cut) {
     return PASS == 1 ? (v < cut) : (v <= cut);
 }
 
+// Per tile: predicate count in the low 32 bits and, on pass 1, the count of
+// points equal to the cut value in the high 32 bits.
 template <int PASS>
-__global__ void __launch_bounds__(KD_TILE) kd_count_kernel(const KdSeg* segs, const uint32_t* tile_first,
-                                                           const uint32_t* tile_seg,
-                                                           const KdSplit* sp, const int32_t* rx,
-                                                           const int32_t* ry, const int32_t* rz,
-                                                           const Transform* tfs, uint32_t* tile_cnt) {
+__global__ void __launch_bounds__(KD_THREADS) kd_count_kernel(const KdSeg* segs, const uint32_t* tile_first,
+                                                              const uint32_t* tile_seg,
+                                                              const KdSplit* sp, const int32_t* rx,
+                                                              const int32_t* ry, const int32_t* rz,
+                                                              const Transform* tfs,
+                                                              unsigned long long* tile_cnt) {
+    __shared__ unsigned long long red[KD_THREADS / 32];
     const uint32_t t = blockIdx.x;
     const uint32_t s = tile_seg[t];
     const KdSeg sg = segs[s];
     const Transform& tf = tfs[sg.pad];
     const int f = sp[s].f;
     const double cut = sp[s].cutval;
-    const uint32_t i = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
-    bool p = false;
-    if (i < sg.end) p = kd_pred<PASS>(ref_coord(kd_coord(rx, ry, rz, f, i), tf.scale[f], tf.offset[f]), cut);
-    int c = __syncthreads_count(p);
-    if (threadIdx.x == 0) tile_cnt[t] = (uint32_t)c;
+    const int32_t* rc = f == 0 ? rx : (f == 1 ? ry : rz);
+    const uint32_t i0 = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
+    unsigned long long c = 0;
+#pragma unroll
+    for (int k = 0; k < KD_ITEMS; ++k) {
+        const uint32_t i = i0 + k * KD_THREADS;
+        if (i < sg.end) {
+            const double v = ref_coord(rc[i], tf.scale[f], tf.offset[f]);
+            c += kd_pred<PASS>(v, cut) ? 1ull : 0ull;
+            if (PASS == 1 && v == cut) c += 1ull << 32;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long r = 0;
+        for (int k = 0; k < KD_THREADS / 32; ++k) r += red[k];
+        tile_cnt[t] = r;
+    }
 }
 
-// L and the number of misplaced pairs m for each segment
+// L and the number of misplaced pairs m for each segment (one warp each: the
+// count before L inside L's tile is recounted by the warp).
 template <int PASS>
 __global__ void kd_seg_count_kernel(const KdSeg* segs, uint32_t S, const uint32_t* tile_first,
-                                    const uint32_t* tile_pref, KdSplit* sp, const int32_t* rx,
+                                    const unsigned long long* tile_pref, KdSplit* sp, const int32_t* rx,
                                     const int32_t* ry, const int32_t* rz, const Transform* tfs) {
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (s >= S) return;
     const KdSeg sg = segs[s];
     const Transform& tf = tfs[sg.pad];
@@ -342,18 +386,26 @@ __global__ void kd_seg_count_kernel(const KdSeg* segs, uint32_t S, const uint32_
     const uint32_t len = sg.end - sg.begin;
     const int f = sp[s].f;
     const double cut = sp[s].cutval;
-    uint32_t L = tile_pref[first + nt] - tile_pref[first];
-    uint32_t tl = L / KD_TILE;
+    const int32_t* rc = f == 0 ? rx : (f == 1 ? ry : rz);
+    const unsigned long long tot = tile_pref[first + nt] - tile_pref[first];
+    const uint32_t L = (uint32_t)tot, eq = (uint32_t)(tot >> 32);
+    const uint32_t tl = L / KD_TILE;
     uint32_t pleft = 0;
     if (len) {
-        pleft = tile_pref[first + tl] - tile_pref[first];
-        for (uint32_t i = sg.begin + tl * KD_TILE; i < sg.begin + L; ++i)
-            pleft += kd_pred<PASS>(ref_coord(kd_coord(rx, ry, rz, f, i), tf.scale[f], tf.offset[f]), cut);
+        pleft = (uint32_t)(tile_pref[first + tl] - tile_pref[first]);
+        for (uint32_t base = sg.begin + tl * KD_TILE; base < sg.begin + L; base += 32) {
+            const uint32_t i = base + lane;
+            const bool p = i < sg.begin + L &&
+                           kd_pred<PASS>(ref_coord(rc[i], tf.scale[f], tf.offset[f]), cut);
+            pleft += __popc(__ballot_sync(0xffffffffu, p));
+        }
     }
-    uint32_t m = L - pleft;
+    if (lane) return;
+    const uint32_t m = L - pleft;
     if (PASS == 1) {
         sp[s].L = L;
         sp[s].m = m;
+        sp[s].eq = eq;
     } else {
         sp[s].L2 = L;
         sp[s].m2 = m;
@@ -361,14 +413,14 @@ __global__ void kd_seg_count_kernel(const KdSeg* segs, uint32_t S, const uint32_
 }
 
 template <int PASS>
-__global__ void __launch_bounds__(KD_TILE) kd_classify_kernel(const KdSeg* segs, const uint32_t* tile_first,
-                                                              const uint32_t* tile_seg,
-                                                              const uint32_t* tile_pref,
-                                                              const KdSplit* sp, const int32_t* rx,
-                                                              const int32_t* ry, const int32_t* rz,
-                                                              const Transform* tfs, uint32_t* mlpos,
-                                                              uint32_t* mrpos) {
-    typedef cub::BlockScan<uint32_t, KD_TILE> Scan;
+__global__ void __launch_bounds__(KD_THREADS) kd_classify_kernel(const KdSeg* segs, const uint32_t* tile_first,
+                                                                 const uint32_t* tile_seg,
+                                                                 const unsigned long long* tile_pref,
+                                                                 const KdSplit* sp, const int32_t* rx,
+                                                                 const int32_t* ry, const int32_t* rz,
+                                                                 const Transform* tfs, uint32_t* mlpos,
+                                                                 uint32_t* mrpos) {
+    typedef cub::BlockScan<uint32_t, KD_THREADS> Scan;
     __shared__ typename Scan::TempStorage tmp;
     const uint32_t t = blockIdx.x;
     const uint32_t s = tile_seg[t];
@@ -376,55 +428,87 @@ __global__ void __launch_bounds__(KD_TILE) kd_classify_kernel(const KdSeg* segs,
     const Transform& tf = tfs[sg.pad];
     const int f = sp[s].f;
     const double cut = sp[s].cutval;
+    const int32_t* rc = f == 0 ? rx : (f == 1 ? ry : rz);
     const uint32_t L = PASS == 1 ? sp[s].L : sp[s].L2;
     const uint32_t m = PASS == 1 ? sp[s].m : sp[s].m2;
-    const uint32_t i = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
-    uint32_t p = 0;
-    if (i < sg.end) p = kd_pred<PASS>(ref_coord(kd_coord(rx, ry, rz, f, i), tf.scale[f], tf.offset[f]), cut);
-    uint32_t rank;
+    // blocked arrangement: thread j owns elements j*KD_ITEMS .. j*KD_ITEMS+KD_ITEMS-1
+    const uint32_t i0 = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x * KD_ITEMS;
+    uint32_t p[KD_ITEMS], rank[KD_ITEMS];
+#pragma unroll
+    for (int k = 0; k < KD_ITEMS; ++k) {
+        const uint32_t i = i0 + k;
+        p[k] = i < sg.end && kd_pred<PASS>(ref_coord(rc[i], tf.scale[f], tf.offset[f]), cut);
+    }
     Scan(tmp).ExclusiveSum(p, rank);
-    if (i >= sg.end) return;
-    const uint32_t prank = tile_pref[t] - tile_pref[tile_first[s]] + rank;  // P before i in segment
-    const uint32_t li = i - sg.begin;
-    if (li < L) {
-        if (!p) mlpos[sg.begin + (li - prank)] = i;
-    } else if (p) {
-        const uint32_t rml = prank - (L - m);
-        mrpos[sg.begin + (m - 1 - rml)] = i;
+    const uint32_t before = (uint32_t)(tile_pref[t] - tile_pref[tile_first[s]]);
+#pragma unroll
+    for (int k = 0; k < KD_ITEMS; ++k) {
+        const uint32_t i = i0 + k;
+        if (i >= sg.end) break;
+        const uint32_t prank = before + rank[k];  // predicate holders before i in the segment
+        const uint32_t li = i - sg.begin;
+        if (li < L) {
+            if (!p[k]) mlpos[sg.begin + (li - prank)] = i;
+        } else if (p[k]) {
+            const uint32_t rml = prank - (L - m);
+            mrpos[sg.begin + (m - 1 - rml)] = i;
+        }
     }
 }
 
 template <int PASS>
-__global__ void __launch_bounds__(KD_TILE) kd_swap_kernel(const KdSeg* segs, const uint32_t* tile_first,
-                                                          const uint32_t* tile_seg, const KdSplit* sp,
-                                                          const uint32_t* mlpos,
-                                                          const uint32_t* mrpos, int32_t* rx,
-                                                          int32_t* ry, int32_t* rz, uint32_t* rid) {
+__global__ void __launch_bounds__(KD_THREADS) kd_swap_kernel(const KdSeg* segs, const uint32_t* tile_first,
+                                                             const uint32_t* tile_seg, const KdSplit* sp,
+                                                             const uint32_t* mlpos,
+                                                             const uint32_t* mrpos, int32_t* rx,
+                                                             int32_t* ry, int32_t* rz, uint32_t* rid) {
     const uint32_t t = blockIdx.x;
     const uint32_t s = tile_seg[t];
     const KdSeg sg = segs[s];
     const uint32_t m = PASS == 1 ? sp[s].m : sp[s].m2;
-    const uint32_t li = (t - tile_first[s]) * KD_TILE + threadIdx.x;
-    if (li >= m) return;
-    const uint32_t a = mlpos[sg.begin + li], b = mrpos[sg.begin + li];
-    int32_t tx = rx[a], ty = ry[a], tz = rz[a];
-    uint32_t ti = rid[a];
-    rx[a] = rx[b];
-    ry[a] = ry[b];
-    rz[a] = rz[b];
-    rid[a] = rid[b];
-    rx[b] = tx;
-    ry[b] = ty;
-    rz[b] = tz;
-    rid[b] = ti;
+#pragma unroll
+    for (int k = 0; k < KD_ITEMS; ++k) {
+        const uint32_t li = (t - tile_first[s]) * KD_TILE + threadIdx.x + k * KD_THREADS;
+        if (li >= m) return;
+        const uint32_t a = mlpos[sg.begin + li], b = mrpos[sg.begin + li];
+        const int32_t tx = rx[a], ty = ry[a], tz = rz[a];
+        const uint32_t ti = rid[a];
+        rx[a] = rx[b];
+        ry[a] = ry[b];
+        rz[a] = rz[b];
+        rid[a] = rid[b];
+        rx[b] = tx;
+        ry[b] = ty;
+        rz[b] = tz;
+        rid[b] = ti;
+    }
 }
 
-__global__ void kd_pass2_segs_kernel(const KdSeg* segs, uint32_t S, const KdSplit* sp, KdSeg* seg2) {
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+// Pass 2 runs only on segments with points equal to the cut value: every
+// other segment has L2 = m2 = 0.  Listed segments start at their L and keep
+// their own split record (copied), written back after the pass.
+__global__ void kd_pass2_plan_kernel(const KdSeg* segs, uint32_t S, KdSplit* sp, KdSeg* seg2,
+                                     KdSplit* split2, uint32_t* seg2_from, uint32_t* count) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
+    const KdSplit p = sp[s];
+    sp[s].L2 = 0;
+    sp[s].m2 = 0;
+    if (p.eq == 0) return;
+    const uint32_t k = atomicAdd(count, 1u);
     KdSeg g = segs[s];
-    g.begin = g.begin + sp[s].L;
-    seg2[s] = g;
+    g.begin = g.begin + p.L;
+    seg2[k] = g;
+    split2[k] = p;
+    seg2_from[k] = s;
+}
+
+__global__ void kd_pass2_done_kernel(uint32_t S2, const KdSplit* split2, const uint32_t* seg2_from,
+                                     KdSplit* sp) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= S2) return;
+    sp[seg2_from[k]].L2 = split2[k].L2;
+    sp[seg2_from[k]].m2 = split2[k].m2;
 }
 
 __global__ void kd_children_kernel(const KdSeg* segs, uint32_t S, const KdSplit* sp, KdSeg* next,
@@ -931,10 +1015,11 @@ static int kd_tiles(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, u
         if (kd->tile_seg) kd_release(ctx, kd, kd->tile_seg);
         if (kd->tile_cnt) kd_release(ctx, kd, kd->tile_cnt);
         if (kd->tile_mm) kd_release(ctx, kd, kd->tile_mm);
-        kd->tile_seg = kd->tile_cnt = nullptr;
+        kd->tile_seg = nullptr;
+        kd->tile_cnt = nullptr;
         kd->tile_mm = nullptr;
         int rc = kd_alloc(ctx, (void**)&kd->tile_seg, (size_t)cap * 4, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->tile_cnt, (size_t)(cap + 1) * 4, kd);
+        if (!rc) rc = kd_alloc(ctx, (void**)&kd->tile_cnt, (size_t)(cap + 1) * 8, kd);
         if (!rc) rc = kd_alloc(ctx, (void**)&kd->tile_mm, (size_t)cap * 24, kd);
         if (rc) return rc;
         kd->tile_cap = cap;
@@ -946,29 +1031,29 @@ static int kd_tiles(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, u
 }
 
 template <int PASS>
-static int kd_pass(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, cudaStream_t st) {
+static int kd_pass(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, KdSplit* sp,
+                   cudaStream_t st) {
     uint32_t ntiles = 0;
     int rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
     if (rc) return rc;
     if (ntiles) {
-        kd_count_kernel<PASS><<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->split,
-                                                          kd->rx, kd->ry, kd->rz, kd->tfs,
-                                                          kd->tile_cnt);
+        kd_count_kernel<PASS><<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg, sp, kd->rx,
+                                                             kd->ry, kd->rz, kd->tfs, kd->tile_cnt);
     }
-    cudaMemsetAsync(kd->tile_cnt + ntiles, 0, 4, st);
+    cudaMemsetAsync(kd->tile_cnt + ntiles, 0, 8, st);
     size_t tb = kd->scan_bytes;
     cub::DeviceScan::ExclusiveSum(kd->scan_tmp, tb, kd->tile_cnt, kd->tile_cnt, (int)(ntiles + 1), st);
-    kd_seg_count_kernel<PASS><<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->nt, kd->tile_cnt,
-                                                               kd->split, kd->rx, kd->ry, kd->rz,
-                                                               kd->tfs);
+    kd_seg_count_kernel<PASS><<<(S * 32 + 255) / 256, 256, 0, st>>>(segs, S, kd->nt, kd->tile_cnt,
+                                                                    sp, kd->rx, kd->ry, kd->rz,
+                                                                    kd->tfs);
     if (ntiles) {
-        kd_classify_kernel<PASS><<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg,
-                                                             kd->tile_cnt, kd->split, kd->rx,
-                                                             kd->ry, kd->rz, kd->tfs, kd->mlpos,
-                                                             kd->mrpos);
-        kd_swap_kernel<PASS><<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->split,
-                                                         kd->mlpos, kd->mrpos, kd->rx, kd->ry,
-                                                         kd->rz, kd->rid);
+        kd_classify_kernel<PASS><<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg,
+                                                                kd->tile_cnt, sp, kd->rx, kd->ry,
+                                                                kd->rz, kd->tfs, kd->mlpos,
+                                                                kd->mrpos);
+        kd_swap_kernel<PASS><<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg, sp,
+                                                            kd->mlpos, kd->mrpos, kd->rx, kd->ry,
+                                                            kd->rz, kd->rid);
     }
     NBG_LAUNCHED(3 + (ntiles ? 3 : 0));
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
@@ -1071,19 +1156,34 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
         rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
         if (rc) return rc;
         if (ntiles) {
-            kd_minmax_kernel<<<ntiles, KD_TILE, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->rx, kd->ry,
-                                                         kd->rz, kd->tile_mm);
-            kd_seg_minmax_kernel<<<(S * 32 + 255) / 256, 256, 0, st>>>(S, kd->nt, kd->tile_mm,
-                                                                      kd->split);
+            kd_minmax_kernel<<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->rx, kd->ry,
+                                                            kd->rz, kd->tile_mm);
+            kd_seg_minmax_kernel<<<S, KD_THREADS, 0, st>>>(S, kd->nt, kd->tile_mm, kd->split);
             NBG_LAUNCHED(1);
         }
         kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->tfs, kd->bmin, kd->bmax);
         NBG_LAUNCHED(2 + (ntiles ? 1 : 0));
-        rc = kd_pass<1>(ctx, kd, segs, S, st);
+        rc = kd_pass<1>(ctx, kd, segs, S, kd->split, st);
         if (rc) return rc;
-        kd_pass2_segs_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg2);
-        rc = kd_pass<2>(ctx, kd, kd->seg2, S, st);
-        if (rc) return rc;
+        // pass 2 only where points equal the cut value
+        cudaMemsetAsync(kd->counters + 5, 0, 4, st);
+        kd_pass2_plan_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg2,
+                                                              kd->split2, kd->seg2_from,
+                                                              kd->counters + 5);
+        uint32_t S2 = 0;
+        cudaMemcpyAsync(&S2, kd->counters + 5, 4, cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            ctx->err = "KD replica pass-2 plan failed";
+            return NBG_ERR_CUDA;
+        }
+        NBG_LAUNCHED(1);
+        if (S2) {
+            rc = kd_pass<2>(ctx, kd, kd->seg2, S2, kd->split2, st);
+            if (rc) return rc;
+            kd_pass2_done_kernel<<<(S2 + 127) / 128, 128, 0, st>>>(S2, kd->split2, kd->seg2_from,
+                                                                   kd->split);
+            NBG_LAUNCHED(1);
+        }
         cudaMemsetAsync(kd->counters, 0, 4, st);
         NBG_LAUNCHED(2);
         kd_children_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->seg[cur ^ 1],
@@ -1195,14 +1295,19 @@ int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t st)
     if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg2, kd->seg_cap * sizeof(KdSeg), kd);
     if (!rc) rc = kd_alloc(ctx, (void**)&kd->small, kd->seg_cap * sizeof(KdSeg), kd);
     if (!rc) rc = kd_alloc(ctx, (void**)&kd->split, kd->seg_cap * sizeof(KdSplit), kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->split2, kd->seg_cap * sizeof(KdSplit), kd);
+    if (!rc) rc = kd_alloc(ctx, (void**)&kd->seg2_from, kd->seg_cap * 4, kd);
     if (!rc) rc = kd_alloc(ctx, (void**)&kd->nt, (kd->seg_cap + 1) * 4, kd);
     kd->leaf_cap = (uint32_t)(n / 16 + 1024 + T);
     if (!rc) rc = kd_alloc(ctx, (void**)&kd->leaves, (size_t)kd->leaf_cap * 4, kd);
     if (!rc) rc = kd_alloc(ctx, (void**)&kd->counters, 64, kd);
     if (!rc) rc = kd_alloc(ctx, (void**)&kd->tfs, (size_t)T * sizeof(Transform), kd);
-    size_t b1 = 0;
+    size_t b1 = 0, b2 = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, b1, (uint32_t*)nullptr, (uint32_t*)nullptr,
                                   (int)(n / KD_TILE + kd->seg_cap + 2));
+    cub::DeviceScan::ExclusiveSum(nullptr, b2, (unsigned long long*)nullptr,
+                                  (unsigned long long*)nullptr, (int)(n / KD_TILE + kd->seg_cap + 2));
+    b1 = std::max(b1, b2);
     kd->scan_bytes = b1;
     if (!rc) rc = kd_alloc(ctx, (void**)&kd->scan_tmp, b1, kd);
     if (!rc) rc = kd_grow_nodes(ctx, kd, (uint32_t)(n / 25 + 64 + 2 * (uint64_t)T), st);
