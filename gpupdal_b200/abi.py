@@ -245,6 +245,30 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_stage_noalloc.restype = ctypes.c_int
     lib.nbg_debug_kd_export.argtypes = [vp, vp] + [vp] * 9 + [ctypes.c_uint32]
     lib.nbg_debug_kd_export.restype = ctypes.c_int
+    cp = ctypes.c_char_p
+    lib.nbg_filter_create.argtypes = [cp, cp, i32, i32, ctypes.POINTER(vp), cp, ctypes.c_size_t]
+    lib.nbg_filter_create.restype = ctypes.c_int
+    lib.nbg_filter_options.argtypes = [vp, ctypes.POINTER(StageOpts)]
+    lib.nbg_filter_options.restype = ctypes.c_int
+    lib.nbg_filter_dims.argtypes = [vp, cp, ctypes.c_size_t]
+    lib.nbg_filter_dims.restype = ctypes.c_int
+    lib.nbg_filter_log.argtypes = [vp]
+    lib.nbg_filter_log.restype = cp
+    lib.nbg_filter_report.argtypes = [vp, ctypes.POINTER(RowException), ctypes.c_uint32, i32, cp,
+                                      ctypes.c_size_t]
+    lib.nbg_filter_report.restype = ctypes.c_int
+    lib.nbg_filter_free.argtypes = [vp]
+    lib.nbg_filter_free.restype = None
+    lib.nbg_pipeline_parse.argtypes = [cp, ctypes.POINTER(vp), cp, ctypes.c_size_t]
+    lib.nbg_pipeline_parse.restype = ctypes.c_int
+    lib.nbg_pipeline_size.argtypes = [vp]
+    lib.nbg_pipeline_size.restype = i32
+    lib.nbg_pipeline_type.argtypes = [vp, i32]
+    lib.nbg_pipeline_type.restype = cp
+    lib.nbg_pipeline_options.argtypes = [vp, i32]
+    lib.nbg_pipeline_options.restype = cp
+    lib.nbg_pipeline_free.argtypes = [vp]
+    lib.nbg_pipeline_free.restype = None
     lib.nbg_run_batch.argtypes = [vp, ctypes.POINTER(BatchItem), i32, ctypes.c_uint32,
                                   ctypes.POINTER(RunStats), vp]
     lib.nbg_run_batch.restype = ctypes.c_int

@@ -207,6 +207,41 @@ int nbg_neighbor_sets(nbg_context* ctx, nbg_tile* tile, int32_t knn,
                       uint32_t* ids_out, int32_t ids_on_device,
                       nbg_run_stats* stats, void* stream);
 
+/* Stage layer ------------------------------------------------------------
+ * PDAL pipeline JSON and the stage logic above nbg_run, so an existing
+ * pipeline is a drop-in.  nbg_filter_create parses one stage's options
+ * object as ProgramArgs would (NormalFilter.cpp:85-97, EigenvaluesFilter.cpp:
+ * 77-87, CovarianceFeaturesFilter.cpp:102-113; value errors as ProgramArgs.hpp:
+ * 415-435), registers its dimensions (addDimensions) and runs prepared()'s
+ * checks; has_optimal_knn / has_optimal_radius say whether the input view
+ * carries those dimensions.  A check the reference throws from returns
+ * NBG_ERR_INVALID with "<stage>: <the reference's message>" in err. */
+typedef struct nbg_filter nbg_filter;
+int nbg_filter_create(const char* type, const char* options_json, int32_t has_optimal_knn,
+                      int32_t has_optimal_radius, nbg_filter** filter, char* err, size_t err_len);
+/* The stage's nbg_stage_opts (knn as the user gave it).  NBG_ERR_UNSUPPORTED
+ * (with *out still filled) for radius/min_k, stride > 1 and optimized. */
+int nbg_filter_options(const nbg_filter* filter, nbg_stage_opts* out);
+/* Registered output dimensions, comma separated, in the library's order. */
+int nbg_filter_dims(const nbg_filter* filter, char* names, size_t len);
+/* Lines the stage logged (prepared() warnings, then per-row skip lines). */
+const char* nbg_filter_log(const nbg_filter* filter);
+/* The reference's reaction to a run's row exceptions for this stage (its
+ * index in the nbg_run call): Info lines appended to the log in point order,
+ * or NBG_ERR_INVALID with the text its loop would throw. */
+int nbg_filter_report(nbg_filter* filter, const nbg_row_exception* exceptions, uint32_t n,
+                      int32_t stage_index, char* err, size_t err_len);
+void nbg_filter_free(nbg_filter* filter);
+
+/* A pipeline JSON (an array of stages, or {"pipeline": [...]}): its stages'
+ * types ("file" for a bare file name) and option objects as JSON text. */
+typedef struct nbg_pipeline nbg_pipeline;
+int nbg_pipeline_parse(const char* json, nbg_pipeline** pipeline, char* err, size_t err_len);
+int32_t nbg_pipeline_size(const nbg_pipeline* pipeline);
+const char* nbg_pipeline_type(const nbg_pipeline* pipeline, int32_t index);
+const char* nbg_pipeline_options(const nbg_pipeline* pipeline, int32_t index);
+void nbg_pipeline_free(nbg_pipeline* pipeline);
+
 /* Batched form -----------------------------------------------------------
  * Many tiles of uneven size and knn in one call: the tiles' grids are built,
  * then one persistent kernel per neighbour-count class drains a device work

@@ -176,3 +176,32 @@ def test_knn_larger_than_cloud(nbg, port):
             outs, ex, _ = nbg.run(tile, [o])
             _, st = port.tree(*(syn.to_double(v) for v in (x, y, z))).run_stage(o, mode=0)
             assert np.array_equal(U.status_from_exceptions(n, ex), st)
+
+
+def test_pipeline_json_runs_the_path_stages(nbg):
+    from gpupdal_b200.stages import run_pipeline
+    g = U.golden("c1_terrain")
+    pipe = ('["input.las", {"type": "filters.normal", "knn": 8}, '
+            '{"type": "filters.eigenvalues", "knn": 8, "normalize": true}, '
+            '{"type": "writers.las", "filename": "out.las"}]')
+    dims, log = run_pipeline(nbg, pipe, g["x"], g["y"], g["z"])
+    assert "not run: file" in log and "not run: writers.las" in log
+    tile = nbg.tile(g["x"], g["y"], g["z"])
+    (nrm,), _, _ = nbg.run(tile, [abi.make_opts(abi.STAGE_NORMAL, knn=8)])
+    (eig,), _, _ = nbg.run(tile, [abi.make_opts(abi.STAGE_EIGENVALUES, knn=8, normalize=True)])
+    for k, name in enumerate(["NormalX", "NormalY", "NormalZ", "Curvature"]):
+        assert np.array_equal(dims[name], nrm[k])
+    for k in range(3):
+        assert np.array_equal(dims[f"Eigenvalue{k}"], eig[k])
+    # the golden reference outputs, through the same bars as the direct call
+    want = g["normal8_out"]
+    o = U.opts_from_bytes(g["normal8_opts"])
+    got = np.stack([dims[n] for n in ("NormalX", "NormalY", "NormalZ", "Curvature")])
+    lam, _ = f64_eigen(port_for_pipeline(), *U.doubles(g), 8)
+    U.compare_stage(o, got, want, g["normal8_status"], g["normal8_status"], lam=lam,
+                    label="pipeline normal8 vs reference", gap_min=1e-2, sign_eps=1e-6)
+
+
+def port_for_pipeline():
+    from oracle.oracle import Oracle
+    return Oracle("port")
