@@ -213,11 +213,11 @@ def served_leg(ctx, args):
     from gpupdal_b200.native import Server
     reqs = served.make_stream(args.served_requests, seed=1000)
     pts = sum(len(r["x"]) for r in reqs)
-    served.run_plain(ctx, reqs[:4])  # warm the plain context's caches
+    served.run_plain(ctx, reqs)  # warm-up pass: the plain context's block cache
     plain_s = sum(served.run_plain(ctx, reqs))
     srv = Server(0, slots=args.served_slots, hbm_budget=120 * 10**9)
     try:
-        served.run_served(srv, reqs[:8])  # warm-up: worker contexts' caches
+        served.run_served(srv, reqs)  # warm-up pass: every worker context's block cache
         cap_s, cap_lat, _ = served.run_served(srv, reqs)
         rate_s, lat, res = served.run_served(srv, reqs, rate=args.served_rate, seed=1)
     finally:
