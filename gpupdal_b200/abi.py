@@ -42,6 +42,7 @@ FEATURES = [
     "Density",
 ]
 FEAT_BIT = {name: 1 << i for i, name in enumerate(FEATURES)}
+globals().update({"FEAT_" + name.upper(): 1 << i for i, name in enumerate(FEATURES)})
 FEAT_DIMENSIONALITY = 0x0F
 FEAT_ALL = 0x7FF
 

@@ -520,14 +520,15 @@ int validate_stages(Context* ctx, const nbg_stage_opts* stages, int n_stages,
             return fail(ctx, NBG_ERR_INVALID, "knn must be in [0, 64]");
         if (o.kind != NBG_STAGE_NORMAL && o.stride != 1 && o.stride != 0)
             return fail(ctx, NBG_ERR_UNSUPPORTED, "stride > 1 is not supported");
-        if (o.kind == NBG_STAGE_COVARIANCEFEATURES && o.optimized)
-            return fail(ctx, NBG_ERR_UNSUPPORTED, "optimized is not supported");
+        if (o.kind != NBG_STAGE_COVARIANCEFEATURES && o.optimized)
+            return fail(ctx, NBG_ERR_INVALID, "optimized applies to covariancefeatures only");
         if (o.kind == NBG_STAGE_COVARIANCEFEATURES &&
             (o.mode < NBG_MODE_RAW || o.mode > NBG_MODE_NORMALIZED))
             return fail(ctx, NBG_ERR_INVALID, "invalid mode");
         if (outputs[s].ndims != ndims_of(o))
             return fail(ctx, NBG_ERR_INVALID, "output ndims does not match the stage");
-        if (o.kind == NBG_STAGE_COVARIANCEFEATURES && (o.feature_mask & NBG_FEAT_DENSITY))
+        if (o.kind == NBG_STAGE_COVARIANCEFEATURES &&
+            ((o.feature_mask & NBG_FEAT_DENSITY) || o.optimized))
             *need_aux = true;
     }
     return NBG_OK;
@@ -545,6 +546,51 @@ void fill_stage(StageDev& d, const nbg_stage_opts& o, const nbg_columns& c) {
     d.base = (char*)c.base;
     d.point_stride = c.point_stride;
     for (int k = 0; k < NBG_MAX_DIMS; ++k) d.offset[k] = c.offset[k];
+}
+
+__global__ void optimal_k_max_kernel(const double* k, uint64_t n, unsigned long long* out) {
+    double mx = 0.0;
+    int bad = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const double v = k[i];
+        if (!(v > -0.5) || !(v < 1.8446744073709552e19)) bad = 1;
+        else mx = fmax(mx, v);
+    }
+    // non-negative doubles order as their bit patterns
+    atomicMax(&out[0], (unsigned long long)__double_as_longlong(mx));
+    if (bad) atomicOr(&out[1], 1ull);
+}
+
+// Largest OptimalKNN of a column (host or device); `bad` when a value is
+// negative, NaN or beyond uint64 (the reference's numericCast would fail).
+int optimal_k_max(Context* ctx, const double* k, uint64_t n, bool on_device, cudaStream_t stream,
+                  double* mx, bool* bad) {
+    *mx = 0.0;
+    *bad = false;
+    if (!on_device) {
+        for (uint64_t i = 0; i < n; ++i) {
+            const double v = k[i];
+            if (!(v > -0.5) || !(v < 1.8446744073709552e19)) *bad = true;
+            else if (v > *mx) *mx = v;
+        }
+        return NBG_OK;
+    }
+    unsigned long long* d = nullptr;
+    int rc = ctx_alloc(ctx, (void**)&d, 16);
+    if (rc) return rc;
+    unsigned long long h[2] = {0, 0};
+    cudaMemsetAsync(d, 0, 16, stream);
+    optimal_k_max_kernel<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 1024)), 256, 0,
+                           stream>>>(k, n, d);
+    NBG_LAUNCHED(1);
+    cudaError_t e = cudaMemcpyAsync(h, d, 16, cudaMemcpyDeviceToHost, stream);
+    if (!e) e = cudaStreamSynchronize(stream);
+    ctx_free(ctx, d, 16);
+    if (e) return cuda_fail(ctx, e, "OptimalKNN scan");
+    *mx = __builtin_bit_cast(double, (long long)h[0]);
+    *bad = h[1] != 0;
+    return NBG_OK;
 }
 
 struct HostOut {
@@ -574,8 +620,16 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     bool need_aux = false;
     int vrc = validate_stages(ctx, stages, n_stages, outputs, &need_aux);
     if (vrc) return vrc;
-    if (need_aux && (!optimal_knn || !optimal_radius))
+    bool need_radius = false, any_optimized = false;
+    for (int s = 0; s < n_stages; ++s) {
+        if (stages[s].kind == NBG_STAGE_COVARIANCEFEATURES && (stages[s].feature_mask & NBG_FEAT_DENSITY))
+            need_radius = true;
+        if (stages[s].optimized) any_optimized = true;
+    }
+    if (need_radius && (!optimal_knn || !optimal_radius))
         return fail(ctx, NBG_ERR_INVALID, "Density needs OptimalKNN and OptimalRadius");
+    if (any_optimized && !optimal_knn)
+        return fail(ctx, NBG_ERR_INVALID, "optimized needs OptimalKNN");
     const uint64_t n = t->n;
     if (n == 0 || n_stages == 0) return NBG_OK;
     int rc = ensure_scratch(ctx, n, std::max<uint64_t>(exception_capacity, 1));
@@ -670,27 +724,52 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     }
     const double* kopt = optimal_knn;
     const double* ropt = optimal_radius;
+    // largest per-point k of the optimized stages (sizes their launch)
+    int opt_k = 0;
+    if (any_optimized) {
+        double mx = 0.0;
+        bool bad = false;
+        rc = optimal_k_max(ctx, optimal_knn, n, aux_on_device != 0, stream, &mx, &bad);
+        if (rc) { cleanup(); return rc; }
+        if (bad) {
+            cleanup();
+            return fail(ctx, NBG_ERR_INVALID, "OptimalKNN holds a value that is not a neighbour count");
+        }
+        opt_k = (int)std::min<double>((double)n, std::floor(mx + 0.5));
+        if (opt_k > 65) {
+            cleanup();
+            return fail(ctx, NBG_ERR_UNSUPPORTED, "OptimalKNN above 65 is not supported");
+        }
+    }
     if (need_aux && !aux_on_device) {
         rc = dev_alloc(ctx, (void**)&aux_dev[0], n * 8, nullptr);
-        if (!rc) rc = dev_alloc(ctx, (void**)&aux_dev[1], n * 8, nullptr);
+        if (!rc && optimal_radius) rc = dev_alloc(ctx, (void**)&aux_dev[1], n * 8, nullptr);
         if (rc) { cleanup(); return rc; }
         rc = host_to_device(ctx, aux_dev[0], optimal_knn, n * 8, stream);
-        if (!rc) rc = host_to_device(ctx, aux_dev[1], optimal_radius, n * 8, stream);
+        if (!rc && optimal_radius) rc = host_to_device(ctx, aux_dev[1], optimal_radius, n * 8, stream);
         if (rc) { cleanup(); return rc; }
         kopt = aux_dev[0];
-        ropt = aux_dev[1];
+        ropt = optimal_radius ? aux_dev[1] : nullptr;
     }
 
     // group stages by neighbour count
     std::vector<int> order(n_stages);
     for (int s = 0; s < n_stages; ++s) order[s] = s;
+    // neighbour count of a stage's launch: knn + 1 (capped at n), or the
+    // largest OptimalKNN for optimized stages (their rows then use their own)
+    auto stage_k = [&](int s) -> int {
+        if (stages[s].optimized) return std::max(1, opt_k);
+        return (int)std::min<uint64_t>(n, (uint64_t)stages[s].knn + 1);
+    };
     std::vector<std::vector<int>> groups;
     for (int s = 0; s < n_stages; ++s) {
-        const int K = (int)std::min<uint64_t>(n, (uint64_t)stages[s].knn + 1);
         bool placed = false;
         for (auto& gr : groups) {
-            const int K0 = (int)std::min<uint64_t>(n, (uint64_t)stages[gr[0]].knn + 1);
-            if (K0 == K) { gr.push_back(s); placed = true; break; }
+            if (stage_k(gr[0]) == stage_k(s) && !stages[gr[0]].optimized == !stages[s].optimized) {
+                gr.push_back(s);
+                placed = true;
+                break;
+            }
         }
         if (!placed) groups.push_back({s});
     }
@@ -702,7 +781,8 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     ExceptionSink sink{ctx->ex_rows, ctx->counters + 3, (uint32_t)std::max<uint32_t>(exception_capacity, 1)};
     if (cudaMemsetAsync(ctx->counters, 0, 64 * sizeof(uint32_t), stream)) { cleanup(); return NBG_ERR_CUDA; }
     for (auto& gr : groups) {
-        const int K = (int)std::min<uint64_t>(n, (uint64_t)stages[gr[0]].knn + 1);
+        const int K = stage_k(gr[0]);
+        const double* row_k = stages[gr[0]].optimized ? kopt : nullptr;
         cudaEventRecord(ctx->ev[1], stream);
         rc = ensure_grid(ctx, t, K, stream);
         if (rc) { cleanup(); return rc; }
@@ -735,6 +815,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         ql.ties = ctx->ties;
         ql.tie_cap = (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX);
         ql.sums = ctx->sums;
+        ql.row_k = row_k;
         // the KD replica does not depend on the query: build it on the side
         // stream while the query kernel runs (tie rows almost always need it)
         const bool speculative = !(t->kd && kd_built(t)) && n > 100;
@@ -786,6 +867,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
                 tl.exact_rows = ctx->exact_rows;
                 tl.counters = ctx->counters;
                 tl.ids_out = nullptr;
+                tl.row_k = row_k;
                 rc = launch_ties(ctx, tl, stream);
                 if (!rc) {
                     e = cudaMemcpyAsync(cnt, ctx->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -795,7 +877,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
                 }
             }
             replay_rows += cnt[0];
-            if (!rc) rc = kd_run_rows(ctx, t, K, g, sink, ctx->exact_rows, cnt[0], stream);
+            if (!rc) rc = kd_run_rows(ctx, t, K, g, sink, ctx->exact_rows, cnt[0], stream, row_k);
             if (rc) { cleanup(); return rc; }
             cudaEventRecord(ctx->ev[5], stream);
             e = cudaStreamSynchronize(stream);

@@ -110,7 +110,19 @@ struct QueryArgs {
     uint2* ties;         // tie list {id, (D_K - 2^23 bias) | R << 24}; null: ties go to exact_rows
     uint32_t tie_cap;
     RowSums* sums;       // split form: per sorted position, read by knn_finish_kernel
+    const double* row_k; // covariancefeatures optimized: per-point k = OptimalKNN (null: K)
 };
+
+// Neighbour count of a row: K, or the point's OptimalKNN rounded half away
+// from zero (Utils::numericCast, pdal/util/Utils.hpp:747-764) capped at the
+// tile's size, as KD3Index::neighbors(p, k, 1) in
+// CovarianceFeaturesFilter.cpp:212-214.
+__device__ __forceinline__ int row_neighbours(const double* row_k, int K, uint64_t n, uint32_t id) {
+    if (!row_k) return K;
+    const double v = row_k[id];
+    const double k = v > 0.0 ? floor(v + 0.5) : ceil(v - 0.5);
+    return (int)(k < (double)n ? k : (double)n);
+}
 
 // One tile of a batch: its query arguments and the first work item (block of
 // queries) it owns in the batch's queue.

@@ -128,6 +128,7 @@ struct QueryLaunch {
     uint2* ties = nullptr;  // tie list (null: tie rows join exact_rows)
     uint32_t tie_cap = 0;
     RowSums* sums = nullptr;  // split select/finish kernels (null: one fused kernel)
+    const double* row_k = nullptr;  // per-row neighbour count (optimized), device
 };
 int launch_query(Context* ctx, const QueryLaunch& q, cudaStream_t stream);
 // Select pass over a sample of `blocks` blocks of 128 rows, `stride` rows apart.
@@ -146,6 +147,7 @@ struct TieLaunch {
     uint32_t* exact_rows;  // rows the resolver hands to the search replay
     uint32_t* counters;
     uint32_t* ids_out;     // neighbour-set export (null in the fused path)
+    const double* row_k = nullptr;
 };
 int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream);
 
@@ -154,7 +156,8 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t stream);
 // One forest holding the replicas of every listed tile that has none.
 int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t stream);
 int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const ExceptionSink& ex,
-                const uint32_t* rows, uint32_t nrows, cudaStream_t stream);
+                const uint32_t* rows, uint32_t nrows, cudaStream_t stream,
+                const double* row_k = nullptr);
 int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
                      uint32_t* ids_out, cudaStream_t stream);
 KdOrder kd_order(const Tile* t);

@@ -874,15 +874,20 @@ __global__ void kd_search_kernel(KdDev kd, Transform tf, const int32_t* __restri
                                  const int32_t* __restrict__ y, const int32_t* __restrict__ z,
                                  const uint32_t* __restrict__ rows, uint32_t nrows, int K,
                                  uint32_t* __restrict__ nbr, uint32_t* __restrict__ counts,
-                                 uint32_t* errors) {
+                                 uint32_t* errors, const double* row_k, uint64_t npts) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrows) return;
     const uint32_t id = rows[r];
+    const int Kr = row_neighbours(row_k, K, npts, id);  // <= K
     const double q[3] = {ref_coord(x[id], tf.scale[0], tf.offset[0]),
                          ref_coord(y[id], tf.scale[1], tf.offset[1]),
                          ref_coord(z[id], tf.scale[2], tf.offset[2])};
+    if (Kr <= 0) {
+        counts[r] = 0;
+        return;
+    }
     KdResult rs;
-    rs.init(K);
+    rs.init(Kr);
     const bool ok = kd_search(kd, tf, q, rs);
     for (int s = 0; s < K; ++s) nbr[(uint64_t)r * K + s] = s < rs.count ? rs.idx[s] : 0u;
     counts[r] = ok ? (uint32_t)rs.count : 0u;
@@ -1386,7 +1391,8 @@ static KdDev kd_view(const Tile* t) {
 
 // Searches the listed rows into per-call scratch (nbr, counts).
 static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
-                          uint32_t** nbr, uint32_t** counts, cudaStream_t st) {
+                          uint32_t** nbr, uint32_t** counts, cudaStream_t st,
+                          const double* row_k = nullptr) {
     if (K > KD_CAP) return NBG_ERR_INVALID;
     KdForest* kd = t->kd->f;
     *nbr = nullptr;
@@ -1402,7 +1408,7 @@ static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, ui
     cudaMemsetAsync(kd->counters + 2, 0, 4, st);
     kd_search_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(kd_view(t), t->tf, t->x, t->y, t->z,
                                                           rows, nrows, K, *nbr, *counts,
-                                                          kd->counters + 2);
+                                                          kd->counters + 2, row_k, t->n);
     NBG_LAUNCHED(1);
     cudaError_t le = cudaGetLastError();
     uint32_t err = 0;
@@ -1420,10 +1426,10 @@ static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, ui
 }
 
 int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const ExceptionSink& ex,
-                const uint32_t* rows, uint32_t nrows, cudaStream_t st) {
+                const uint32_t* rows, uint32_t nrows, cudaStream_t st, const double* row_k) {
     if (!nrows) return NBG_OK;
     uint32_t *nbr = nullptr, *counts = nullptr;
-    int rc = kd_search_rows(ctx, t, K, rows, nrows, &nbr, &counts, st);
+    int rc = kd_search_rows(ctx, t, K, rows, nrows, &nbr, &counts, st, row_k);
     if (!rc) {
         kd_finish_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(t->tf, t->x, t->y, t->z, rows, nrows,
                                                               K, nbr, counts, grp, ex);

@@ -231,10 +231,9 @@ __device__ __forceinline__ void defer_row(const QueryArgs& a, uint32_t id, bool 
 // the grid path; `R` is the final ring and `kk` the K-th key.
 template <int KS>
 __device__ __forceinline__ bool select_kth(const QueryArgs& a, const GridParams& g,
-                                           const QueryCell& qc, const float4 q, int& R,
+                                           const QueryCell& qc, const float4 q, int K, int& R,
                                            uint32_t& kk, bool& tie) {
     tie = false;
-    const int K = a.K;
     const int off = KS - (K + 1);
     TopK<KS> top;
     top.init(off);
@@ -276,6 +275,7 @@ __global__ void __launch_bounds__(128) knn_fused_kernel(const QueryArgs a) {
     const GridParams g = *a.gp;
     const float4 q = __ldg(&a.gv.sorted[i]);
     const uint32_t id = __float_as_uint(q.w);
+    const int K = a.K;
     QueryCell qc;
     qc.qx = __float2int_rz(q.x);
     qc.qy = __float2int_rz(q.y);
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(128) knn_fused_kernel(const QueryArgs a) {
     int R;
     uint32_t kk;
     bool tie;
-    if (!select_kth<KS>(a, g, qc, q, R, kk, tie)) {
+    if (!select_kth<KS>(a, g, qc, q, K, R, kk, tie)) {
         defer_row(a, id, tie, kk, R);
         return;
     }
@@ -316,6 +316,18 @@ __device__ __forceinline__ void select_row(const QueryArgs& a, const uint64_t i)
     const GridParams g = *a.gp;
     const float4 q = __ldg(&a.gv.sorted[i]);
     const uint32_t id = __float_as_uint(q.w);
+    const int K = row_neighbours(a.row_k, a.K, a.n, id);
+    if (K <= 0) {
+        // no neighbours: the reference's covariance of an empty set is zero
+        const long long M[6] = {0, 0, 0, 0, 0, 0};
+        const int32_t qraw[3] = {__float2int_rz(q.x) + g.minx, __float2int_rz(q.y) + g.miny,
+                                 __float2int_rz(q.z) + g.minz};
+        nbg_finish_row(a.grp, a.tf, a.ex, id, 0, M, qraw);
+        RowSums z;
+        z.cnt = 0;
+        a.sums[i] = z;
+        return;
+    }
     QueryCell qc;
     qc.qx = __float2int_rz(q.x);
     qc.qy = __float2int_rz(q.y);
@@ -328,14 +340,14 @@ __device__ __forceinline__ void select_row(const QueryArgs& a, const uint64_t i)
     bool tie;
     RowSums out;
     out.cnt = 0;
-    if (!select_kth<KS>(a, g, qc, q, R, kk, tie)) {
+    if (!select_kth<KS>(a, g, qc, q, K, R, kk, tie)) {
         defer_row(a, id, tie, kk, R);
         a.sums[i] = out;
         return;
     }
     Pass2Fn f2{q.x, q.y, q.z, kk, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int r = 0; r <= R; ++r) scan_shell(a.gv, g, qc, r, f2);
-    if (f2.cnt != a.K) {
+    if (f2.cnt != K) {
         defer_row(a, id, false, kk, R);
         a.sums[i] = out;
         return;
@@ -479,6 +491,7 @@ __global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
     const GridParams g = *a.gp;
     const float4 q = __ldg(&a.gv.sorted[i]);
     const uint32_t id = __float_as_uint(q.w);
+    const int K = a.K;
     QueryCell qc;
     qc.qx = __float2int_rz(q.x);
     qc.qy = __float2int_rz(q.y);
@@ -489,7 +502,7 @@ __global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
     int R;
     uint32_t kk;
     bool tie;
-    if (!select_kth<KS>(a, g, qc, q, R, kk, tie)) {
+    if (!select_kth<KS>(a, g, qc, q, K, R, kk, tie)) {
         defer_row(a, id, tie, kk, R);
         return;
     }
@@ -590,6 +603,8 @@ struct TieFn {
 struct TieArgs {
     GridView gv;
     const GridParams* gp;
+    uint64_t n;
+    const double* row_k;
     const int32_t* x;  // raw coordinates in caller order
     const int32_t* y;
     const int32_t* z;
@@ -613,6 +628,7 @@ __global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
     const uint32_t kk = KEY_BASE + (e.y & 0xFFFFFFu);
     const int R = (int)(e.y >> 24);
     const GridParams g = *a.gp;
+    const int K = row_neighbours(a.row_k, a.K, a.n, id);
     const int32_t qraw[3] = {__ldg(&a.x[id]), __ldg(&a.y[id]), __ldg(&a.z[id])};
     QueryCell qc;
     qc.qx = qraw[0] - g.minx;
@@ -630,9 +646,9 @@ __global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
     f.less = 0;
     f.gcnt = 0;
     f.row = a.ids_out ? a.ids_out + (uint64_t)id * a.K : nullptr;
-    f.K = a.K;
+    f.K = K;
     for (int ring = 0; ring <= R; ++ring) scan_shell(a.gv, g, qc, ring, f);
-    const int m = a.K - f.less;
+    const int m = K - f.less;
     if (f.gcnt > TIE_CAP || m <= 0 || m > f.gcnt) {
         const uint32_t slot = atomicAdd(&a.counters[0], 1u);
         a.exact_rows[slot] = id;
@@ -670,7 +686,7 @@ __global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
     }
     if (f.row) {
         uint32_t* row = f.row;
-        for (int s = 1; s < a.K; ++s) {
+        for (int s = 1; s < K; ++s) {
             const uint32_t v = row[s];
             int t = s - 1;
             while (t >= 0 && row[t] > v) {
@@ -681,7 +697,7 @@ __global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
         }
         return;
     }
-    const long long n = a.K;
+    const long long n = K;
     long long M[6];
     M[0] = n * f.sxx - (long long)f.s1x * f.s1x;
     M[1] = n * f.syx - (long long)f.s1y * f.s1x;
@@ -698,6 +714,8 @@ int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream) {
     TieArgs a;
     a.gv = grid_view(tl.tile);
     a.gp = tl.tile->gp;
+    a.n = tl.tile->n;
+    a.row_k = tl.row_k;
     a.x = tl.tile->x;
     a.y = tl.tile->y;
     a.z = tl.tile->z;
@@ -797,6 +815,7 @@ int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
     la.q.ties = ql.ties;
     la.q.tie_cap = ql.tie_cap;
     la.q.sums = ql.sums;
+    la.q.row_k = ql.row_k;
     la.stream = stream;
     la.ids = false;
     return dispatch_slots<KnnLauncher>(ql.K, la);
@@ -819,6 +838,7 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
     la.q.ties = ties;
     la.q.tie_cap = tie_cap;
     la.q.sums = nullptr;
+    la.q.row_k = nullptr;
     la.stream = stream;
     la.ids = true;
     return dispatch_slots<KnnLauncher>(K, la);
@@ -861,6 +881,7 @@ int launch_select_sample(Context* ctx, const QueryLaunch& ql, uint64_t stride, u
     s.q.ties = ql.ties;
     s.q.tie_cap = ql.tie_cap;
     s.q.sums = ql.sums;
+    s.q.row_k = ql.row_k;
     s.stride = stride;
     s.blocks = blocks;
     s.stream = stream;

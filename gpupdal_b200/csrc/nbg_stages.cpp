@@ -521,7 +521,7 @@ extern "C" int nbg_filter_options(const nbg_filter* f, nbg_stage_opts* out) {
     if (!f || !out) return NBG_ERR_INVALID;
     *out = f->opts;
     if (f->radius_set) return NBG_ERR_UNSUPPORTED;  // radius / min_k: not on this path yet
-    if (f->opts.stride > 1 || f->opts.optimized) return NBG_ERR_UNSUPPORTED;
+    if (f->opts.stride > 1) return NBG_ERR_UNSUPPORTED;
     return NBG_OK;
 }
 

@@ -220,7 +220,7 @@ typedef struct nbg_filter nbg_filter;
 int nbg_filter_create(const char* type, const char* options_json, int32_t has_optimal_knn,
                       int32_t has_optimal_radius, nbg_filter** filter, char* err, size_t err_len);
 /* The stage's nbg_stage_opts (knn as the user gave it).  NBG_ERR_UNSUPPORTED
- * (with *out still filled) for radius/min_k, stride > 1 and optimized. */
+ * (with *out still filled) for radius/min_k and stride > 1. */
 int nbg_filter_options(const nbg_filter* filter, nbg_stage_opts* out);
 /* Registered output dimensions, comma separated, in the library's order. */
 int nbg_filter_dims(const nbg_filter* filter, char* names, size_t len);

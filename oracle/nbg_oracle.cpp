@@ -280,7 +280,10 @@ public:
         Result rs;
         rs.cap = k2;
         rs.init(out.data(), dist.data());
-        if (n != 0) {
+        // k = 0: the reference's result set then reads outside its (empty)
+        // buffer (KDImpl.hpp:357-371 with nanoflann's worstDist); the only
+        // observable outcome is the empty neighbourhood, returned here
+        if (n != 0 && k2 != 0) {
             double dists[3] = {0, 0, 0};
             double distsq = 0.0;
             for (int i = 0; i < 3; ++i) {

@@ -77,6 +77,7 @@ struct RefTree {
         k = (std::min<uint64_t>)(cloud.pts.size(), k);
         uint64_t k2 = stride * k;
         PointIdList output(k2);
+        if (k2 == 0) return output;  // nanoflann's worstDist would read before its buffer
         std::vector<double> out_dist_sqr(k2);
         std::vector<double> pt{x, y, z};
         nanoflann::KNNResultSet<double, PointId, uint64_t> resultSet(k2);

@@ -205,3 +205,27 @@ def test_pipeline_json_runs_the_path_stages(nbg):
 def port_for_pipeline():
     from oracle.oracle import Oracle
     return Oracle("port")
+
+
+def test_covariancefeatures_optimized_per_point_k(nbg, port):
+    """optimized=true: each point's k is its OptimalKNN (rounded, capped at n,
+    without the +1 of knn; CovarianceFeaturesFilter.cpp:212-214); k = 0 rows
+    have an empty neighbourhood and are skipped as zero covariance."""
+    x, y, z = syn.mixture(4_000_000, 1)
+    m = (x < 9000) & (y < 9000)
+    x, y, z = x[m], y[m], z[m]
+    n = len(x)
+    rng = np.random.default_rng(5)
+    kopt = rng.integers(3, 41, n).astype(np.float64)
+    kopt[rng.random(n) < 0.01] = 0.0
+    ropt = rng.uniform(0.3, 1.5, n)
+    mask = (abi.FEAT_LINEARITY | abi.FEAT_PLANARITY | abi.FEAT_SCATTERING | abi.FEAT_ANISOTROPY |
+            abi.FEAT_SURFACEVARIATION | abi.FEAT_DENSITY)
+    o = abi.make_opts(abi.STAGE_COVARIANCEFEATURES, knn=10, feature_mask=mask, optimized=True)
+    tile = nbg.tile(x, y, z)
+    outs, ex, stats = nbg.run(tile, [o], optimal_knn=kopt, optimal_radius=ropt)
+    X, Y, Z = (syn.to_double(v) for v in (x, y, z))
+    want, st = port.tree(X, Y, Z).run_stage(o, mode=1, optimal_knn=kopt, optimal_radius=ropt)
+    got_status = U.status_from_exceptions(n, ex)
+    assert np.count_nonzero(st) == np.count_nonzero(kopt == 0)
+    U.compare_stage(o, outs[0], want, st, got_status, label="optimized vs f64")

@@ -85,7 +85,8 @@ def test_covariancefeatures_prepared_checks():
     with pytest.raises(StageError, match="Missing OptimalKNN dimension in input PointView."):
         Filter("filters.covariancefeatures", {"optimized": True})
     f = Filter("filters.covariancefeatures", {"optimized": True}, True, False)
-    assert f.options()[1] == abi.NBG_ERR_UNSUPPORTED
+    o, rc = f.options()
+    assert rc == abi.NBG_OK and o.optimized == 1
 
 
 def test_row_reports():
