@@ -54,6 +54,7 @@ ROW_TOO_FEW = 1
 ROW_ZERO_COV = 2
 ROW_EIGEN_FAIL = 3
 ROW_ZERO_LAMBDA = 4
+ROW_RADIUS_FEW = 5
 
 MAX_DIMS = 16
 NOALLOC_MAX_POINTS = 524288
@@ -75,6 +76,9 @@ class StageOpts(ctypes.Structure):
         ("mode", ctypes.c_int32),
         ("stride", ctypes.c_int32),
         ("optimized", ctypes.c_int32),
+        ("use_radius", ctypes.c_int32),
+        ("min_k", ctypes.c_int32),
+        ("radius", ctypes.c_double),
     ]
 
 
@@ -176,7 +180,7 @@ def stage_dims(opts: StageOpts) -> list:
 
 def make_opts(kind, knn=8, always_up=True, viewpoint=None, refine=False,
               normalize=False, feature_mask=FEAT_DIMENSIONALITY, mode=MODE_SQRT,
-              stride=1, optimized=False) -> StageOpts:
+              stride=1, optimized=False, radius=None, min_k=3) -> StageOpts:
     o = StageOpts()
     o.kind = int(kind)
     o.knn = int(knn)
@@ -191,6 +195,9 @@ def make_opts(kind, knn=8, always_up=True, viewpoint=None, refine=False,
     o.mode = int(mode)
     o.stride = int(stride)
     o.optimized = int(bool(optimized))
+    o.use_radius = int(radius is not None)
+    o.radius = float(radius) if radius is not None else 0.0
+    o.min_k = int(min_k)
     return o
 
 

@@ -494,9 +494,18 @@ int nbg_tile_free(nbg_context* h, nbg_tile* th) {
 namespace nbg {
 
 // Grid for neighbour count k1 (rebuilt when k1 moves far from the build's).
-static int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
-    if (t->grid_valid && k1 <= 2 * t->grid_k1 && 2 * k1 >= t->grid_k1) return NBG_OK;
+// Grid for neighbour count k1, or with a fixed cell edge `cell` raw units
+// (radius stages); rebuilt when k1 moves far from the build's or the edge rule
+// changes.
+static int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream, int32_t cell = 0) {
+    const int32_t fixed = cell ? cell : t->fixed_cell;
+    if (t->grid_valid && t->grid_fixed == fixed &&
+        (fixed || (k1 <= 2 * t->grid_k1 && 2 * k1 >= t->grid_k1)))
+        return NBG_OK;
+    const int32_t saved = t->fixed_cell;
+    t->fixed_cell = fixed;
     int rc = build_grid(ctx, t, k1, stream);
+    t->fixed_cell = saved;
     if (rc) return fail(ctx, rc, "grid build failed");
     NBG_TRY(cudaMemcpyAsync(&t->host_gp, t->gp, sizeof(GridParams), cudaMemcpyDeviceToHost, stream),
             "grid params");
@@ -507,6 +516,7 @@ static int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
         return fail(ctx, NBG_ERR_UNSUPPORTED, "tile extent must be below 2^24 raw units per axis");
     t->grid_valid = true;
     t->grid_k1 = k1;
+    t->grid_fixed = fixed;
     return NBG_OK;
 }
 
@@ -518,8 +528,13 @@ int validate_stages(Context* ctx, const nbg_stage_opts* stages, int n_stages,
         if (o.kind < 1 || o.kind > 3) return fail(ctx, NBG_ERR_INVALID, "unknown stage kind");
         if (o.knn < 0 || o.knn > 64)
             return fail(ctx, NBG_ERR_INVALID, "knn must be in [0, 64]");
-        if (o.kind != NBG_STAGE_NORMAL && o.stride != 1 && o.stride != 0)
+        // a radius makes the reference ignore knn and stride
+        // (EigenvaluesFilter.cpp:96-100, CovarianceFeaturesFilter.cpp:216-225)
+        const bool by_radius = o.use_radius && !(o.kind == NBG_STAGE_COVARIANCEFEATURES && o.optimized);
+        if (!by_radius && o.kind != NBG_STAGE_NORMAL && o.stride != 1 && o.stride != 0)
             return fail(ctx, NBG_ERR_UNSUPPORTED, "stride > 1 is not supported");
+        if (by_radius && !(o.radius == o.radius))
+            return fail(ctx, NBG_ERR_INVALID, "radius is not a number");
         if (o.kind != NBG_STAGE_COVARIANCEFEATURES && o.optimized)
             return fail(ctx, NBG_ERR_INVALID, "optimized applies to covariancefeatures only");
         if (o.kind == NBG_STAGE_COVARIANCEFEATURES &&
@@ -761,10 +776,15 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         if (stages[s].optimized) return std::max(1, opt_k);
         return (int)std::min<uint64_t>(n, (uint64_t)stages[s].knn + 1);
     };
+    auto by_radius = [&](int s) {
+        return stages[s].use_radius &&
+               !(stages[s].kind == NBG_STAGE_COVARIANCEFEATURES && stages[s].optimized);
+    };
     std::vector<std::vector<int>> groups;
     for (int s = 0; s < n_stages; ++s) {
         bool placed = false;
         for (auto& gr : groups) {
+            if (by_radius(gr[0]) || by_radius(s)) continue;  // radius stages run alone
             if (stage_k(gr[0]) == stage_k(s) && !stages[gr[0]].optimized == !stages[s].optimized) {
                 gr.push_back(s);
                 placed = true;
@@ -783,8 +803,15 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     for (auto& gr : groups) {
         const int K = stage_k(gr[0]);
         const double* row_k = stages[gr[0]].optimized ? kopt : nullptr;
+        const bool radius_group = by_radius(gr[0]);
+        int32_t radius_cell = 0;
+        if (radius_group) {
+            // cells one radius wide (plus a margin): the ball fits in one ring
+            const double r_raw = std::fabs(stages[gr[0]].radius) / t->tf.scale[0];
+            radius_cell = (int32_t)std::min(1.0e9, std::ceil(r_raw * 1.001) + 1.0);
+        }
         cudaEventRecord(ctx->ev[1], stream);
-        rc = ensure_grid(ctx, t, K, stream);
+        rc = ensure_grid(ctx, t, K, stream, radius_cell);
         if (rc) { cleanup(); return rc; }
         cudaEventRecord(ctx->ev[2], stream);
         StageGroup g{};
@@ -803,6 +830,25 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             cudaMemsetAsync(ctx->counters + 4, 0, sizeof(uint32_t), stream)) {
             cleanup();
             return NBG_ERR_CUDA;
+        }
+        if (radius_group) {
+            RadiusLaunch rl;
+            rl.tile = t;
+            rl.grp = g;
+            rl.ex = sink;
+            rl.radius = stages[gr[0]].radius;
+            rl.min_k = stages[gr[0]].min_k;
+            rc = launch_radius(ctx, rl, stream);
+            if (rc) { cleanup(); return fail(ctx, rc, "radius launch failed"); }
+            cudaEventRecord(ctx->ev[3], stream);
+            cudaError_t e = cudaStreamSynchronize(stream);
+            if (e) { cleanup(); return cuda_fail(ctx, e, "radius kernel"); }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+            grid_ms += ms;
+            cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+            query_ms += ms;
+            continue;
         }
         QueryLaunch ql;
         ql.tile = t;

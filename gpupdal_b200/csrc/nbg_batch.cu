@@ -135,6 +135,9 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
                 return fail(ctx, NBG_ERR_UNSUPPORTED, "the stages of a batch item share one knn");
             if (it.outputs[s].on_device != 1)
                 return fail(ctx, NBG_ERR_UNSUPPORTED, "batch outputs are device-resident");
+            if (it.stages[s].use_radius || it.stages[s].optimized)
+                return fail(ctx, NBG_ERR_UNSUPPORTED,
+                            "radius and optimized stages run through nbg_run, not the batch");
         }
         const Tile* t = &it.tile->t;
         if (t->n == 0) continue;
@@ -198,7 +201,9 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
     cudaStreamWaitEvent(st, B->ev[0], 0);
     for (int i : live) {
         Tile* t = &items[i].tile->t;
-        if (t->grid_valid && Ks[i] <= 2 * t->grid_k1 && 2 * Ks[i] >= t->grid_k1) continue;
+        if (t->grid_valid && t->grid_fixed == t->fixed_cell &&
+            (t->fixed_cell || (Ks[i] <= 2 * t->grid_k1 && 2 * Ks[i] >= t->grid_k1)))
+            continue;
         t->grid_valid = false;
         rc = build_grid_async(ctx, t, Ks[i], st);
         if (rc) return fail(ctx, rc, "grid build failed");
@@ -226,6 +231,7 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
         }
         t->grid_valid = true;
         t->grid_k1 = Ks[live[j]];
+        t->grid_fixed = t->fixed_cell;
     }
     // ---- jobs: select order grouped by class, then finish order
     std::vector<int> order(live);

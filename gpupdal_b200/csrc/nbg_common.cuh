@@ -433,14 +433,14 @@ __device__ inline bool nbg_eigen_fast(const double low[6], double eval[3], doubl
 // int64), so cov = M * s_i*s_j / (n*(n-1)).  Writes every stage's outputs,
 // or appends the reference's skip/throw code to the exception sink.
 __device__ inline void nbg_append_exception(const ExceptionSink& ex, uint32_t id, int stage,
-                                            int code) {
+                                            int code, uint16_t reserved = 0) {
     uint32_t slot = atomicAdd(ex.count, 1u);
     if (slot < ex.capacity) {
         nbg_row_exception r;
         r.point_id = id;
         r.stage = (uint8_t)stage;
         r.code = (uint8_t)code;
-        r.reserved = 0;
+        r.reserved = reserved;
         ex.rows[slot] = r;
     }
 }
@@ -449,19 +449,21 @@ __device__ __forceinline__ void nbg_store(const StageDev& st, uint32_t id, int d
     *reinterpret_cast<double*>(st.base + (int64_t)id * st.point_stride + st.offset[d]) = v;
 }
 
-__device__ inline void nbg_finish_row(const StageGroup& g, const Transform& tf,
-                                      const ExceptionSink& ex, uint32_t id, int nnb,
-                                      const long long M[6], const int32_t qraw[3]) {
+// Md = n*S2 - S1*S1^T of the neighbours' raw offsets (exact integers, as
+// doubles), lower triangle m00, m10, m11, m20, m21, m22.
+__device__ inline void nbg_finish_row_d(const StageGroup& g, const Transform& tf,
+                                        const ExceptionSink& ex, uint32_t id, int nnb,
+                                        const double Md[6], const int32_t qraw[3]) {
     // covariance as the reference forms it, up to its float narrowing
     const double s0 = tf.scale[0], s1 = tf.scale[1], s2 = tf.scale[2];
     double denom = (double)nnb * (double)(nnb - 1);
     double C[6];  // c00, c10, c11, c20, c21, c22
-    C[0] = (double)M[0] * (s0 * s0) / denom;
-    C[1] = (double)M[1] * (s1 * s0) / denom;
-    C[2] = (double)M[2] * (s1 * s1) / denom;
-    C[3] = (double)M[3] * (s2 * s0) / denom;
-    C[4] = (double)M[4] * (s2 * s1) / denom;
-    C[5] = (double)M[5] * (s2 * s2) / denom;
+    C[0] = Md[0] * (s0 * s0) / denom;
+    C[1] = Md[1] * (s1 * s0) / denom;
+    C[2] = Md[2] * (s1 * s1) / denom;
+    C[3] = Md[3] * (s2 * s0) / denom;
+    C[4] = Md[4] * (s2 * s1) / denom;
+    C[5] = Md[5] * (s2 * s2) / denom;
     bool zero = true;
     int nonfinite = nnb <= 1;
 #pragma unroll
@@ -576,4 +578,12 @@ __device__ inline void nbg_finish_row(const StageGroup& g, const Transform& tf,
             }
         }
     }
+}
+
+__device__ inline void nbg_finish_row(const StageGroup& g, const Transform& tf,
+                                      const ExceptionSink& ex, uint32_t id, int nnb,
+                                      const long long M[6], const int32_t qraw[3]) {
+    const double Md[6] = {(double)M[0], (double)M[1], (double)M[2],
+                          (double)M[3], (double)M[4], (double)M[5]};
+    nbg_finish_row_d(g, tf, ex, id, nnb, Md, qraw);
 }

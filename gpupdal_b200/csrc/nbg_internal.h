@@ -99,6 +99,7 @@ struct Tile {
     float cell_factor = 4.0f;
     int32_t fixed_cell = 0;
     int grid_k1 = 0;
+    int32_t grid_fixed = 0;      // fixed cell edge the current grid was built with (0: density)
     bool grid_valid = false;
     GridParams host_gp{};
     // exact replica of the reference's KD tree (built on first need)
@@ -150,6 +151,17 @@ struct TieLaunch {
     const double* row_k = nullptr;
 };
 int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream);
+
+// Radius neighbourhoods of one stage (no tie order: every point within the
+// radius belongs to the set).
+struct RadiusLaunch {
+    const Tile* tile;
+    StageGroup grp;   // one stage
+    ExceptionSink ex;
+    double radius;
+    int32_t min_k;    // rows below it are skipped (not for normal)
+};
+int launch_radius(Context* ctx, const RadiusLaunch& rl, cudaStream_t stream);
 
 // Exact path: nanoflann replica build (lazy) + DFS for the listed rows.
 int kd_ensure(Context* ctx, Tile* t, cudaStream_t stream);

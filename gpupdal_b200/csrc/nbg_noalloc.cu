@@ -94,6 +94,9 @@ extern "C" int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32
         return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "stride > 1 is not supported");
     if (opts->kind == NBG_STAGE_COVARIANCEFEATURES && opts->optimized)
         return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "optimized is not supported");
+    if (opts->use_radius)
+        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED,
+                       "radius neighbourhoods are not supported by this entry point");
     const int ndims = opts->kind == NBG_STAGE_NORMAL ? 4
                       : opts->kind == NBG_STAGE_EIGENVALUES
                           ? 3

@@ -734,6 +734,133 @@ int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream) {
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
 }
 
+// ---------------------------------------------------------------------------
+// Radius neighbourhoods (NormalFilter.cpp:149-150, EigenvaluesFilter.cpp:
+// 121-134, CovarianceFeaturesFilter.cpp:216-225 through KD3Index::radius,
+// KDImpl.hpp:398-415): the points whose squared FP64 distance, formed as the
+// reference forms it, is below fl(r*r).  nanoflann's RadiusResultSet keeps
+// every such point, so there is no tie order.  A candidate whose exact integer
+// distance is clearly beyond the radius (relative 1e-5, far above the FP64
+// rounding of the coordinates) is dropped; every other candidate is tested
+// with the reference's FP64 distance.  Sums are int64 (exact while the
+// neighbourhood's sum of squared offsets stays below 2^63 raw units^2).
+struct RadiusFn {
+    float qx, qy, qz;
+    int32_t qraw[3];
+    double q64[3];
+    double rr;
+    unsigned long long dout;
+    Transform tf;
+    long long s1x, s1y, s1z, sxx, syx, syy, szx, szy, szz;
+    uint32_t cnt;
+    __device__ __forceinline__ unsigned long long limit() const { return dout; }
+    __device__ __forceinline__ void operator()(const float4 p) {
+        const int ix = (int)(p.x - qx), iy = (int)(p.y - qy), iz = (int)(p.z - qz);
+        const unsigned long long D = (unsigned long long)((long long)ix * ix + (long long)iy * iy +
+                                                          (long long)iz * iz);
+        if (D > dout) return;
+        const int off[3] = {ix, iy, iz};
+        double acc = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double pc = ref_coord(qraw[d] + off[d], tf.scale[d], tf.offset[d]);
+            const double df = __dsub_rn(q64[d], pc);
+            acc = __dadd_rn(acc, __dmul_rn(df, df));
+        }
+        if (!(acc < rr)) return;
+        s1x += ix;
+        s1y += iy;
+        s1z += iz;
+        sxx += (long long)ix * ix;
+        syx += (long long)iy * ix;
+        syy += (long long)iy * iy;
+        szx += (long long)iz * ix;
+        szy += (long long)iz * iy;
+        szz += (long long)iz * iz;
+        ++cnt;
+    }
+};
+
+struct RadiusArgs {
+    GridView gv;
+    const GridParams* gp;
+    uint64_t n;
+    StageGroup grp;
+    Transform tf;
+    ExceptionSink ex;
+    double rr;                 // fl(r * r)
+    unsigned long long dout;   // integer squared distances above it are outside
+    double r_raw;              // radius in raw units (for the ring count)
+    int32_t min_k;
+};
+
+__device__ __forceinline__ double m_entry(long long n, long long sab, long long sa, long long sb) {
+    return (double)((__int128)n * sab - (__int128)sa * sb);
+}
+
+__global__ void __launch_bounds__(128) knn_radius_kernel(const RadiusArgs a) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const GridParams g = *a.gp;
+    const float4 q = __ldg(&a.gv.sorted[i]);
+    const uint32_t id = __float_as_uint(q.w);
+    QueryCell qc;
+    qc.qx = __float2int_rz(q.x);
+    qc.qy = __float2int_rz(q.y);
+    qc.qz = __float2int_rz(q.z);
+    qc.cx = qc.qx / g.cell;
+    qc.cy = qc.qy / g.cell;
+    qc.cz = qc.qz / g.cell;
+    RadiusFn f;
+    f.qx = q.x;
+    f.qy = q.y;
+    f.qz = q.z;
+    f.qraw[0] = qc.qx + g.minx;
+    f.qraw[1] = qc.qy + g.miny;
+    f.qraw[2] = qc.qz + g.minz;
+    for (int d = 0; d < 3; ++d) f.q64[d] = ref_coord(f.qraw[d], a.tf.scale[d], a.tf.offset[d]);
+    f.rr = a.rr;
+    f.dout = a.dout;
+    f.tf = a.tf;
+    f.s1x = f.s1y = f.s1z = f.sxx = f.syx = f.syy = f.szx = f.szy = f.szz = 0;
+    f.cnt = 0;
+    const int R = (int)ceil(a.r_raw / (double)g.cell);
+    for (int r = 0; r <= R; ++r) scan_shell(a.gv, g, qc, r, f);
+    const StageDev& st = a.grp.st[0];
+    if (st.kind != NBG_STAGE_NORMAL && (long long)f.cnt < (long long)a.min_k) {
+        nbg_append_exception(a.ex, id, a.grp.stage_index[0], NBG_ROW_RADIUS_FEW,
+                             (uint16_t)min(f.cnt, 65535u));
+        return;
+    }
+    const long long n = f.cnt;
+    const double Md[6] = {m_entry(n, f.sxx, f.s1x, f.s1x), m_entry(n, f.syx, f.s1y, f.s1x),
+                          m_entry(n, f.syy, f.s1y, f.s1y), m_entry(n, f.szx, f.s1z, f.s1x),
+                          m_entry(n, f.szy, f.s1z, f.s1y), m_entry(n, f.szz, f.s1z, f.s1z)};
+    nbg_finish_row_d(a.grp, a.tf, a.ex, id, (int)min(f.cnt, 0x7FFFFFFFu), Md, f.qraw);
+}
+
+int launch_radius(Context* ctx, const RadiusLaunch& rl, cudaStream_t stream) {
+    (void)ctx;
+    const Tile* t = rl.tile;
+    if (!t->n) return NBG_OK;
+    RadiusArgs a;
+    a.gv = grid_view(t);
+    a.gp = t->gp;
+    a.n = t->n;
+    a.grp = rl.grp;
+    a.tf = t->tf;
+    a.ex = rl.ex;
+    a.rr = rl.radius * rl.radius;
+    const double s = t->tf.scale[0];
+    const double rr_raw = a.rr / (s * s);
+    a.dout = rr_raw > 0.0 ? (unsigned long long)ceil(rr_raw * (1.0 + 1e-5)) + 2ull : 0ull;
+    a.r_raw = sqrt((double)a.dout);
+    a.min_k = rl.min_k;
+    knn_radius_kernel<<<(unsigned)((t->n + 127) / 128), 128, 0, stream>>>(a);
+    NBG_LAUNCHED(1);
+    return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+}
+
 static int slots_for(int K) {
     const int need = K + 1;
     if (need <= 10) return 10;

@@ -520,7 +520,14 @@ extern "C" int nbg_filter_create(const char* type, const char* options_json, int
 extern "C" int nbg_filter_options(const nbg_filter* f, nbg_stage_opts* out) {
     if (!f || !out) return NBG_ERR_INVALID;
     *out = f->opts;
-    if (f->radius_set) return NBG_ERR_UNSUPPORTED;  // radius / min_k: not on this path yet
+    if (f->radius_set) {
+        out->use_radius = 1;
+        out->radius = f->radius;
+        out->min_k = (int32_t)std::max<int64_t>(0, std::min<int64_t>(f->min_k, INT32_MAX));
+        out->knn = 0;  // the reference zeroes or ignores knn with a radius
+        return NBG_OK;
+    }
+    out->min_k = (int32_t)std::max<int64_t>(0, std::min<int64_t>(f->min_k, INT32_MAX));
     if (f->opts.stride > 1) return NBG_ERR_UNSUPPORTED;
     return NBG_OK;
 }

@@ -81,6 +81,8 @@ extern "C" {
 #define NBG_ROW_ZERO_COV 2      /* covariance isZero() (|b_ij| <= 1e-12)      */
 #define NBG_ROW_EIGEN_FAIL 3    /* eigensolver reported failure               */
 #define NBG_ROW_ZERO_LAMBDA 4   /* covariancefeatures: largest eigenvalue 0   */
+#define NBG_ROW_RADIUS_FEW 5    /* radius search found fewer than min_k points;
+                                   `reserved` holds the count (capped at 65535) */
 
 #define NBG_MAX_DIMS 16
 
@@ -102,6 +104,12 @@ typedef struct nbg_stage_opts {
     int32_t mode;          /* covariancefeatures: NBG_MODE_*                 */
     int32_t stride;        /* keep every stride-th of knn*stride neighbours  */
     int32_t optimized;     /* covariancefeatures: per-point k = OptimalKNN   */
+    int32_t use_radius;    /* neighbours = the points within `radius` (squared
+                              FP64 distance < radius*radius) instead of knn
+                              (KDImpl.hpp:398-415)                           */
+    int32_t min_k;         /* eigenvalues/covariancefeatures with a radius:
+                              rows with fewer neighbours are skipped         */
+    double radius;
 } nbg_stage_opts;
 
 /* Output placement: dimension d of point id is the double at
@@ -219,8 +227,9 @@ int nbg_neighbor_sets(nbg_context* ctx, nbg_tile* tile, int32_t knn,
 typedef struct nbg_filter nbg_filter;
 int nbg_filter_create(const char* type, const char* options_json, int32_t has_optimal_knn,
                       int32_t has_optimal_radius, nbg_filter** filter, char* err, size_t err_len);
-/* The stage's nbg_stage_opts (knn as the user gave it).  NBG_ERR_UNSUPPORTED
- * (with *out still filled) for radius/min_k and stride > 1. */
+/* The stage's nbg_stage_opts (knn as the user gave it; with a radius,
+ * use_radius/radius/min_k set).  NBG_ERR_UNSUPPORTED (with *out still
+ * filled) for stride > 1 without a radius. */
 int nbg_filter_options(const nbg_filter* filter, nbg_stage_opts* out);
 /* Registered output dimensions, comma separated, in the library's order. */
 int nbg_filter_dims(const nbg_filter* filter, char* names, size_t len);

@@ -226,6 +226,17 @@ public:
         }
     };
 
+    // nanoflann's RadiusResultSet (nanoflann.hpp:225-275): keeps every point
+    // with dist < radius; its worst distance is the radius itself
+    struct RadiusResult {
+        double radius = 0.0;
+        std::vector<std::pair<uint64_t, double>> found;
+        double worst() const { return radius; }
+        void add(double dist, uint64_t id) {
+            if (dist < radius) found.emplace_back(id, dist);
+        }
+    };
+
     double metric(const double* q, uint64_t id) const {
         double r = 0.0;
         for (int d = 0; d < 3; ++d) {
@@ -235,7 +246,8 @@ public:
         return r;
     }
 
-    void search_level(Result& rs, const double* q, int64_t node, double mindistsq,
+    template <class RS>
+    void search_level(RS& rs, const double* q, int64_t node, double mindistsq,
                       double* dists) const {
         const Node& nd = nodes[node];
         if (nd.child1 < 0 && nd.child2 < 0) {
@@ -268,6 +280,33 @@ public:
         dists[idx] = cut;
         if (mindistsq * 1.0f <= rs.worst()) search_level(rs, q, other, mindistsq, dists);
         dists[idx] = dst;
+    }
+
+    // KD3ImplT::radius(x, y, z, r): ids with squared distance < r*r, sorted by
+    // distance (KDImpl.hpp:398-415; radiusSearch with params.sorted)
+    void radius_neighbors(const double q[3], double r, std::vector<uint64_t>& out) const {
+        RadiusResult rs;
+        rs.radius = r * r;
+        out.clear();
+        if (n == 0) return;
+        double dists[3] = {0, 0, 0};
+        double distsq = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            if (q[i] < root_lo[i]) {
+                dists[i] = (q[i] - root_lo[i]) * (q[i] - root_lo[i]);
+                distsq += dists[i];
+            }
+            if (q[i] > root_hi[i]) {
+                dists[i] = (q[i] - root_hi[i]) * (q[i] - root_hi[i]);
+                distsq += dists[i];
+            }
+        }
+        search_level(rs, q, 0, distsq, dists);
+        std::stable_sort(rs.found.begin(), rs.found.end(),
+                         [](const std::pair<uint64_t, double>& a, const std::pair<uint64_t, double>& b) {
+                             return a.second < b.second;
+                         });
+        for (auto& f : rs.found) out.push_back(f.first);
     }
 
     // KD3ImplT::neighbors(x, y, z, k, stride): returns the id list
@@ -815,6 +854,23 @@ int orc_run_stage(void* hv, const nbg_stage_opts* opts, const double* optimal_kn
         for (uint64_t i = b; i < e; ++i) {
             double q[3] = {X[0][i], X[1][i], X[2][i]};
             uint64_t k, stride = o.stride > 0 ? (uint64_t)o.stride : 1;
+            double kopt_i = optimal_knn ? optimal_knn[i] : 0.0;
+            double ropt_i = optimal_radius ? optimal_radius[i] : 0.0;
+            if (o.use_radius && !(o.kind == NBG_STAGE_COVARIANCEFEATURES && o.optimized)) {
+                // NormalFilter.cpp:149-150; EigenvaluesFilter.cpp:121-134;
+                // CovarianceFeaturesFilter.cpp:216-225
+                h->t.radius_neighbors(q, o.radius, ids);
+                if (o.kind != NBG_STAGE_NORMAL && ids.size() < (size_t)o.min_k) {
+                    status[i] = NBG_ROW_RADIUS_FEW;
+                    continue;
+                }
+                orc::Eig eg = orc::eigensystem(X, ids, mode);
+                int code = orc::project(o, eg, ids.size(), q, kopt_i, ropt_i, vals);
+                status[i] = (uint8_t)code;
+                if (code == 0)
+                    for (int d = 0; d < nd; ++d) out_cols[d][i] = vals[d];
+                continue;
+            }
             if (o.kind == NBG_STAGE_NORMAL) {
                 k = (uint64_t)(o.knn + 1);
                 stride = 1;

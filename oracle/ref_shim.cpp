@@ -73,6 +73,18 @@ struct RefTree {
     KDTree index;
     RefTree() : index(3, cloud, nanoflann::KDTreeSingleIndexAdaptorParams(100)) {}
 
+    // KD3ImplT::radius (KDImpl.hpp:398-415)
+    PointIdList radius(double x, double y, double z, double r) const {
+        PointIdList output;
+        std::vector<std::pair<std::size_t, double>> ret_matches;
+        nanoflann::SearchParams params;
+        params.sorted = true;
+        std::vector<double> pt{x, y, z};
+        const std::size_t count = index.radiusSearch(&pt[0], r * r, ret_matches, params);
+        for (std::size_t i = 0; i < count; ++i) output.push_back(ret_matches[i].first);
+        return output;
+    }
+
     PointIdList neighbors(double x, double y, double z, uint64_t k, size_t stride) const {
         k = (std::min<uint64_t>)(cloud.pts.size(), k);
         uint64_t k2 = stride * k;
@@ -131,7 +143,8 @@ int stage_row(const nbg_stage_opts& o, const RefTree& t, uint64_t i, const doubl
     const auto& p = t.cloud.pts[i];
     PointIdList ids;
     if (o.kind == NBG_STAGE_NORMAL) {
-        ids = t.neighbors(p[0], p[1], p[2], (uint64_t)(o.knn + 1), 1);
+        if (o.use_radius) ids = t.radius(p[0], p[1], p[2], o.radius);
+        else ids = t.neighbors(p[0], p[1], p[2], (uint64_t)(o.knn + 1), 1);
         if (ids.size() < 3) return NBG_ROW_TOO_FEW;
         auto B = covariance(t.cloud, ids);
         if (B.isZero()) return NBG_ROW_ZERO_COV;
@@ -156,7 +169,12 @@ int stage_row(const nbg_stage_opts& o, const RefTree& t, uint64_t i, const doubl
         return 0;
     }
     if (o.kind == NBG_STAGE_EIGENVALUES) {
-        ids = t.neighbors(p[0], p[1], p[2], (uint64_t)(o.knn + 1), (size_t)o.stride);
+        if (o.use_radius) {
+            ids = t.radius(p[0], p[1], p[2], o.radius);
+            if (ids.size() < (size_t)o.min_k) return NBG_ROW_RADIUS_FEW;
+        } else {
+            ids = t.neighbors(p[0], p[1], p[2], (uint64_t)(o.knn + 1), (size_t)o.stride);
+        }
         Eigen::Matrix3d B = covariance(t.cloud, ids);
         if (B.isZero()) return NBG_ROW_ZERO_COV;
         Eigen::SelfAdjointEigenSolver<Eigen::Matrix3d> solver(B);
@@ -171,10 +189,14 @@ int stage_row(const nbg_stage_opts& o, const RefTree& t, uint64_t i, const doubl
         out[2] = ev[2];
         return 0;
     }
-    if (o.optimized)
+    if (o.optimized) {
         ids = t.neighbors(p[0], p[1], p[2], (uint64_t)kopt_col[i], 1);
-    else
+    } else if (o.use_radius) {
+        ids = t.radius(p[0], p[1], p[2], o.radius);
+        if (ids.size() < (size_t)o.min_k) return NBG_ROW_RADIUS_FEW;
+    } else {
         ids = t.neighbors(p[0], p[1], p[2], (uint64_t)(o.knn + 1), (size_t)o.stride);
+    }
     auto B = covariance(t.cloud, ids);
     if (B.isZero()) return NBG_ROW_ZERO_COV;
     Eigen::SelfAdjointEigenSolver<Eigen::Matrix3d> solver(B);

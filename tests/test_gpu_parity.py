@@ -229,3 +229,61 @@ def test_covariancefeatures_optimized_per_point_k(nbg, port):
     got_status = U.status_from_exceptions(n, ex)
     assert np.count_nonzero(st) == np.count_nonzero(kopt == 0)
     U.compare_stage(o, outs[0], want, st, got_status, label="optimized vs f64")
+
+
+def _radius_lam(port, X, Y, Z, r):
+    lam, _ = port.tree(X, Y, Z).run_stage(abi.make_opts(abi.STAGE_EIGENVALUES, radius=r, min_k=0),
+                                          mode=1)
+    return lam
+
+
+@pytest.mark.parametrize("workload,r", [("terrain", 1.0), ("mixture", 0.6), ("stress", 0.4)])
+def test_radius_stages_match_oracle(nbg, port, ref, workload, r):
+    """radius/min_k (KD3Index::radius, KDImpl.hpp:398-415): the set of points
+    with squared FP64 distance < r*r; statuses (incl. too few within the
+    radius) exact; outputs within the stated bars of the FP64 oracle and of
+    the reference's own arithmetic."""
+    if workload == "terrain":
+        x, y, z = syn.terrain(250_000, 0)
+        m = (x < 8000) & (y < 8000)
+    elif workload == "mixture":
+        x, y, z = syn.mixture(4_000_000, 1)
+        m = (x < 7000) & (y < 7000)
+    else:
+        x, y, z = syn.stress(4_000_000, 2)
+        m = (x < 7000) & (y < 7000)
+    x, y, z = x[m], y[m], z[m]
+    n = len(x)
+    X, Y, Z = (syn.to_double(v) for v in (x, y, z))
+    kopt, ropt = syn.optimal_columns(n, 4, knn=10)
+    lam = _radius_lam(port, X, Y, Z, r)
+    tile = nbg.tile(x, y, z)
+    for o in (abi.make_opts(abi.STAGE_NORMAL, radius=r),
+              abi.make_opts(abi.STAGE_EIGENVALUES, radius=r, min_k=6),
+              abi.make_opts(abi.STAGE_COVARIANCEFEATURES, radius=r, min_k=4, feature_mask=abi.FEAT_ALL)):
+        outs, ex, _ = nbg.run(tile, [o], optimal_knn=kopt, optimal_radius=ropt)
+        got_status = U.status_from_exceptions(n, ex)
+        want64, st64 = port.tree(X, Y, Z).run_stage(o, mode=1, optimal_knn=kopt, optimal_radius=ropt)
+        U.compare_stage(o, outs[0], want64, st64, got_status, lam=lam, label=f"{workload} radius vs f64")
+        few = ex[ex["code"] == abi.ROW_RADIUS_FEW]
+        if o.kind != abi.STAGE_NORMAL:
+            assert (st64 == abi.ROW_RADIUS_FEW).sum() == len(few)
+        wref, stref = ref.tree(X, Y, Z).run_stage(o, mode=0, optimal_knn=kopt, optimal_radius=ropt)
+        U.compare_stage(o, outs[0], wref, stref, got_status, lam=lam,
+                        label=f"{workload} radius vs reference", gap_min=1e-2, sign_eps=1e-6,
+                        lam0_floor=1e-6)
+
+
+def test_radius_normal_known_answer(nbg):
+    # NormalFilterTest.cpp:255-313: two tilted 4-point patches, radius 2
+    x = np.array([0, 0, 1, 1, 9, 9, 10, 10], np.int32)
+    y = np.array([0, 1, 0, 1, 9, 10, 9, 10], np.int32)
+    z = np.array([0, 1, 0, 1, 9, 10, 9, 10], np.int32)
+    tile = nbg.tile(x, y, z, scale=(1.0, 1.0, 1.0))
+    (out,), ex, _ = nbg.run(tile, [abi.make_opts(abi.STAGE_NORMAL, radius=2.0)])
+    e = np.sqrt(2.0) / 2.0
+    assert len(ex) == 0
+    np.testing.assert_allclose(out[0], 0.0, atol=1e-6)
+    np.testing.assert_allclose(out[1], -e, atol=1e-6)
+    np.testing.assert_allclose(out[2], e, atol=1e-6)
+    np.testing.assert_allclose(out[3], 0.0, atol=1e-6)

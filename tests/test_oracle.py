@@ -193,3 +193,42 @@ def test_f64_mode_close_to_reference(port):
     assert np.array_equal(status, g["normal8_status"])
     # the reference narrows the centred coordinates to float: ~1e-7 differences
     assert np.nanmax(np.abs(outs - g["normal8_out"])) < 1e-4
+
+
+def test_reference_normal_radius(port):
+    # NormalFilterTest.cpp:255-313: two tilted 4-point patches, radius 2
+    X = np.array([0, 0, 1, 1, 9, 9, 10, 10], np.float64)
+    Y = np.array([0, 1, 0, 1, 9, 10, 9, 10], np.float64)
+    Z = np.array([0, 1, 0, 1, 9, 10, 9, 10], np.float64)
+    t = port.tree(X, Y, Z)
+    o = abi.make_opts(abi.STAGE_NORMAL, knn=8, radius=2.0)
+    out, status = t.run_stage(o, mode=0)
+    e = math.sqrt(2.0) / 2.0
+    assert (status == 0).all()
+    np.testing.assert_allclose(out[0], 0.0, atol=1e-6)
+    np.testing.assert_allclose(out[1], -e, atol=1e-6)
+    np.testing.assert_allclose(out[2], e, atol=1e-6)
+    np.testing.assert_allclose(out[3], 0.0, atol=1e-6)
+
+
+def test_port_matches_reference_radius_stages(port, ref):
+    """Radius search (KDImpl.hpp:398-415, nanoflann radiusSearch) and the
+    stages' radius/min_k branches: same statuses; outputs equal up to the
+    order in which equal-distance neighbours are summed."""
+    rng = np.random.default_rng(12)
+    x, y, z = syn.terrain(250_000, 0)
+    m = (x < 3000) & (y < 3000)
+    x, y, z = x[m], y[m], z[m]
+    X, Y, Z = (syn.to_double(v) for v in (x, y, z))
+    tp, tr = port.tree(X, Y, Z), ref.tree(X, Y, Z)
+    kopt, ropt = syn.optimal_columns(len(x), 3, knn=10)
+    for o in (abi.make_opts(abi.STAGE_NORMAL, radius=1.2),
+              abi.make_opts(abi.STAGE_EIGENVALUES, radius=0.9, min_k=8),
+              abi.make_opts(abi.STAGE_COVARIANCEFEATURES, radius=1.5, min_k=5,
+                            feature_mask=abi.FEAT_ALL)):
+        a, sa = tp.run_stage(o, mode=0, optimal_knn=kopt, optimal_radius=ropt)
+        b, sb = tr.run_stage(o, mode=0, optimal_knn=kopt, optimal_radius=ropt)
+        assert np.array_equal(sa, sb)
+        assert (sa == abi.ROW_RADIUS_FEW).any() or o.kind == abi.STAGE_NORMAL
+        ok = sa == 0
+        np.testing.assert_allclose(a[:, ok], b[:, ok], rtol=1e-9, atol=1e-12)

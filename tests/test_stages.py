@@ -39,7 +39,8 @@ def test_normal_knn_and_radius_conflict():
     with pytest.raises(StageError, match=r"^filters\.normal: Cannot set both knn and radius\.$"):
         Filter("filters.normal", {"knn": 8, "radius": 1.0})
     f = Filter("filters.normal", {"radius": 1.0})
-    assert f.options()[1] == abi.NBG_ERR_UNSUPPORTED
+    o, rc = f.options()
+    assert rc == abi.NBG_OK and o.use_radius == 1 and o.radius == 1.0
 
 
 def test_value_errors_as_programargs():
@@ -60,6 +61,9 @@ def test_eigenvalues_prepared_logs():
     f = Filter("filters.eigenvalues", {"radius": -1})
     assert f.log() == ["Radius has been set. Ignoring knn and stride values.",
                        "Radius must be greater than 0."]
+    f = Filter("filters.eigenvalues", {"radius": 2.5, "min_k": 6, "stride": 3})
+    o, rc = f.options()
+    assert rc == abi.NBG_OK and (o.use_radius, o.radius, o.min_k) == (1, 2.5, 6)
     assert Filter("filters.eigenvalues", {"stride": 2}).options()[1] == abi.NBG_ERR_UNSUPPORTED
 
 
