@@ -531,8 +531,10 @@ int validate_stages(Context* ctx, const nbg_stage_opts* stages, int n_stages,
         // a radius makes the reference ignore knn and stride
         // (EigenvaluesFilter.cpp:96-100, CovarianceFeaturesFilter.cpp:216-225)
         const bool by_radius = o.use_radius && !(o.kind == NBG_STAGE_COVARIANCEFEATURES && o.optimized);
-        if (!by_radius && o.kind != NBG_STAGE_NORMAL && o.stride != 1 && o.stride != 0)
-            return fail(ctx, NBG_ERR_UNSUPPORTED, "stride > 1 is not supported");
+        if (!by_radius && o.kind != NBG_STAGE_NORMAL && o.stride > 1 && !o.optimized &&
+            (int64_t)o.stride * (o.knn + 1) > 65)
+            return fail(ctx, NBG_ERR_UNSUPPORTED, "stride * (knn + 1) above 65 is not supported");
+        if (o.stride < 0) return fail(ctx, NBG_ERR_INVALID, "stride must be positive");
         if (by_radius && !(o.radius == o.radius))
             return fail(ctx, NBG_ERR_INVALID, "radius is not a number");
         if (o.kind != NBG_STAGE_COVARIANCEFEATURES && o.optimized)
@@ -780,11 +782,17 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         return stages[s].use_radius &&
                !(stages[s].kind == NBG_STAGE_COVARIANCEFEATURES && stages[s].optimized);
     };
+    // strided stages (eigenvalues / covariancefeatures; normal has no stride)
+    auto strided = [&](int s) {
+        return !by_radius(s) && stages[s].kind != NBG_STAGE_NORMAL && stages[s].stride > 1 &&
+               !stages[s].optimized;
+    };
     std::vector<std::vector<int>> groups;
     for (int s = 0; s < n_stages; ++s) {
         bool placed = false;
         for (auto& gr : groups) {
-            if (by_radius(gr[0]) || by_radius(s)) continue;  // radius stages run alone
+            // radius and strided stages run alone
+            if (by_radius(gr[0]) || by_radius(s) || strided(gr[0]) || strided(s)) continue;
             if (stage_k(gr[0]) == stage_k(s) && !stages[gr[0]].optimized == !stages[s].optimized) {
                 gr.push_back(s);
                 placed = true;
@@ -830,6 +838,43 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             cudaMemsetAsync(ctx->counters + 4, 0, sizeof(uint32_t), stream)) {
             cleanup();
             return NBG_ERR_CUDA;
+        }
+        if (strided(gr[0])) {
+            const int stride = stages[gr[0]].stride;
+            const int kpick = K;  // min(n, knn + 1)
+            const int K2 = kpick * stride;
+            rc = kd_ensure(ctx, t, stream);
+            if (rc) { cleanup(); return rc; }
+            QueryLaunch ql;
+            ql.tile = t;
+            ql.K = K2;
+            ql.rmax = 8;
+            ql.grp = g;
+            ql.ex = sink;
+            ql.exact_rows = ctx->exact_rows;
+            ql.counters = ctx->counters;
+            rc = launch_stride(ctx, ql, stride, kpick, kd_order(t), stream);
+            if (rc) { cleanup(); return fail(ctx, rc, "stride launch failed"); }
+            cudaEventRecord(ctx->ev[3], stream);
+            uint32_t cnt[3] = {0, 0, 0};
+            cudaError_t e = cudaMemcpyAsync(cnt, ctx->counters, sizeof(cnt), cudaMemcpyDeviceToHost,
+                                            stream);
+            if (!e) e = cudaStreamSynchronize(stream);
+            if (e) { cleanup(); return cuda_fail(ctx, e, "stride kernel"); }
+            tie_rows += cnt[1];
+            deferred_rows += cnt[2];
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+            grid_ms += ms;
+            cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+            query_ms += ms;
+            if (cnt[0]) {
+                replay_rows += cnt[0];
+                rc = kd_run_rows(ctx, t, K2, g, sink, ctx->exact_rows, cnt[0], stream, nullptr,
+                                 stride, kpick);
+                if (rc) { cleanup(); return rc; }
+            }
+            continue;
         }
         if (radius_group) {
             RadiusLaunch rl;

@@ -135,9 +135,10 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
                 return fail(ctx, NBG_ERR_UNSUPPORTED, "the stages of a batch item share one knn");
             if (it.outputs[s].on_device != 1)
                 return fail(ctx, NBG_ERR_UNSUPPORTED, "batch outputs are device-resident");
-            if (it.stages[s].use_radius || it.stages[s].optimized)
+            if (it.stages[s].use_radius || it.stages[s].optimized ||
+                (it.stages[s].kind != NBG_STAGE_NORMAL && it.stages[s].stride > 1))
                 return fail(ctx, NBG_ERR_UNSUPPORTED,
-                            "radius and optimized stages run through nbg_run, not the batch");
+                            "radius, optimized and strided stages run through nbg_run, not the batch");
         }
         const Tile* t = &it.tile->t;
         if (t->n == 0) continue;

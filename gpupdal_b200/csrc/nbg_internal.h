@@ -169,7 +169,11 @@ int kd_ensure(Context* ctx, Tile* t, cudaStream_t stream);
 int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t stream);
 int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const ExceptionSink& ex,
                 const uint32_t* rows, uint32_t nrows, cudaStream_t stream,
-                const double* row_k = nullptr);
+                const double* row_k = nullptr, int stride = 1, int kpick = 0);
+// Strided neighbourhoods of one stage over every row (K = k * stride);
+// needs the tile's KD replica.
+int launch_stride(Context* ctx, const QueryLaunch& q, int stride, int kpick, const KdOrder& kd,
+                  cudaStream_t stream);
 int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
                      uint32_t* ids_out, cudaStream_t stream);
 KdOrder kd_order(const Tile* t);

@@ -900,15 +900,17 @@ __global__ void kd_finish_kernel(Transform tf, const int32_t* __restrict__ x,
                                  const uint32_t* __restrict__ rows, uint32_t nrows, int K,
                                  const uint32_t* __restrict__ nbr,
                                  const uint32_t* __restrict__ counts, StageGroup g,
-                                 ExceptionSink ex) {
+                                 ExceptionSink ex, int stride, int kpick) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrows) return;
     const uint32_t id = rows[r];
     const int32_t qraw[3] = {x[id], y[id], z[id]};
-    const int cnt = (int)counts[r];
+    // with a stride the reference keeps entries 0, stride, ... of its k*stride
+    // list, unfilled entries reading point 0 (KDImpl.hpp:359-380)
+    const int cnt = stride > 1 ? kpick : (int)counts[r];
     long long s1[3] = {0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
     for (int s = 0; s < cnt; ++s) {
-        const uint32_t j = nbr[(uint64_t)r * K + s];
+        const uint32_t j = nbr[(uint64_t)r * K + (uint64_t)s * (stride > 1 ? stride : 1)];
         const long long d0 = (long long)x[j] - qraw[0];
         const long long d1 = (long long)y[j] - qraw[1];
         const long long d2 = (long long)z[j] - qraw[2];
@@ -1426,13 +1428,15 @@ static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, ui
 }
 
 int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const ExceptionSink& ex,
-                const uint32_t* rows, uint32_t nrows, cudaStream_t st, const double* row_k) {
+                const uint32_t* rows, uint32_t nrows, cudaStream_t st, const double* row_k,
+                int stride, int kpick) {
     if (!nrows) return NBG_OK;
     uint32_t *nbr = nullptr, *counts = nullptr;
     int rc = kd_search_rows(ctx, t, K, rows, nrows, &nbr, &counts, st, row_k);
     if (!rc) {
         kd_finish_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(t->tf, t->x, t->y, t->z, rows, nrows,
-                                                              K, nbr, counts, grp, ex);
+                                                              K, nbr, counts, grp, ex, stride,
+                                                              kpick);
         NBG_LAUNCHED(1);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);

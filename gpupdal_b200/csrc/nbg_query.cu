@@ -735,6 +735,183 @@ int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream) {
 }
 
 // ---------------------------------------------------------------------------
+// Strided neighbourhoods (eigenvalues / covariancefeatures stride > 1;
+// KD3ImplT::neighbors, KDImpl.hpp:351-381): the reference takes its k*stride
+// nearest in its own order and keeps every stride-th, so the order inside the
+// list matters, not only the set.  Per row: the ring search finds the
+// (k*stride)-th distance D; the points strictly closer and the group at D are
+// collected; m members of the group are chosen, and the whole list ordered,
+// by (FP64 distance as the reference forms it, then the order the reference's
+// search meets them on the KD replica's tree); positions 0, stride, 2*stride,
+// ... give the neighbourhood.  Rows the ring search cannot finish, or whose
+// group exceeds the collection, go to the search replay.
+static constexpr int STRIDE_LIST = 66;
+
+struct StrideFn {
+    float qx, qy, qz;
+    uint32_t kk;
+    int less, gcnt;
+    uint32_t id[STRIDE_LIST + TIE_CAP];  // [0, less): closer than D; then the group
+    int off[STRIDE_LIST + TIE_CAP][3];
+    uint32_t gid[TIE_CAP];
+    int goff[TIE_CAP][3];
+    __device__ __forceinline__ unsigned long long limit() const {
+        return (unsigned long long)(kk - KEY_BASE);
+    }
+    __device__ __forceinline__ void operator()(const float4 p) {
+        const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+        const uint32_t key = dist_key(dx, dy, dz);
+        if (key < kk) {
+            if (less < STRIDE_LIST) {
+                id[less] = __float_as_uint(p.w);
+                off[less][0] = small_int(dx);
+                off[less][1] = small_int(dy);
+                off[less][2] = small_int(dz);
+            }
+            ++less;
+        } else if (key == kk) {
+            if (gcnt < TIE_CAP) {
+                gid[gcnt] = __float_as_uint(p.w);
+                goff[gcnt][0] = small_int(dx);
+                goff[gcnt][1] = small_int(dy);
+                goff[gcnt][2] = small_int(dz);
+            }
+            ++gcnt;
+        }
+    }
+};
+
+struct StrideArgs {
+    QueryArgs q;       // K = k * stride (list length), ties null
+    int32_t stride;
+    int32_t kpick;     // k: entries kept
+    KdOrder kd;
+};
+
+__device__ __forceinline__ double ref_dist2(const double q64[3], const int32_t qraw[3],
+                                            const int o[3], const Transform& tf) {
+    double acc = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double pc = ref_coord(qraw[d] + o[d], tf.scale[d], tf.offset[d]);
+        const double df = __dsub_rn(q64[d], pc);
+        acc = __dadd_rn(acc, __dmul_rn(df, df));
+    }
+    return acc;
+}
+
+template <int KS>
+__global__ void __launch_bounds__(128) knn_stride_kernel(const StrideArgs sa) {
+    const QueryArgs& a = sa.q;
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const GridParams g = *a.gp;
+    const float4 q = __ldg(&a.gv.sorted[i]);
+    const uint32_t rid = __float_as_uint(q.w);
+    const int K = a.K;
+    QueryCell qc;
+    qc.qx = __float2int_rz(q.x);
+    qc.qy = __float2int_rz(q.y);
+    qc.qz = __float2int_rz(q.z);
+    qc.cx = qc.qx / g.cell;
+    qc.cy = qc.qy / g.cell;
+    qc.cz = qc.qz / g.cell;
+    int R;
+    uint32_t kk;
+    bool tie;
+    if (!select_kth<KS>(a, g, qc, q, K, R, kk, tie) && !tie) {
+        const uint32_t slot = atomicAdd(&a.counters[0], 1u);
+        a.exact_rows[slot] = rid;
+        return;
+    }
+    StrideFn f;
+    f.qx = q.x;
+    f.qy = q.y;
+    f.qz = q.z;
+    f.kk = kk;
+    f.less = 0;
+    f.gcnt = 0;
+    for (int r = 0; r <= R; ++r) scan_shell(a.gv, g, qc, r, f);
+    const int m = K - f.less;
+    if (f.gcnt > TIE_CAP || f.less > STRIDE_LIST || m <= 0 || m > f.gcnt) {
+        const uint32_t slot = atomicAdd(&a.counters[0], 1u);
+        a.exact_rows[slot] = rid;
+        return;
+    }
+    const int32_t qraw[3] = {qc.qx + g.minx, qc.qy + g.miny, qc.qz + g.minz};
+    const double q64[3] = {ref_coord(qraw[0], a.tf.scale[0], a.tf.offset[0]),
+                           ref_coord(qraw[1], a.tf.scale[1], a.tf.offset[1]),
+                           ref_coord(qraw[2], a.tf.scale[2], a.tf.offset[2])};
+    // the group's m members the reference admits (as the tie-order resolver)
+    double gd[TIE_CAP];
+    for (int t = 0; t < f.gcnt; ++t) gd[t] = ref_dist2(q64, qraw, f.goff[t], a.tf);
+    uint32_t taken = 0;
+    for (int j = 0; j < m; ++j) {
+        int best = -1;
+        for (int t = 0; t < f.gcnt; ++t) {
+            if ((taken >> t) & 1u) continue;
+            if (best < 0 || gd[t] < gd[best] ||
+                (gd[t] == gd[best] &&
+                 kd_meets_first(sa.kd, q64, __ldg(&sa.kd.kpos[sa.kd.base + f.gid[t]]),
+                                __ldg(&sa.kd.kpos[sa.kd.base + f.gid[best]]))))
+                best = t;
+        }
+        taken |= 1u << best;
+        f.id[f.less + j] = f.gid[best];
+        f.off[f.less + j][0] = f.goff[best][0];
+        f.off[f.less + j][1] = f.goff[best][1];
+        f.off[f.less + j][2] = f.goff[best][2];
+    }
+    // the list in the reference's order: FP64 distance, then visiting order
+    double d[STRIDE_LIST + TIE_CAP];
+    for (int t = 0; t < K; ++t) d[t] = ref_dist2(q64, qraw, f.off[t], a.tf);
+    for (int t = 1; t < K; ++t) {
+        const double dv = d[t];
+        const uint32_t iv = f.id[t];
+        const int o0 = f.off[t][0], o1 = f.off[t][1], o2 = f.off[t][2];
+        int u = t - 1;
+        while (u >= 0 &&
+               (d[u] > dv || (d[u] == dv && kd_meets_first(sa.kd, q64, __ldg(&sa.kd.kpos[sa.kd.base + iv]),
+                                                           __ldg(&sa.kd.kpos[sa.kd.base + f.id[u]]))))) {
+            d[u + 1] = d[u];
+            f.id[u + 1] = f.id[u];
+            f.off[u + 1][0] = f.off[u][0];
+            f.off[u + 1][1] = f.off[u][1];
+            f.off[u + 1][2] = f.off[u][2];
+            --u;
+        }
+        d[u + 1] = dv;
+        f.id[u + 1] = iv;
+        f.off[u + 1][0] = o0;
+        f.off[u + 1][1] = o1;
+        f.off[u + 1][2] = o2;
+    }
+    long long s1[3] = {0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
+    for (int j = 0; j < sa.kpick; ++j) {
+        const int t = j * sa.stride;  // < K by construction (K = kpick * stride)
+        const long long d0 = f.off[t][0], d1 = f.off[t][1], d2 = f.off[t][2];
+        s1[0] += d0;
+        s1[1] += d1;
+        s1[2] += d2;
+        s2[0] += d0 * d0;
+        s2[1] += d1 * d0;
+        s2[2] += d1 * d1;
+        s2[3] += d2 * d0;
+        s2[4] += d2 * d1;
+        s2[5] += d2 * d2;
+    }
+    const long long n = sa.kpick;
+    long long M[6];
+    M[0] = n * s2[0] - s1[0] * s1[0];
+    M[1] = n * s2[1] - s1[1] * s1[0];
+    M[2] = n * s2[2] - s1[1] * s1[1];
+    M[3] = n * s2[3] - s1[2] * s1[0];
+    M[4] = n * s2[4] - s1[2] * s1[1];
+    M[5] = n * s2[5] - s1[2] * s1[2];
+    nbg_finish_row(a.grp, a.tf, a.ex, rid, (int)n, M, qraw);
+}
+
+// ---------------------------------------------------------------------------
 // Radius neighbourhoods (NormalFilter.cpp:149-150, EigenvaluesFilter.cpp:
 // 121-134, CovarianceFeaturesFilter.cpp:216-225 through KD3Index::radius,
 // KDImpl.hpp:398-415): the points whose squared FP64 distance, formed as the
@@ -1029,6 +1206,51 @@ int launch_finish_queue(Context* ctx, const BatchJob* jobs, int njobs, uint64_t 
     knn_finish_queue_kernel<<<(unsigned)grid, 128, 0, stream>>>(jobs, njobs, items, head);
     NBG_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+}
+
+struct StrideLaunchArgs {
+    StrideArgs s;
+    unsigned blocks;
+    cudaStream_t stream;
+};
+
+template <int KS>
+struct StrideLauncher {
+    using Args = StrideLaunchArgs;
+    static int run(const StrideLaunchArgs& l) {
+        if (!l.blocks) return NBG_OK;
+        knn_stride_kernel<KS><<<l.blocks, 128, 0, l.stream>>>(l.s);
+        NBG_LAUNCHED(1);
+        return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+    }
+};
+
+int launch_stride(Context* ctx, const QueryLaunch& ql, int stride, int kpick, const KdOrder& kd,
+                  cudaStream_t stream) {
+    (void)ctx;
+    StrideLaunchArgs l{};
+    QueryArgs& q = l.s.q;
+    q.gv = grid_view(ql.tile);
+    q.gp = ql.tile->gp;
+    q.n = ql.tile->n;
+    q.K = ql.K;
+    q.rmax = ql.rmax;
+    q.grp = ql.grp;
+    q.tf = ql.tile->tf;
+    q.ex = ql.ex;
+    q.exact_rows = ql.exact_rows;
+    q.counters = ql.counters;
+    q.ids_out = nullptr;
+    q.ties = nullptr;
+    q.tie_cap = 0;
+    q.sums = nullptr;
+    q.row_k = nullptr;
+    l.s.stride = stride;
+    l.s.kpick = kpick;
+    l.s.kd = kd;
+    l.blocks = (unsigned)((ql.tile->n + 127) / 128);
+    l.stream = stream;
+    return dispatch_slots<StrideLauncher>(ql.K, l);
 }
 
 }  // namespace nbg

@@ -528,7 +528,8 @@ extern "C" int nbg_filter_options(const nbg_filter* f, nbg_stage_opts* out) {
         return NBG_OK;
     }
     out->min_k = (int32_t)std::max<int64_t>(0, std::min<int64_t>(f->min_k, INT32_MAX));
-    if (f->opts.stride > 1) return NBG_ERR_UNSUPPORTED;
+    if (f->opts.stride > 1 && (int64_t)f->opts.stride * (f->opts.knn + 1) > 65)
+        return NBG_ERR_UNSUPPORTED;
     return NBG_OK;
 }
 

@@ -229,7 +229,7 @@ int nbg_filter_create(const char* type, const char* options_json, int32_t has_op
                       int32_t has_optimal_radius, nbg_filter** filter, char* err, size_t err_len);
 /* The stage's nbg_stage_opts (knn as the user gave it; with a radius,
  * use_radius/radius/min_k set).  NBG_ERR_UNSUPPORTED (with *out still
- * filled) for stride > 1 without a radius. */
+ * filled) when stride * (knn + 1) exceeds 65. */
 int nbg_filter_options(const nbg_filter* filter, nbg_stage_opts* out);
 /* Registered output dimensions, comma separated, in the library's order. */
 int nbg_filter_dims(const nbg_filter* filter, char* names, size_t len);

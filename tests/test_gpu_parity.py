@@ -287,3 +287,38 @@ def test_radius_normal_known_answer(nbg):
     np.testing.assert_allclose(out[1], -e, atol=1e-6)
     np.testing.assert_allclose(out[2], e, atol=1e-6)
     np.testing.assert_allclose(out[3], 0.0, atol=1e-6)
+
+
+@pytest.mark.parametrize("workload", ["mixture", "stress", "ties_lattice"])
+def test_strided_stages_match_oracle(nbg, port, ref, workload):
+    """stride > 1 (KD3ImplT::neighbors, KDImpl.hpp:351-381): entries 0,
+    stride, 2*stride, ... of the reference's own k*stride ordering (FP64
+    distance, then its search's visiting order), so the lattice's many equal
+    distances exercise the order inside the list, not only its boundary."""
+    if workload == "ties_lattice":
+        g = U.golden("ties_lattice")
+        x, y, z = g["x"], g["y"], g["z"]
+    elif workload == "mixture":
+        x, y, z = syn.mixture(4_000_000, 1)
+        m = (x < 8000) & (y < 8000)
+        x, y, z = x[m], y[m], z[m]
+    else:
+        x, y, z = syn.stress(4_000_000, 2)
+        m = (x < 8000) & (y < 8000)
+        x, y, z = x[m], y[m], z[m]
+    n = len(x)
+    X, Y, Z = (syn.to_double(v) for v in (x, y, z))
+    tile = nbg.tile(x, y, z)
+    kopt, ropt = syn.optimal_columns(n, 6, knn=10)
+    for o in (abi.make_opts(abi.STAGE_EIGENVALUES, knn=8, stride=2),
+              abi.make_opts(abi.STAGE_COVARIANCEFEATURES, knn=10, stride=3,
+                            feature_mask=abi.FEAT_ALL, mode=abi.MODE_NORMALIZED)):
+        outs, ex, _ = nbg.run(tile, [o], optimal_knn=kopt, optimal_radius=ropt)
+        got_status = U.status_from_exceptions(n, ex)
+        lam, _ = f64_eigen(port, X, Y, Z, o.knn, stride=o.stride)
+        want64, st64 = port.tree(X, Y, Z).run_stage(o, mode=1, optimal_knn=kopt, optimal_radius=ropt)
+        U.compare_stage(o, outs[0], want64, st64, got_status, lam=lam, label=f"{workload} stride vs f64")
+        wref, stref = ref.tree(X, Y, Z).run_stage(o, mode=0, optimal_knn=kopt, optimal_radius=ropt)
+        U.compare_stage(o, outs[0], wref, stref, got_status, lam=lam,
+                        label=f"{workload} stride vs reference", gap_min=1e-2, sign_eps=1e-6,
+                        lam0_floor=1e-6)

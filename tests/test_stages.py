@@ -64,7 +64,8 @@ def test_eigenvalues_prepared_logs():
     f = Filter("filters.eigenvalues", {"radius": 2.5, "min_k": 6, "stride": 3})
     o, rc = f.options()
     assert rc == abi.NBG_OK and (o.use_radius, o.radius, o.min_k) == (1, 2.5, 6)
-    assert Filter("filters.eigenvalues", {"stride": 2}).options()[1] == abi.NBG_ERR_UNSUPPORTED
+    assert Filter("filters.eigenvalues", {"stride": 2}).options()[1] == abi.NBG_OK
+    assert Filter("filters.eigenvalues", {"stride": 8, "knn": 8}).options()[1] == abi.NBG_ERR_UNSUPPORTED
 
 
 def test_covariancefeatures_feature_sets_and_mode():
