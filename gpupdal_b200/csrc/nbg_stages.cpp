@@ -566,6 +566,12 @@ extern "C" int nbg_filter_report(nbg_filter* f, const nbg_row_exception* ex, uin
             f->log += o.str() + "\n";
             continue;
         }
+        if (r.code == NBG_ROW_RADIUS_FEW) {
+            o << "Skipping point " << id << ". Found " << r.reserved << " neighbors but required "
+              << f->min_k << ".";
+            f->log += o.str() + "\n";
+            continue;
+        }
         if (r.code == NBG_ROW_ZERO_COV) {
             o << "Skipping point " << id << ". Covariance matrix is all zeros. This suggests a large "
                  "number of redundant points. Consider using filters.sample with a small radius to "

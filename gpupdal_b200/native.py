@@ -23,6 +23,11 @@ def _dptr(a):
     return ctypes.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
 
 
+# row exceptions as returned: the point, the stage index, the NBG_ROW_* code and
+# the code's detail (the neighbour count of NBG_ROW_RADIUS_FEW rows)
+EXC_DTYPE = [("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8), ("reserved", np.uint16)]
+
+
 def record_columns(base_ptr, stages, record_bytes, on_device):
     """abi.Columns for `stages` sharing one record per point: the stages'
     dims are laid out one after another from offset 0."""
@@ -123,9 +128,9 @@ class Context:
                               ctypes.c_void_p(stream) if stream else None)
         self._check(rc)
         m = min(nexc.value, cap)
-        ex = np.zeros(m, dtype=[("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8)])
+        ex = np.zeros(m, dtype=EXC_DTYPE)
         for j in range(m):
-            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code)
+            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code, exc[j].reserved)
         return [o[: len(abi.stage_dims(s))] for o, s in zip(outs, stages)], ex, stats
 
     def run_columns(self, tile, stages, columns, optimal_knn=None, optimal_radius=None,
@@ -149,9 +154,9 @@ class Context:
                               ctypes.c_void_p(stream) if stream else None)
         self._check(rc)
         m = min(nexc.value, cap)
-        ex = np.zeros(m, dtype=[("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8)])
+        ex = np.zeros(m, dtype=EXC_DTYPE)
         for j in range(m):
-            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code)
+            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code, exc[j].reserved)
         return ex, stats
 
     def run_batch(self, tiles, stages, outputs, optimal=None, graph=True, autotune=False,
@@ -191,9 +196,9 @@ class Context:
         out = []
         for i in range(m):
             k = min(nex[i], exception_capacity)
-            ex = np.zeros(k, dtype=[("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8)])
+            ex = np.zeros(k, dtype=EXC_DTYPE)
             for j in range(k):
-                ex[j] = (excs[i][j].point_id, excs[i][j].stage, excs[i][j].code)
+                ex[j] = (excs[i][j].point_id, excs[i][j].stage, excs[i][j].code, excs[i][j].reserved)
             out.append(ex)
         return out, stats
 
@@ -367,9 +372,9 @@ class Server:
         if res.status != abi.NBG_OK:
             raise NbgError(res.status, self.lib.nbg_server_last_error(self.h).decode())
         m = min(res.n_exceptions, len(exc))
-        ex = np.zeros(m, dtype=[("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8)])
+        ex = np.zeros(m, dtype=EXC_DTYPE)
         for j in range(m):
-            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code)
+            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code, exc[j].reserved)
         return [o[: len(abi.stage_dims(s))] for o, s in zip(outs, stages)], ex, res
 
     def close(self):

@@ -57,6 +57,8 @@ class Filter:
         arr = (abi.RowException * max(n, 1))()
         for i, e in enumerate(exceptions):
             arr[i].point_id, arr[i].stage, arr[i].code = int(e["point_id"]), int(e["stage"]), int(e["code"])
+            if "reserved" in e.dtype.names:
+                arr[i].reserved = int(e["reserved"])
         err = ctypes.create_string_buffer(1024)
         rc = self.lib.nbg_filter_report(self.h, arr, n, int(stage_index), err, len(err))
         if rc != abi.NBG_OK:

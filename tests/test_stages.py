@@ -125,3 +125,9 @@ def test_pipeline_json_forms():
         parse_pipeline('{"stages": []}')
     with pytest.raises(StageError):
         parse_pipeline('[{"type": "filters.normal",]')
+
+
+def test_radius_few_report():
+    f = Filter("filters.covariancefeatures", {"radius": 1.0, "min_k": 7})
+    f.report(_ex([(12, 0, abi.ROW_RADIUS_FEW)]))
+    assert f.log()[-1] == "Skipping point 12. Found 0 neighbors but required 7."
