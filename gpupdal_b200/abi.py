@@ -169,6 +169,23 @@ class RequestResult(ctypes.Structure):
     ]
 
 
+class LasInfo(ctypes.Structure):
+    _fields_ = [
+        ("version_major", ctypes.c_uint8),
+        ("version_minor", ctypes.c_uint8),
+        ("point_format", ctypes.c_uint8),
+        ("compressed", ctypes.c_uint8),
+        ("point_record_length", ctypes.c_uint16),
+        ("reserved", ctypes.c_uint16),
+        ("offset_to_points", ctypes.c_uint32),
+        ("point_count", ctypes.c_uint64),
+        ("scale", ctypes.c_double * 3),
+        ("offset", ctypes.c_double * 3),
+        ("min", ctypes.c_double * 3),
+        ("max", ctypes.c_double * 3),
+    ]
+
+
 def stage_dims(opts: StageOpts) -> list:
     """Output dimension names of one stage, in the library's order."""
     if opts.kind == STAGE_NORMAL:
@@ -229,6 +246,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                     ctypes.POINTER(ctypes.c_double), i32, vp,
                                     ctypes.POINTER(vp)]
     lib.nbg_tile_upload.restype = ctypes.c_int
+    lib.nbg_las_header.argtypes = [vp, ctypes.c_size_t, ctypes.POINTER(LasInfo)]
+    lib.nbg_las_header.restype = ctypes.c_int
+    lib.nbg_tile_upload_las.argtypes = [vp, vp, u64, ctypes.c_uint32, i32,
+                                        ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_double), vp, ctypes.POINTER(vp)]
+    lib.nbg_tile_upload_las.restype = ctypes.c_int
     lib.nbg_tile_free.argtypes = [vp, vp]
     lib.nbg_tile_free.restype = ctypes.c_int
     lib.nbg_tile_tune.argtypes = [vp, vp, ctypes.c_float, i32]

@@ -405,6 +405,41 @@ int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const in
     Context* ctx = &h->c;
     *out = nullptr;
     if (n > 0 && (!x || !y || !z)) return fail(ctx, NBG_ERR_INVALID, "null coordinate array");
+    nbg_tile* th = nullptr;
+    int rc = tile_alloc(ctx, n, scale, offset, &th);
+    if (rc) return rc;
+    Tile* t = &th->t;
+    cudaStream_t stream = (cudaStream_t)stream_v;
+    if (n) {
+        int urc = NBG_OK;
+        if (on_device) {
+            cudaError_t e = cudaMemcpyAsync(t->x, x, n * 4, cudaMemcpyDeviceToDevice, stream);
+            if (!e) e = cudaMemcpyAsync(t->y, y, n * 4, cudaMemcpyDeviceToDevice, stream);
+            if (!e) e = cudaMemcpyAsync(t->z, z, n * 4, cudaMemcpyDeviceToDevice, stream);
+            if (e) urc = cuda_fail(ctx, e, "coordinate upload");
+        } else {
+            urc = host_to_device(ctx, t->x, x, n * 4, stream);
+            if (!urc) urc = host_to_device(ctx, t->y, y, n * 4, stream);
+            if (!urc) urc = host_to_device(ctx, t->z, z, n * 4, stream);
+        }
+        if (urc) {
+            tile_release(ctx, t);
+            delete th;
+            return urc;
+        }
+    }
+    *out = th;
+    return NBG_OK;
+}
+
+}  // extern "C"
+
+namespace nbg {
+
+// A tile of n points with its device storage, coordinates not yet filled.
+int tile_alloc(Context* ctx, uint64_t n, const double scale[3], const double offset[3],
+               nbg_tile** out) {
+    *out = nullptr;
     if (n >= 0x7FFFFFF0ull) return fail(ctx, NBG_ERR_UNSUPPORTED, "tile larger than 2^31 points");
     if (!scale || !offset) return fail(ctx, NBG_ERR_INVALID, "null scale/offset");
     for (int d = 0; d < 3; ++d)
@@ -414,7 +449,6 @@ int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const in
         return fail(ctx, NBG_ERR_UNSUPPORTED,
                     "the integer distance order needs one scale for x, y and z");
     cudaSetDevice(ctx->device);
-    cudaStream_t stream = (cudaStream_t)stream_v;
     nbg_tile* th = new (std::nothrow) nbg_tile();
     if (!th) return NBG_ERR_OOM;
     Tile* t = &th->t;
@@ -448,27 +482,18 @@ int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const in
         delete th;
         return rc;
     }
-    if (n) {
-        int urc = NBG_OK;
-        if (on_device) {
-            cudaError_t e = cudaMemcpyAsync(t->x, x, n * 4, cudaMemcpyDeviceToDevice, stream);
-            if (!e) e = cudaMemcpyAsync(t->y, y, n * 4, cudaMemcpyDeviceToDevice, stream);
-            if (!e) e = cudaMemcpyAsync(t->z, z, n * 4, cudaMemcpyDeviceToDevice, stream);
-            if (e) urc = cuda_fail(ctx, e, "coordinate upload");
-        } else {
-            urc = host_to_device(ctx, t->x, x, n * 4, stream);
-            if (!urc) urc = host_to_device(ctx, t->y, y, n * 4, stream);
-            if (!urc) urc = host_to_device(ctx, t->z, z, n * 4, stream);
-        }
-        if (urc) {
-            tile_release(ctx, t);
-            delete th;
-            return urc;
-        }
-    }
     *out = th;
     return NBG_OK;
 }
+
+void tile_destroy(Context* ctx, nbg_tile* th) {
+    tile_release(ctx, &th->t);
+    delete th;
+}
+
+}  // namespace nbg
+
+extern "C" {
 
 int nbg_tile_tune(nbg_context* h, nbg_tile* th, float cell_factor, int32_t fixed_cell) {
     if (!h || !th) return NBG_ERR_INVALID;

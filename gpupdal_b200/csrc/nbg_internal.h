@@ -13,6 +13,8 @@
 
 #include "nbg_common.cuh"
 
+struct nbg_tile;
+
 namespace nbg {
 
 struct KdReplica;  // exact nanoflann replica (nbg_kdtree.cu)
@@ -192,6 +194,12 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
 // Autotuner (nbg_tile_autotune without the context lock).
 int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, int32_t n_candidates,
                   bool use_cache, float* chosen, cudaStream_t stream);
+
+// A tile of n points with its device storage allocated (coordinates unset),
+// and its release (nbg_api.cu).
+int tile_alloc(Context* ctx, uint64_t n, const double scale[3], const double offset[3],
+               nbg_tile** out);
+void tile_destroy(Context* ctx, nbg_tile* th);
 
 // Batched form: the context's batch scratch and cached graph (nbg_batch.cu).
 void batch_release(Context* ctx);

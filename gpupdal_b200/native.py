@@ -77,6 +77,28 @@ class Context:
     def tile(self, x, y, z, scale=(0.01, 0.01, 0.01), offset=(0.0, 0.0, 0.0), stream=None):
         return Tile(self, x, y, z, scale, offset, stream)
 
+    def tile_from_las(self, src, records=None, stream=None):
+        """A tile straight from LAS point records (nbg_tile_upload_las).
+
+        `src` is a path or a las.LasFile; its records are copied from the
+        mapped file and decoded on the device.  `records` overrides them with
+        the same records already on the device (a uint8 torch tensor of
+        point_count x point_record_length bytes)."""
+        from . import las
+        f = src if isinstance(src, las.LasFile) else las.LasFile(src)
+        rec = f.records if records is None else records
+        if records is not None and int(records.numel()) != f.n * f.record_length:
+            raise ValueError("device records do not match the file's record extent")
+        sc = (ctypes.c_double * 3)(*f.scale)
+        of = (ctypes.c_double * 3)(*f.offset)
+        h = ctypes.c_void_p()
+        rc = self.lib.nbg_tile_upload_las(self.h, _dptr(rec), f.n, f.record_length,
+                                          int(records is not None), sc, of,
+                                          ctypes.c_void_p(stream) if stream else None,
+                                          ctypes.byref(h))
+        self._check(rc)
+        return Tile._adopt(self, h, f.n, (f, rec))
+
     # -- stages -----------------------------------------------------------
     def run(self, tile, stages, optimal_knn=None, optimal_radius=None, device_out=False,
             fresh=True, exception_capacity=None, stream=None, out=None):
@@ -248,6 +270,12 @@ class Tile:
                                      ctypes.byref(h))
         ctx._check(rc)
         self.h = h
+
+    @classmethod
+    def _adopt(cls, ctx, h, n, keep):
+        t = cls.__new__(cls)
+        t.ctx, t.h, t.n, t._keep = ctx, h, int(n), keep
+        return t
 
     def tune(self, cell_factor=4.0, fixed_cell=0):
         self.ctx._check(self.ctx.lib.nbg_tile_tune(self.ctx.h, self.h, float(cell_factor),

@@ -215,6 +215,34 @@ int nbg_neighbor_sets(nbg_context* ctx, nbg_tile* tile, int32_t knn,
                       uint32_t* ids_out, int32_t ids_on_device,
                       nbg_run_stats* stats, void* stream);
 
+/* LAS ingest -------------------------------------------------------------
+ * The fields of a LAS 1.0-1.4 public header block the path needs, and a tile
+ * made straight from the file's point records: the records (host or device
+ * memory, record_length bytes each, X/Y/Z int32 at their start as in every
+ * point format 0-10) are decoded on the device, so coordinates enter as the
+ * file's own raw integers with its scale and offset.  Replaces the reader
+ * step of the fork's device LAS path (src/io/las/LasKernels.cu:266-321,
+ * src/pdal/PdgNeighborhood.cpp:1115-1192).  LAZ (compressed) records are not
+ * decoded here: nbg_las_header reports them in `compressed`. */
+typedef struct nbg_las_info {
+    uint8_t version_major;
+    uint8_t version_minor;
+    uint8_t point_format;         /* 0-10                                   */
+    uint8_t compressed;           /* LAZ: records are not plain LAS records  */
+    uint16_t point_record_length;
+    uint16_t reserved;
+    uint32_t offset_to_points;    /* byte offset of the first record         */
+    uint64_t point_count;
+    double scale[3];
+    double offset[3];
+    double min[3];
+    double max[3];
+} nbg_las_info;
+int nbg_las_header(const void* bytes, size_t size, nbg_las_info* info);
+int nbg_tile_upload_las(nbg_context* ctx, const void* records, uint64_t n,
+                        uint32_t record_length, int32_t on_device, const double scale[3],
+                        const double offset[3], void* stream, nbg_tile** tile);
+
 /* Stage layer ------------------------------------------------------------
  * PDAL pipeline JSON and the stage logic above nbg_run, so an existing
  * pipeline is a drop-in.  nbg_filter_create parses one stage's options

@@ -52,6 +52,8 @@ int main(void) {
   printf("%zu %zu %zu %zu %zu %zu\n", sizeof(nbg_request), sizeof(nbg_request_result),
          offsetof(nbg_request, stages), offsetof(nbg_request, user_tag),
          offsetof(nbg_request_result, stats), offsetof(nbg_run_stats, kd_build_ms));
+  printf("%zu %zu %zu\n", sizeof(nbg_las_info), offsetof(nbg_las_info, point_count),
+         offsetof(nbg_las_info, max));
   return 0;
 }
 """
@@ -71,6 +73,9 @@ int main(void) {
     assert served == [ctypes.sizeof(abi.Request), ctypes.sizeof(abi.RequestResult),
                       abi.Request.stages.offset, abi.Request.user_tag.offset,
                       abi.RequestResult.stats.offset, abi.RunStats.kd_build_ms.offset]
+    las = [int(v) for v in lines[3].split()]
+    assert las == [ctypes.sizeof(abi.LasInfo), abi.LasInfo.point_count.offset,
+                   abi.LasInfo.max.offset]
 
 
 def test_loader_fails_loudly_without_the_library(tmp_path):
