@@ -26,6 +26,12 @@ NBG_ERR_EXCEPTIONS = 8
 STAGE_NORMAL = 1
 STAGE_EIGENVALUES = 2
 STAGE_COVARIANCEFEATURES = 3
+STAGE_APPROXIMATECOPLANAR = 4
+STAGE_ESTIMATERANK = 5
+STAGE_NNDISTANCE = 6
+STAGE_OPTIMALNEIGHBORHOOD = 7
+STAGE_LOF = 8
+STAGE_OUTLIER = 9
 
 # covariance feature bits, reference order of feature_set "all"
 FEATURES = [
@@ -61,6 +67,14 @@ NOALLOC_MAX_POINTS = 524288
 
 NORMAL_DIMS = ["NormalX", "NormalY", "NormalZ", "Curvature"]
 EIGENVALUE_DIMS = ["Eigenvalue0", "Eigenvalue1", "Eigenvalue2"]
+CONSUMER_DIMS = {
+    STAGE_APPROXIMATECOPLANAR: ["Coplanar"],
+    STAGE_ESTIMATERANK: ["Rank"],
+    STAGE_NNDISTANCE: ["NNDistance"],
+    STAGE_OPTIMALNEIGHBORHOOD: ["OptimalKNN", "OptimalRadius"],
+    STAGE_LOF: ["NNDistance", "LocalReachabilityDistance", "LocalOutlierFactor"],
+    STAGE_OUTLIER: ["Classification"],
+}
 
 
 class StageOpts(ctypes.Structure):
@@ -79,6 +93,10 @@ class StageOpts(ctypes.Structure):
         ("use_radius", ctypes.c_int32),
         ("min_k", ctypes.c_int32),
         ("radius", ctypes.c_double),
+        ("thresh1", ctypes.c_double),
+        ("thresh2", ctypes.c_double),
+        ("label", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
     ]
 
 
@@ -114,6 +132,8 @@ class RunStats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint64),
         ("replay_rows", ctypes.c_uint64),
         ("kd_build_ms", ctypes.c_double),
+        ("outliers", ctypes.c_uint64),
+        ("inliers", ctypes.c_uint64),
     ]
 
 
@@ -192,12 +212,15 @@ def stage_dims(opts: StageOpts) -> list:
         return list(NORMAL_DIMS)
     if opts.kind == STAGE_EIGENVALUES:
         return list(EIGENVALUE_DIMS)
+    if opts.kind in CONSUMER_DIMS:
+        return list(CONSUMER_DIMS[opts.kind])
     return [f for i, f in enumerate(FEATURES) if opts.feature_mask & (1 << i)]
 
 
 def make_opts(kind, knn=8, always_up=True, viewpoint=None, refine=False,
               normalize=False, feature_mask=FEAT_DIMENSIONALITY, mode=MODE_SQRT,
-              stride=1, optimized=False, radius=None, min_k=3) -> StageOpts:
+              stride=1, optimized=False, radius=None, min_k=3, thresh1=0.0, thresh2=0.0,
+              label=0) -> StageOpts:
     o = StageOpts()
     o.kind = int(kind)
     o.knn = int(knn)
@@ -215,7 +238,36 @@ def make_opts(kind, knn=8, always_up=True, viewpoint=None, refine=False,
     o.use_radius = int(radius is not None)
     o.radius = float(radius) if radius is not None else 0.0
     o.min_k = int(min_k)
+    o.thresh1 = float(thresh1)
+    o.thresh2 = float(thresh2)
+    o.label = int(label)
     return o
+
+
+def consumer_opts(kind, **kw) -> StageOpts:
+    """Options of a kNN-consumer stage under the reference's option names
+    and defaults (ApproximateCoplanarFilter.cpp:66-71, EstimateRankFilter.cpp:
+    66-70, NNDistanceFilter.cpp:95-99, OptimalNeighborhoodFilter.cpp:62-66,
+    LOFFilter.cpp:62-65, OutlierFilter.cpp:62-71)."""
+    if kind == STAGE_APPROXIMATECOPLANAR:
+        return make_opts(kind, knn=kw.get("knn", 8), thresh1=kw.get("thresh1", 25.0),
+                         thresh2=kw.get("thresh2", 6.0))
+    if kind == STAGE_ESTIMATERANK:
+        return make_opts(kind, knn=kw.get("knn", 8), thresh1=kw.get("thresh", 0.01))
+    if kind == STAGE_NNDISTANCE:
+        return make_opts(kind, knn=kw.get("k", 10), mode={"kth": 0, "avg": 1}[kw.get("mode", "kth")])
+    if kind == STAGE_OPTIMALNEIGHBORHOOD:
+        return make_opts(kind, knn=kw.get("max_k", 14), min_k=kw.get("min_k", 10))
+    if kind == STAGE_LOF:
+        return make_opts(kind, knn=kw.get("minpts", 10))
+    if kind == STAGE_OUTLIER:
+        method = kw.get("method", "statistical")
+        o = make_opts(kind, knn=kw.get("mean_k", 8), min_k=kw.get("min_k", 2),
+                      thresh1=kw.get("multiplier", 2.0), label=kw.get("cls", 7),
+                      mode={"statistical": 0, "radius": 1}[method])
+        o.radius = float(kw.get("radius", 1.0))
+        return o
+    raise ValueError(f"not a consumer stage kind: {kind}")
 
 
 _LIB = None
@@ -288,6 +340,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_filter_report.argtypes = [vp, ctypes.POINTER(RowException), ctypes.c_uint32, i32, cp,
                                       ctypes.c_size_t]
     lib.nbg_filter_report.restype = ctypes.c_int
+    lib.nbg_filter_outcome.argtypes = [vp, ctypes.POINTER(RunStats)]
+    lib.nbg_filter_outcome.restype = ctypes.c_int
     lib.nbg_filter_free.argtypes = [vp]
     lib.nbg_filter_free.restype = None
     lib.nbg_pipeline_parse.argtypes = [cp, ctypes.POINTER(vp), cp, ctypes.c_size_t]

@@ -304,9 +304,14 @@ int grid_grow_table(Context* ctx, Tile* t, uint64_t entries) {
 }
 
 static int ndims_of(const nbg_stage_opts& o) {
-    if (o.kind == NBG_STAGE_NORMAL) return 4;
-    if (o.kind == NBG_STAGE_EIGENVALUES) return 3;
-    return __builtin_popcount(o.feature_mask & NBG_FEAT_ALL);
+    switch (o.kind) {
+        case NBG_STAGE_NORMAL: return 4;
+        case NBG_STAGE_EIGENVALUES: return 3;
+        case NBG_STAGE_COVARIANCEFEATURES: return __builtin_popcount(o.feature_mask & NBG_FEAT_ALL);
+        case NBG_STAGE_OPTIMALNEIGHBORHOOD: return 2;
+        case NBG_STAGE_LOF: return 3;
+        default: return 1;
+    }
 }
 
 }  // namespace nbg
@@ -522,7 +527,7 @@ namespace nbg {
 // Grid for neighbour count k1, or with a fixed cell edge `cell` raw units
 // (radius stages); rebuilt when k1 moves far from the build's or the edge rule
 // changes.
-static int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream, int32_t cell = 0) {
+int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream, int32_t cell) {
     const int32_t fixed = cell ? cell : t->fixed_cell;
     if (t->grid_valid && t->grid_fixed == fixed &&
         (fixed || (k1 <= 2 * t->grid_k1 && 2 * k1 >= t->grid_k1)))
@@ -550,9 +555,27 @@ int validate_stages(Context* ctx, const nbg_stage_opts* stages, int n_stages,
     *need_aux = false;
     for (int s = 0; s < n_stages; ++s) {
         const nbg_stage_opts& o = stages[s];
-        if (o.kind < 1 || o.kind > 3) return fail(ctx, NBG_ERR_INVALID, "unknown stage kind");
+        if (o.kind < 1 || o.kind > NBG_STAGE_OUTLIER)
+            return fail(ctx, NBG_ERR_INVALID, "unknown stage kind");
         if (o.knn < 0 || o.knn > 64)
             return fail(ctx, NBG_ERR_INVALID, "knn must be in [0, 64]");
+        if (o.kind > NBG_STAGE_COVARIANCEFEATURES) {
+            // the other kNN consumers: their own options only
+            if (outputs[s].ndims != ndims_of(o))
+                return fail(ctx, NBG_ERR_INVALID, "output ndims does not match the stage");
+            if ((o.kind == NBG_STAGE_APPROXIMATECOPLANAR || o.kind == NBG_STAGE_ESTIMATERANK) &&
+                o.knn < 1)
+                return fail(ctx, NBG_ERR_UNSUPPORTED,
+                            "knn 0 reads before the search's result buffer in the reference");
+            if (o.kind == NBG_STAGE_OPTIMALNEIGHBORHOOD && (o.min_k < 1 || o.min_k > o.knn))
+                return fail(ctx, NBG_ERR_INVALID, "optimalneighborhood needs 1 <= min_k <= max_k");
+            if ((o.kind == NBG_STAGE_NNDISTANCE && (o.mode < 0 || o.mode > 1)) ||
+                (o.kind == NBG_STAGE_OUTLIER && (o.mode < 0 || o.mode > 2)))
+                return fail(ctx, NBG_ERR_INVALID, "invalid mode");
+            if (o.kind == NBG_STAGE_OUTLIER && o.mode == 1 && !(std::fabs(o.radius) < 1e300))
+                return fail(ctx, NBG_ERR_INVALID, "radius is not a finite number");
+            continue;
+        }
         // a radius makes the reference ignore knn and stride
         // (EigenvaluesFilter.cpp:96-100, CovarianceFeaturesFilter.cpp:216-225)
         const bool by_radius = o.use_radius && !(o.kind == NBG_STAGE_COVARIANCEFEATURES && o.optimized);
@@ -584,6 +607,10 @@ void fill_stage(StageDev& d, const nbg_stage_opts& o, const nbg_columns& c) {
     for (int k = 0; k < 3; ++k) d.viewpoint[k] = o.viewpoint[k];
     d.feature_mask = o.feature_mask & NBG_FEAT_ALL;
     d.mode = o.mode;
+    d.ip = o.min_k;
+    d.t1 = o.thresh1;
+    d.t2 = o.thresh2;
+    d.aux = nullptr;
     d.ndims = c.ndims;
     d.base = (char*)c.base;
     d.point_stride = c.point_stride;
@@ -801,19 +828,28 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     // largest OptimalKNN for optimized stages (their rows then use their own)
     auto stage_k = [&](int s) -> int {
         if (stages[s].optimized) return std::max(1, opt_k);
-        return (int)std::min<uint64_t>(n, (uint64_t)stages[s].knn + 1);
+        // approximatecoplanar / estimaterank query knn points, the point included
+        const int extra = (stages[s].kind == NBG_STAGE_APPROXIMATECOPLANAR ||
+                           stages[s].kind == NBG_STAGE_ESTIMATERANK) ? 0 : 1;
+        return (int)std::min<uint64_t>(n, (uint64_t)stages[s].knn + extra);
     };
     auto by_radius = [&](int s) {
-        return stages[s].use_radius &&
+        return stages[s].use_radius && stages[s].kind <= NBG_STAGE_COVARIANCEFEATURES &&
                !(stages[s].kind == NBG_STAGE_COVARIANCEFEATURES && stages[s].optimized);
     };
     // strided stages (eigenvalues / covariancefeatures; normal has no stride)
     auto strided = [&](int s) {
-        return !by_radius(s) && stages[s].kind != NBG_STAGE_NORMAL && stages[s].stride > 1 &&
-               !stages[s].optimized;
+        return !by_radius(s) && (stages[s].kind == NBG_STAGE_EIGENVALUES ||
+                                 stages[s].kind == NBG_STAGE_COVARIANCEFEATURES) &&
+               stages[s].stride > 1 && !stages[s].optimized;
     };
     std::vector<std::vector<int>> groups;
+    std::vector<int> consumers;  // list / outlier stages: run_consumer
     for (int s = 0; s < n_stages; ++s) {
+        if (is_list_consumer(stages[s].kind)) {
+            consumers.push_back(s);
+            continue;
+        }
         bool placed = false;
         for (auto& gr : groups) {
             // radius and strided stages run alone
@@ -1002,6 +1038,19 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             tree_ms += ms;
         }
     }
+    ConsumerCounts cc;
+    for (int s : consumers) {
+        cudaEventRecord(ctx->ev[1], stream);
+        rc = run_consumer(ctx, t, stages[s], s, dcols[s], sink, stream, &cc);
+        if (rc) { cudaStreamSynchronize(stream); cleanup(); return rc; }
+        cudaEventRecord(ctx->ev[2], stream);
+        cudaStreamSynchronize(stream);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+        query_ms += ms;
+    }
+    tie_rows += cc.tie_rows;
+    replay_rows += cc.replay_rows;
     // results back to host layouts
     if (packed) {
         rc = device_to_host(ctx, outputs[0].base, packed_dev, packed_bytes, stream);
@@ -1039,7 +1088,9 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     cudaStreamSynchronize(stream);
     if (n_exceptions) *n_exceptions = nex;
     if (stats) {
-        stats->points = n * groups.size();
+        stats->points = n * (groups.size() + consumers.size());
+        stats->outliers = cc.outliers;
+        stats->inliers = cc.inliers;
         stats->tie_rows = tie_rows;
         stats->deferred_rows = deferred_rows;
         stats->resolved_rows = nresolve;

@@ -131,6 +131,9 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
         if (need_aux && (!it.optimal_knn || !it.optimal_radius))
             return fail(ctx, NBG_ERR_INVALID, "Density needs OptimalKNN and OptimalRadius");
         for (int s = 0; s < it.n_stages; ++s) {
+            if (it.stages[s].kind > NBG_STAGE_COVARIANCEFEATURES)
+                return fail(ctx, NBG_ERR_UNSUPPORTED,
+                            "the other kNN consumers run through nbg_run, not the batch");
             if (it.stages[s].knn != it.stages[0].knn)
                 return fail(ctx, NBG_ERR_UNSUPPORTED, "the stages of a batch item share one knn");
             if (it.outputs[s].on_device != 1)

@@ -42,10 +42,12 @@ struct StageDev {
     uint32_t feature_mask;
     int32_t mode;
     int32_t ndims;
-    int32_t pad;
+    int32_t ip;       // optimalneighborhood min_k; outlier (radius) min_k
     char* base;
     int64_t point_stride;
     int64_t offset[NBG_MAX_DIMS];
+    double t1, t2;    // approximatecoplanar thresh1/2; estimaterank thresh
+    double* aux;      // outlier (radius): per-row flag, 1 = outlier (device, n)
 };
 
 struct StageGroup {
@@ -56,6 +58,7 @@ struct StageGroup {
     const double* optimal_knn;     // device, may be null
     const double* optimal_radius;  // device, may be null
     uint32_t* resolve_count;       // rows the fast eigensolver handed to the chain (may be null)
+    int32_t no_eigen;              // every stage reads the neighbour count only
 };
 
 // The KD replica's nodes as the tie-order resolver reads them: a child's
@@ -472,6 +475,7 @@ __device__ inline void nbg_finish_row_d(const StageGroup& g, const Transform& tf
     if (nnb == 0) zero = true;
     double ev[3] = {0, 0, 0}, V[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     int ok = 1;
+    if (g.no_eigen) zero = true;
     if (!zero) {
         if (nonfinite) ok = 0;
         else if (g.sign_exact) ok = nbg_eigen_chain(C, ev, V);
@@ -523,6 +527,42 @@ __device__ inline void nbg_finish_row_d(const StageGroup& g, const Transform& tf
             nbg_store(st, id, 1, n1);
             nbg_store(st, id, 2, n2);
             nbg_store(st, id, 3, curv);
+        } else if (st.kind == NBG_STAGE_APPROXIMATECOPLANAR) {
+            // ApproximateCoplanarFilter.cpp:85-113: skipped on a zero
+            // covariance; coplanar when l1 > thresh1*l0 and thresh2*l1 > l2
+            if (zero) { nbg_append_exception(ex, id, sidx, NBG_ROW_ZERO_COV); continue; }
+            if (!ok) { nbg_append_exception(ex, id, sidx, NBG_ROW_EIGEN_FAIL); continue; }
+            nbg_store(st, id, 0, (ev[1] > st.t1 * ev[0] && st.t2 * ev[1] > ev[2]) ? 1.0 : 0.0);
+        } else if (st.kind == NBG_STAGE_ESTIMATERANK) {
+            // MathUtils.cpp:197-208: JacobiSVD rank of the covariance with
+            // the float-cast threshold; singular values of the symmetric
+            // matrix are |lambda|, counted when at or above
+            // max(threshold * sigma_max, DBL_MIN)
+            double a0 = 0, a1 = 0, a2 = 0;
+            bool any = false;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) any = any || C[i] != 0.0;
+            if (nnb <= 1) {
+                // 0/0 covariance: the SVD rejects the non-finite input
+                nbg_store(st, id, 0, 0.0);
+                continue;
+            }
+            if (zero && any) {
+                double e2[3], V2[9];
+                if (nbg_eigen_chain(C, e2, V2)) { a0 = fabs(e2[0]); a1 = fabs(e2[1]); a2 = fabs(e2[2]); }
+            } else if (!zero && ok) {
+                a0 = fabs(ev[0]);
+                a1 = fabs(ev[1]);
+                a2 = fabs(ev[2]);
+            }
+            const double smax = fmax(a0, fmax(a1, a2));
+            const double thr = fmax(smax * (double)(float)st.t1, 2.2250738585072014e-308);
+            nbg_store(st, id, 0, (double)((a0 >= thr) + (a1 >= thr) + (a2 >= thr)));
+        } else if (st.kind == NBG_STAGE_OUTLIER) {
+            // OutlierFilter.cpp:80-96: an inlier has more than size_t(min_k)
+            // points (itself included) within the radius; a negative min_k
+            // converts to a count no row exceeds
+            st.aux[id] = (st.ip >= 0 && nnb > st.ip) ? 0.0 : 1.0;
         } else if (st.kind == NBG_STAGE_EIGENVALUES) {
             if (zero) { nbg_append_exception(ex, id, sidx, NBG_ROW_ZERO_COV); continue; }
             if (!ok) { nbg_append_exception(ex, id, sidx, NBG_ROW_EIGEN_FAIL); continue; }

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "nbg_common.cuh"
+#include "nbg_consumers.cuh"
 
 struct nbg_tile;
 
@@ -110,6 +111,8 @@ struct Tile {
 };
 
 int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream);
+// Grid for neighbour count k1 (or a fixed cell edge), rebuilt only when needed.
+int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream, int32_t cell = 0);
 int build_grid_async(Context* ctx, Tile* t, int k1, cudaStream_t stream);
 int fail(Context* c, int code, const std::string& msg);
 int validate_stages(Context* ctx, const nbg_stage_opts* stages, int n_stages,
@@ -174,8 +177,14 @@ int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const Excep
                 const double* row_k = nullptr, int stride = 1, int kpick = 0);
 // Strided neighbourhoods of one stage over every row (K = k * stride);
 // needs the tile's KD replica.
+// With `list`, the ordered list of K entries goes to that kNN consumer's
+// epilogue instead (stride 1, kpick K).
 int launch_stride(Context* ctx, const QueryLaunch& q, int stride, int kpick, const KdOrder& kd,
-                  cudaStream_t stream);
+                  cudaStream_t stream, const ListArgs* list = nullptr);
+// Search replay of the listed rows for a kNN consumer (the replica's own
+// list order is the reference's).
+int kd_list_rows(Context* ctx, Tile* t, int K, const ListArgs& L, const ExceptionSink& ex,
+                 const uint32_t* rows, uint32_t nrows, cudaStream_t stream);
 int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_t nrows,
                      uint32_t* ids_out, cudaStream_t stream);
 KdOrder kd_order(const Tile* t);
@@ -200,6 +209,16 @@ int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, i
 int tile_alloc(Context* ctx, uint64_t n, const double scale[3], const double offset[3],
                nbg_tile** out);
 void tile_destroy(Context* ctx, nbg_tile* th);
+
+// kNN-consumer stages (nndistance, optimalneighborhood, lof, outlier) of one
+// nbg_run call (nbg_consumers.cu); outlier counts accumulate into `stats`.
+struct ConsumerCounts {
+    uint64_t outliers = 0, inliers = 0, tie_rows = 0, replay_rows = 0;
+};
+int run_consumer(Context* ctx, Tile* t, const nbg_stage_opts& o, int stage_index,
+                 const nbg_columns& col, const ExceptionSink& sink, cudaStream_t stream,
+                 ConsumerCounts* counts);
+bool is_list_consumer(int kind);
 
 // Batched form: the context's batch scratch and cached graph (nbg_batch.cu).
 void batch_release(Context* ctx);

@@ -935,6 +935,36 @@ __global__ void kd_finish_kernel(Transform tf, const int32_t* __restrict__ x,
     nbg_finish_row(g, tf, ex, id, cnt, M, qraw);
 }
 
+// A kNN consumer's epilogue over replayed lists (already in the reference's
+// order: the replay is its search).
+__global__ void kd_list_finish_kernel(Transform tf, const int32_t* __restrict__ x,
+                                      const int32_t* __restrict__ y, const int32_t* __restrict__ z,
+                                      const uint32_t* __restrict__ rows, uint32_t nrows, int K,
+                                      const uint32_t* __restrict__ nbr,
+                                      const uint32_t* __restrict__ counts, ListArgs L,
+                                      ExceptionSink ex) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    const uint32_t id = rows[r];
+    const int32_t qraw[3] = {x[id], y[id], z[id]};
+    const double q64[3] = {ref_coord(qraw[0], tf.scale[0], tf.offset[0]),
+                           ref_coord(qraw[1], tf.scale[1], tf.offset[1]),
+                           ref_coord(qraw[2], tf.scale[2], tf.offset[2])};
+    const int cnt = min((int)counts[r], K);
+    uint32_t ids[KD_CAP];
+    int off[KD_CAP][3];
+    double d[KD_CAP];
+    for (int j = 0; j < cnt; ++j) {
+        const uint32_t p = nbr[(uint64_t)r * K + j];
+        ids[j] = p;
+        off[j][0] = x[p] - qraw[0];
+        off[j][1] = y[p] - qraw[1];
+        off[j][2] = z[p] - qraw[2];
+        d[j] = ref_dist2(q64, qraw, off[j], tf);
+    }
+    list_consume(L, tf, ex, id, qraw, cnt, ids, off, d);
+}
+
 // Neighbour-set export: ascending ids into ids_out[id*K ...].
 __global__ void kd_scatter_ids_kernel(const uint32_t* __restrict__ rows, uint32_t nrows, int K,
                                       const uint32_t* __restrict__ nbr,
@@ -1442,6 +1472,27 @@ int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const Excep
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
             ctx->err = std::string("exact KD finish: ") + cudaGetErrorString(e);
+            rc = NBG_ERR_CUDA;
+        }
+    }
+    if (nbr) ctx_free(ctx, nbr, (size_t)nrows * K * 4);
+    if (counts) ctx_free(ctx, counts, (size_t)nrows * 4);
+    return rc;
+}
+
+int kd_list_rows(Context* ctx, Tile* t, int K, const ListArgs& L, const ExceptionSink& ex,
+                 const uint32_t* rows, uint32_t nrows, cudaStream_t st) {
+    if (!nrows) return NBG_OK;
+    uint32_t *nbr = nullptr, *counts = nullptr;
+    int rc = kd_search_rows(ctx, t, K, rows, nrows, &nbr, &counts, st);
+    if (!rc) {
+        kd_list_finish_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(t->tf, t->x, t->y, t->z, rows,
+                                                                   nrows, K, nbr, counts, L, ex);
+        NBG_LAUNCHED(1);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            ctx->err = std::string("exact KD list: ") + cudaGetErrorString(e);
             rc = NBG_ERR_CUDA;
         }
     }

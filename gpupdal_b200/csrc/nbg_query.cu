@@ -786,19 +786,9 @@ struct StrideArgs {
     int32_t stride;
     int32_t kpick;     // k: entries kept
     KdOrder kd;
+    int32_t consumer;  // 1: the ordered list goes to a kNN consumer (L), not a covariance
+    ListArgs L;
 };
-
-__device__ __forceinline__ double ref_dist2(const double q64[3], const int32_t qraw[3],
-                                            const int o[3], const Transform& tf) {
-    double acc = 0.0;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const double pc = ref_coord(qraw[d] + o[d], tf.scale[d], tf.offset[d]);
-        const double df = __dsub_rn(q64[d], pc);
-        acc = __dadd_rn(acc, __dmul_rn(df, df));
-    }
-    return acc;
-}
 
 template <int KS>
 __global__ void __launch_bounds__(128) knn_stride_kernel(const StrideArgs sa) {
@@ -885,6 +875,10 @@ __global__ void __launch_bounds__(128) knn_stride_kernel(const StrideArgs sa) {
         f.off[u + 1][0] = o0;
         f.off[u + 1][1] = o1;
         f.off[u + 1][2] = o2;
+    }
+    if (sa.consumer) {
+        list_consume(sa.L, a.tf, a.ex, rid, qraw, K, f.id, f.off, d);
+        return;
     }
     long long s1[3] = {0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
     for (int j = 0; j < sa.kpick; ++j) {
@@ -1226,9 +1220,13 @@ struct StrideLauncher {
 };
 
 int launch_stride(Context* ctx, const QueryLaunch& ql, int stride, int kpick, const KdOrder& kd,
-                  cudaStream_t stream) {
+                  cudaStream_t stream, const ListArgs* list) {
     (void)ctx;
     StrideLaunchArgs l{};
+    if (list) {
+        l.s.consumer = 1;
+        l.s.L = *list;
+    }
     QueryArgs& q = l.s.q;
     q.gv = grid_view(ql.tile);
     q.gp = ql.tile->gp;

@@ -1,6 +1,8 @@
 // nbg_stages.cpp — the stage layer above the C ABI: PDAL pipeline JSON and
 // the options, dimensions, checks and per-row messages of filters.normal,
-// filters.eigenvalues and filters.covariancefeatures.
+// filters.eigenvalues and filters.covariancefeatures, and of the other
+// consumers of the same index (filters.approximatecoplanar, estimaterank,
+// nndistance, optimalneighborhood, lof, outlier).
 //
 // Mirrors, for a drop-in of an existing pipeline:
 //   NormalFilter::addArgs/addDimensions/prepared      filters/NormalFilter.cpp:85-138
@@ -498,9 +500,106 @@ extern "C" int nbg_filter_create(const char* type, const char* options_json, int
                                "which are missing in the input PointView."};
             if (s.optimized && !has_optimal_knn)
                 throw ArgError{"Missing OptimalKNN dimension in input PointView."};
+        } else if (t == "filters.approximatecoplanar") {
+            // ApproximateCoplanarFilter.cpp:66-77
+            allowed = {"knn", "thresh1", "thresh2"};
+            s.kind = NBG_STAGE_APPROXIMATECOPLANAR;
+            s.knn = 8;
+            s.thresh1 = 25.0;
+            s.thresh2 = 6.0;
+            if (has("knn")) s.knn = (int32_t)arg_int(*o.get("knn"), "knn");
+            if (has("thresh1")) s.thresh1 = arg_double(*o.get("thresh1"), "thresh1");
+            if (has("thresh2")) s.thresh2 = arg_double(*o.get("thresh2"), "thresh2");
+            f->dims = {"Coplanar"};
+        } else if (t == "filters.estimaterank") {
+            // EstimateRankFilter.cpp:66-74
+            allowed = {"knn", "thresh"};
+            s.kind = NBG_STAGE_ESTIMATERANK;
+            s.knn = 8;
+            s.thresh1 = 0.01;
+            if (has("knn")) s.knn = (int32_t)arg_int(*o.get("knn"), "knn");
+            if (has("thresh")) s.thresh1 = arg_double(*o.get("thresh"), "thresh");
+            f->dims = {"Rank"};
+        } else if (t == "filters.nndistance") {
+            // NNDistanceFilter.cpp:66-105: mode kth / avg, case-insensitive
+            allowed = {"mode", "k"};
+            s.kind = NBG_STAGE_NNDISTANCE;
+            s.knn = 10;
+            s.mode = 0;
+            if (has("k")) {
+                const int64_t k = arg_int(*o.get("k"), "k");
+                if (k < 0) throw ArgError{"Invalid value '" + raw_text(*o.get("k")) + "' for argument 'k'."};
+                s.knn = (int32_t)std::min<int64_t>(k, INT32_MAX);
+            }
+            if (has("mode")) {
+                const std::string m = lower(trim(raw_text(*o.get("mode"))));
+                if (m == "kth") s.mode = 0;
+                else if (m == "avg") s.mode = 1;
+                else throw ArgError{"Invalid value '" + raw_text(*o.get("mode")) +
+                                    "' for argument 'mode'."};
+            }
+            f->dims = {"NNDistance"};
+        } else if (t == "filters.optimalneighborhood") {
+            // OptimalNeighborhoodFilter.cpp:62-71
+            allowed = {"min_k", "max_k"};
+            s.kind = NBG_STAGE_OPTIMALNEIGHBORHOOD;
+            int64_t kmin = 10, kmax = 14;
+            if (has("min_k")) kmin = arg_int(*o.get("min_k"), "min_k");
+            if (has("max_k")) kmax = arg_int(*o.get("max_k"), "max_k");
+            if (kmin < 0) throw ArgError{"Invalid value '" + std::to_string(kmin) + "' for argument 'min_k'."};
+            if (kmax < 0) throw ArgError{"Invalid value '" + std::to_string(kmax) + "' for argument 'max_k'."};
+            s.knn = (int32_t)std::min<int64_t>(kmax, INT32_MAX);
+            f->min_k = kmin;
+            f->dims = {"OptimalKNN", "OptimalRadius"};
+        } else if (t == "filters.lof") {
+            // LOFFilter.cpp:62-70
+            allowed = {"minpts"};
+            s.kind = NBG_STAGE_LOF;
+            s.knn = 10;
+            if (has("minpts")) {
+                const int64_t k = arg_int(*o.get("minpts"), "minpts");
+                if (k < 0) throw ArgError{"Invalid value '" + raw_text(*o.get("minpts")) +
+                                          "' for argument 'minpts'."};
+                s.knn = (int32_t)std::min<int64_t>(k, INT32_MAX);
+            }
+            f->dims = {"NNDistance", "LocalReachabilityDistance", "LocalOutlierFactor"};
+        } else if (t == "filters.outlier") {
+            // OutlierFilter.cpp:62-76, 171-189: an unrecognised method leaves
+            // the view unchanged with a warning
+            allowed = {"method", "min_k", "radius", "mean_k", "multiplier", "class"};
+            s.kind = NBG_STAGE_OUTLIER;
+            s.knn = 8;
+            s.thresh1 = 2.0;
+            s.radius = 1.0;
+            s.label = 7;  // ClassLabel::LowPoint
+            f->min_k = 2;
+            std::string method = "statistical";
+            if (has("method")) method = raw_text(*o.get("method"));
+            if (has("min_k")) f->min_k = arg_int(*o.get("min_k"), "min_k");
+            if (has("radius")) s.radius = arg_double(*o.get("radius"), "radius");
+            if (has("mean_k")) s.knn = (int32_t)arg_int(*o.get("mean_k"), "mean_k");
+            if (has("multiplier")) s.thresh1 = arg_double(*o.get("multiplier"), "multiplier");
+            if (has("class")) {
+                const int64_t c = arg_int(*o.get("class"), "class");
+                if (c < 0 || c > 255) throw ArgError{"Invalid value '" + raw_text(*o.get("class")) +
+                                                     "' for argument 'class'."};
+                s.label = (int32_t)c;
+            }
+            const std::string m = lower(method);
+            if (m == "statistical") s.mode = 0;
+            else if (m == "radius") s.mode = 1;
+            else {
+                s.mode = 2;
+                f->log += "Requested method is unrecognized. Please choose from \"statistical\" or "
+                          "\"radius\".\n";
+            }
+            f->dims = {"Classification"};
         } else {
             copy_err(err, err_len, "unknown stage type '" + t + "' (this library runs "
-                                   "filters.normal, filters.eigenvalues, filters.covariancefeatures)");
+                                   "filters.normal, filters.eigenvalues, filters.covariancefeatures, "
+                                   "filters.approximatecoplanar, filters.estimaterank, "
+                                   "filters.nndistance, filters.optimalneighborhood, filters.lof, "
+                                   "filters.outlier)");
             return NBG_ERR_INVALID;
         }
         for (auto& kv : o.obj) {
@@ -508,7 +607,8 @@ extern "C" int nbg_filter_create(const char* type, const char* options_json, int
             if (std::find(allowed.begin(), allowed.end(), kv.first) == allowed.end())
                 throw ArgError{"Unexpected argument '" + kv.first + "'."};
         }
-        if (s.knn < 0) throw ArgError{"Invalid value '" + std::to_string(s.knn) + "' for argument 'knn'."};
+        if (s.knn < 0 && s.kind != NBG_STAGE_OUTLIER)
+            throw ArgError{"Invalid value '" + std::to_string(s.knn) + "' for argument 'knn'."};
     } catch (const ArgError& e) {
         copy_err(err, err_len, t + ": " + e.msg);
         return NBG_ERR_INVALID;
@@ -520,6 +620,11 @@ extern "C" int nbg_filter_create(const char* type, const char* options_json, int
 extern "C" int nbg_filter_options(const nbg_filter* f, nbg_stage_opts* out) {
     if (!f || !out) return NBG_ERR_INVALID;
     *out = f->opts;
+    if (f->opts.kind > NBG_STAGE_COVARIANCEFEATURES) {
+        // the other consumers keep their own min_k (outlier's may be negative)
+        out->min_k = (int32_t)std::max<int64_t>(INT32_MIN, std::min<int64_t>(f->min_k, INT32_MAX));
+        return NBG_OK;
+    }
     if (f->radius_set) {
         out->use_radius = 1;
         out->radius = f->radius;
@@ -585,6 +690,19 @@ extern "C" int nbg_filter_report(nbg_filter* f, const nbg_row_exception* ex, uin
                               : "Cannot perform eigen decomposition.";
         copy_err(err, err_len, f->type + ": " + msg);
         return NBG_ERR_INVALID;
+    }
+    return NBG_OK;
+}
+
+extern "C" int nbg_filter_outcome(nbg_filter* f, const nbg_run_stats* stats) {
+    if (!f || !stats) return NBG_ERR_INVALID;
+    // OutlierFilter.cpp:191-226
+    if (f->opts.kind == NBG_STAGE_OUTLIER && f->opts.mode != 2 && stats->outliers + stats->inliers) {
+        if (!stats->inliers)
+            f->log += "Requested filter would remove all points. Try a larger radius/smaller "
+                      "minimum neighbors.\n";
+        else if (!stats->outliers)
+            f->log += "Filtered cloud has no outliers!\n";
     }
     return NBG_OK;
 }

@@ -5,8 +5,8 @@ path's stages of an existing pipeline JSON on one tile.
     dims, log = run_pipeline(ctx, pipeline_json, x, y, z)
 
 `dims` maps each registered dimension name (NormalX, Eigenvalue0, Linearity,
-...) to a float64 array in point order; rows a stage skips hold 0, as in a
-freshly added PDAL dimension.  `log` holds the lines the stages logged.  A
+Coplanar, NNDistance, OptimalKNN, ...) to a float64 array in point order;
+rows a stage skips hold 0, as in a freshly added PDAL dimension.  `log` holds the lines the stages logged.  A
 check or row the reference throws on raises StageError with its message.
 Stages outside this path (readers, writers, other filters) are not run;
 their types are returned in `log` as "not run: <type>"."""
@@ -19,7 +19,9 @@ import numpy as np
 
 from . import abi
 
-PATH_STAGES = ("filters.normal", "filters.eigenvalues", "filters.covariancefeatures")
+PATH_STAGES = ("filters.normal", "filters.eigenvalues", "filters.covariancefeatures",
+               "filters.approximatecoplanar", "filters.estimaterank", "filters.nndistance",
+               "filters.optimalneighborhood", "filters.lof", "filters.outlier")
 
 
 class StageError(RuntimeError):
@@ -64,6 +66,10 @@ class Filter:
         if rc != abi.NBG_OK:
             raise StageError(err.value.decode())
 
+    def outcome(self, stats):
+        """filters.outlier's warnings for a run's counts (appended to the log)."""
+        self.lib.nbg_filter_outcome(self.h, ctypes.byref(stats))
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.nbg_filter_free(self.h)
@@ -107,12 +113,19 @@ def run_pipeline(ctx, pipeline, x, y, z, scale=(0.01, 0.01, 0.01), offset=(0.0, 
             f = Filter(stype, opts, optimal_knn is not None, optimal_radius is not None)
             o, rc = f.options()
             if rc != abi.NBG_OK:
-                raise StageError(f"{stype}: radius, stride > 1 and optimized are not supported "
+                raise StageError(f"{stype}: stride * (knn + 1) above 65 is not supported "
                                  "by this library")
-            outs, ex, _ = ctx.run(tile, [o], optimal_knn=optimal_knn, optimal_radius=optimal_radius)
+            outs, ex, stats = ctx.run(tile, [o], optimal_knn=optimal_knn,
+                                      optimal_radius=optimal_radius)
             f.report(ex, 0)
+            f.outcome(stats)
             for name, col in zip(f.dims(), outs[0]):
                 dims[name] = col
+            # filters.optimalneighborhood's dimensions feed later stages
+            # (covariancefeatures optimized / Density)
+            if "OptimalKNN" in dims:
+                optimal_knn = np.ascontiguousarray(dims["OptimalKNN"])
+                optimal_radius = np.ascontiguousarray(dims["OptimalRadius"])
             log += [f"({stype}) {l}" for l in f.log()]
             f.close()
     finally:

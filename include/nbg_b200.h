@@ -52,6 +52,31 @@ extern "C" {
 #define NBG_STAGE_NORMAL 1             /* NormalX, NormalY, NormalZ, Curvature */
 #define NBG_STAGE_EIGENVALUES 2        /* Eigenvalue0, Eigenvalue1, Eigenvalue2 */
 #define NBG_STAGE_COVARIANCEFEATURES 3 /* selected features, bit order below */
+/* Other consumers of the same kNN index (the K each queries is noted; the
+ * reference's knnSearch pads a list longer than the cloud with point 0 at
+ * squared distance 0, and these stages keep that):
+ *   approximatecoplanar  Coplanar (0/1); K = knn, thresh1, thresh2
+ *                        (ApproximateCoplanarFilter.cpp:66-114)
+ *   estimaterank         Rank (0-3); K = knn, thresh1 = thresh
+ *                        (EstimateRankFilter.cpp:66-84, MathUtils.cpp:197-208)
+ *   nndistance           NNDistance; K = knn + 1 (knn = k), mode 0 kth / 1 avg
+ *                        (NNDistanceFilter.cpp:108-138)
+ *   optimalneighborhood  OptimalKNN, OptimalRadius; K = knn (= max_k), min_k
+ *                        (OptimalNeighborhoodFilter.cpp:71-163)
+ *   lof                  NNDistance, LocalReachabilityDistance,
+ *                        LocalOutlierFactor; K = knn + 1 (knn = minpts)
+ *                        (LOFFilter.cpp:66-139)
+ *   outlier              Classification, written only on outlier rows and
+ *                        only when some row is an inlier; mode 0 statistical
+ *                        (K = knn + 1, knn = mean_k, thresh1 = multiplier) or
+ *                        mode 1 radius (radius, min_k); label = class
+ *                        (OutlierFilter.cpp:75-229) */
+#define NBG_STAGE_APPROXIMATECOPLANAR 4
+#define NBG_STAGE_ESTIMATERANK 5
+#define NBG_STAGE_NNDISTANCE 6
+#define NBG_STAGE_OPTIMALNEIGHBORHOOD 7
+#define NBG_STAGE_LOF 8
+#define NBG_STAGE_OUTLIER 9
 
 /* covariance feature bits, in the order of feature_set "all"
  * (CovarianceFeaturesFilter.cpp:127-133) */
@@ -101,15 +126,24 @@ typedef struct nbg_stage_opts {
                               copy of the normal)                            */
     int32_t normalize;     /* eigenvalues: divide by their sum               */
     uint32_t feature_mask; /* covariancefeatures: NBG_FEAT_* bits            */
-    int32_t mode;          /* covariancefeatures: NBG_MODE_*                 */
+    int32_t mode;          /* covariancefeatures: NBG_MODE_*; nndistance: 0 kth,
+                              1 avg; outlier: 0 statistical, 1 radius,
+                              2 unrecognised method (the stage is a no-op)   */
     int32_t stride;        /* keep every stride-th of knn*stride neighbours  */
     int32_t optimized;     /* covariancefeatures: per-point k = OptimalKNN   */
     int32_t use_radius;    /* neighbours = the points within `radius` (squared
                               FP64 distance < radius*radius) instead of knn
                               (KDImpl.hpp:398-415)                           */
     int32_t min_k;         /* eigenvalues/covariancefeatures with a radius:
-                              rows with fewer neighbours are skipped         */
+                              rows with fewer neighbours are skipped;
+                              optimalneighborhood: smallest k; outlier
+                              (radius): inliers have more than min_k         */
     double radius;
+    double thresh1;        /* approximatecoplanar thresh1, estimaterank
+                              thresh, outlier multiplier                     */
+    double thresh2;        /* approximatecoplanar thresh2                    */
+    int32_t label;         /* outlier: class written to outlier rows         */
+    int32_t reserved0;
 } nbg_stage_opts;
 
 /* Output placement: dimension d of point id is the double at
@@ -153,6 +187,9 @@ typedef struct nbg_run_stats {
                                  (deferred rows, tie groups over 32 points)     */
     double kd_build_ms;       /* device time of the KD replica build on the side
                                  stream, overlapped with the query kernel       */
+    uint64_t outliers;        /* outlier stages: rows found to be outliers
+                                 (written only when inliers remain)             */
+    uint64_t inliers;         /* outlier stages: rows found to be inliers       */
 } nbg_run_stats;
 
 typedef struct nbg_context nbg_context;
@@ -247,7 +284,8 @@ int nbg_tile_upload_las(nbg_context* ctx, const void* records, uint64_t n,
  * PDAL pipeline JSON and the stage logic above nbg_run, so an existing
  * pipeline is a drop-in.  nbg_filter_create parses one stage's options
  * object as ProgramArgs would (NormalFilter.cpp:85-97, EigenvaluesFilter.cpp:
- * 77-87, CovarianceFeaturesFilter.cpp:102-113; value errors as ProgramArgs.hpp:
+ * 77-87, CovarianceFeaturesFilter.cpp:102-113, and the other consumers' addArgs
+ * listed with their stage kinds above; value errors as ProgramArgs.hpp:
  * 415-435), registers its dimensions (addDimensions) and runs prepared()'s
  * checks; has_optimal_knn / has_optimal_radius say whether the input view
  * carries those dimensions.  A check the reference throws from returns
@@ -268,6 +306,10 @@ const char* nbg_filter_log(const nbg_filter* filter);
  * or NBG_ERR_INVALID with the text its loop would throw. */
 int nbg_filter_report(nbg_filter* filter, const nbg_row_exception* exceptions, uint32_t n,
                       int32_t stage_index, char* err, size_t err_len);
+/* filters.outlier's warnings after a run (OutlierFilter.cpp:191-226):
+ * "would remove all points" when no row is an inlier, "no outliers" when no
+ * row is an outlier; appended to the log.  No-op for the other stages. */
+int nbg_filter_outcome(nbg_filter* filter, const nbg_run_stats* stats);
 void nbg_filter_free(nbg_filter* filter);
 
 /* A pipeline JSON (an array of stages, or {"pipeline": [...]}): its stages'

@@ -40,6 +40,7 @@
 // contraction, and every distance must round exactly as it does there.
 
 #include "../include/nbg_b200.h"
+#include "consumers.hpp"
 
 #include <algorithm>
 #include <cfloat>
@@ -307,6 +308,29 @@ public:
                              return a.second < b.second;
                          });
         for (auto& f : rs.found) out.push_back(f.first);
+    }
+
+    // KD3ImplT::knnSearch (KDImpl.hpp:383-396): min(n, k) entries of the
+    // caller's k-sized vectors filled in the search's order
+    void knn_search(const double q[3], uint64_t k, std::vector<uint64_t>& ids,
+                    std::vector<double>& d2) const {
+        Result rs;
+        rs.cap = std::min<uint64_t>(n, k);
+        if (rs.cap == 0) return;
+        rs.init(ids.data(), d2.data());
+        double dists[3] = {0, 0, 0};
+        double distsq = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            if (q[i] < root_lo[i]) {
+                dists[i] = (q[i] - root_lo[i]) * (q[i] - root_lo[i]);
+                distsq += dists[i];
+            }
+            if (q[i] > root_hi[i]) {
+                dists[i] = (q[i] - root_hi[i]) * (q[i] - root_hi[i]);
+                distsq += dists[i];
+            }
+        }
+        search_level(rs, q, 0, distsq, dists);
     }
 
     // KD3ImplT::neighbors(x, y, z, k, stride): returns the id list
@@ -763,6 +787,55 @@ struct OrcTree {
     std::vector<double> X, Y, Z;
 };
 
+// The port's backend of the shared consumer loops (consumers.hpp).
+struct PortBackend {
+    const OrcTree* h;
+    uint64_t n() const { return h->t.n; }
+    double coord(uint64_t i, int d) const { return d == 0 ? h->X[i] : d == 1 ? h->Y[i] : h->Z[i]; }
+    void knn(uint64_t i, uint64_t k, std::vector<uint64_t>& ids, std::vector<double>& d2) const {
+        const double q[3] = {h->X[i], h->Y[i], h->Z[i]};
+        h->t.knn_search(q, k, ids, d2);
+    }
+    std::vector<uint64_t> neighbors(uint64_t i, uint64_t k) const {
+        const double q[3] = {h->X[i], h->Y[i], h->Z[i]};
+        std::vector<uint64_t> ids;
+        h->t.neighbors(q, k, 1, ids);
+        return ids;
+    }
+    uint64_t radius_count(uint64_t i, double r) const {
+        const double q[3] = {h->X[i], h->Y[i], h->Z[i]};
+        std::vector<uint64_t> ids;
+        h->t.radius_neighbors(q, r, ids);
+        return ids.size();
+    }
+    int cov_eigenvalues(const std::vector<uint64_t>& ids, int mode, double ev[3]) const {
+        const double* X[3] = {h->X.data(), h->Y.data(), h->Z.data()};
+        orc::Eig e = orc::eigensystem(X, ids, mode);
+        if (e.zero) return NBG_ROW_ZERO_COV;
+        if (!e.ok) return NBG_ROW_EIGEN_FAIL;
+        for (int c = 0; c < 3; ++c) ev[c] = e.ev[c];
+        return 0;
+    }
+    // JacobiSVD rank (MathUtils.cpp:197-208): singular values of the
+    // symmetric covariance are |lambda|, counted when at or above
+    // max(float(thresh) * sigma_max, DBL_MIN).  A one-point neighbourhood
+    // (0/0 covariance) has no defined rank in the reference; 0 here.
+    int rank(const std::vector<uint64_t>& ids, double thresh, int mode) const {
+        if (ids.size() <= 1) return 0;
+        const double* X[3] = {h->X.data(), h->Y.data(), h->Z.data()};
+        orc::Eig e = orc::eigensystem(X, ids, mode);
+        if (e.zero || !e.ok) return 0;
+        double a[3] = {std::fabs(e.ev[0]), std::fabs(e.ev[1]), std::fabs(e.ev[2])};
+        double smax = std::max(a[0], std::max(a[1], a[2]));
+        double thr = std::max(smax * (double)(float)thresh, std::numeric_limits<double>::min());
+        return (a[0] >= thr) + (a[1] >= thr) + (a[2] >= thr);
+    }
+    bool sym_eigenvalues(const double A[3][3], double ev[3]) const {
+        double vec[9];
+        return orc::eigen_chain(A, ev, vec) != 0;
+    }
+};
+
 extern "C" {
 
 const char* orc_impl_name(void) { return "port"; }
@@ -847,6 +920,11 @@ int orc_run_stage(void* hv, const nbg_stage_opts* opts, const double* optimal_kn
     const uint64_t n = h->t.n;
     const int nd = orc::ndims_of(o);
     const double* X[3] = {h->X.data(), h->Y.data(), h->Z.data()};
+    if (o.kind > NBG_STAGE_COVARIANCEFEATURES)
+        return orc_consumers::run_consumer(PortBackend{h}, o, mode, out_cols, status, threads,
+                                           [](uint64_t m, int th, auto&& fn) {
+                                               orc::parallel_rows(m, th, fn);
+                                           });
     if (o.kind < 1 || o.kind > 3) return -1;
     orc::parallel_rows(n, threads, [&](uint64_t b, uint64_t e) {
         std::vector<uint64_t> ids;

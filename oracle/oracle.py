@@ -122,10 +122,12 @@ class Tree:
                   ndims=None):
         """Per-point loop of one stage; returns (outputs[ndims, n], status[n]).
 
-        Rows the reference skips keep NaN in `outputs`."""
-        from gpupdal_b200.abi import stage_dims
+        Rows the reference skips keep NaN in `outputs`; an outlier stage's
+        Classification starts at 0 (a fresh dimension) and the number of
+        outliers found is left in `self.outliers`."""
+        from gpupdal_b200.abi import STAGE_OUTLIER, stage_dims
         nd = ndims if ndims is not None else len(stage_dims(opts))
-        outs = np.full((max(nd, 1), self.n), np.nan)
+        outs = np.full((max(nd, 1), self.n), 0.0 if opts.kind == STAGE_OUTLIER else np.nan)
         status = np.zeros(self.n, dtype=np.uint8)
         dp = ctypes.POINTER(ctypes.c_double)
         cols = (dp * max(nd, 1))(*[outs[i].ctypes.data_as(dp) for i in range(max(nd, 1))])
@@ -137,6 +139,8 @@ class Tree:
             ropt.ctypes.data_as(dp) if ropt is not None else None,
             int(mode), cols, status.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
             int(threads or os.cpu_count() or 1))
-        if rc != 0:
+        if opts.kind == STAGE_OUTLIER and rc >= 0:
+            self.outliers = rc
+        elif rc != 0:
             raise RuntimeError(f"orc_run_stage failed ({rc})")
         return outs[:nd], status

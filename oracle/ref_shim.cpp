@@ -11,6 +11,9 @@
 //   filters/NormalFilter.cpp:140-182
 //   filters/EigenvaluesFilter.cpp:115-172
 //   filters/CovarianceFeaturesFilter.cpp:204-367
+// and, through consumers.hpp, the other consumers of the same index
+// (approximatecoplanar, estimaterank, nndistance, optimalneighborhood, lof,
+// outlier).
 // The result is the reference's CPU path without the PDAL framework (which
 // needs GDAL and does not build here).  Output goes to oracle/_ref/ only.
 
@@ -27,6 +30,7 @@
 #include <vector>
 
 #include "../include/nbg_b200.h"
+#include "consumers.hpp"
 
 namespace {
 
@@ -83,6 +87,17 @@ struct RefTree {
         const std::size_t count = index.radiusSearch(&pt[0], r * r, ret_matches, params);
         for (std::size_t i = 0; i < count; ++i) output.push_back(ret_matches[i].first);
         return output;
+    }
+
+    // KD3ImplT::knnSearch (KDImpl.hpp:383-396): the caller's k-sized
+    // vectors, min(n, k) entries filled
+    void knn_search(double x, double y, double z, uint64_t k, PointIdList* indices,
+                    std::vector<double>* sqr_dists) const {
+        k = (std::min<uint64_t>)(cloud.pts.size(), k);
+        nanoflann::KNNResultSet<double, PointId, uint64_t> resultSet(k);
+        resultSet.init(&indices->front(), &sqr_dists->front());
+        std::vector<double> pt{x, y, z};
+        index.findNeighbors(resultSet, &pt[0], nanoflann::SearchParams(10));
     }
 
     PointIdList neighbors(double x, double y, double z, uint64_t k, size_t stride) const {
@@ -265,6 +280,52 @@ int stage_row(const nbg_stage_opts& o, const RefTree& t, uint64_t i, const doubl
     return 0;
 }
 
+// The reference's backend of the shared consumer loops (consumers.hpp):
+// its nanoflann search, its computeCovariance, Eigen's solver and JacobiSVD.
+struct RefBackend {
+    const RefTree* t;
+    uint64_t n() const { return t->cloud.pts.size(); }
+    double coord(uint64_t i, int d) const { return t->cloud.pts[i][d]; }
+    void knn(uint64_t i, uint64_t k, PointIdList& ids, std::vector<double>& d2) const {
+        const auto& p = t->cloud.pts[i];
+        t->knn_search(p[0], p[1], p[2], k, &ids, &d2);
+    }
+    PointIdList neighbors(uint64_t i, uint64_t k) const {
+        const auto& p = t->cloud.pts[i];
+        return t->neighbors(p[0], p[1], p[2], k, 1);
+    }
+    uint64_t radius_count(uint64_t i, double r) const {
+        const auto& p = t->cloud.pts[i];
+        return t->radius(p[0], p[1], p[2], r).size();
+    }
+    int cov_eigenvalues(const PointIdList& ids, int, double ev[3]) const {
+        Eigen::Matrix3d B = covariance(t->cloud, ids);
+        if (B.isZero()) return NBG_ROW_ZERO_COV;
+        Eigen::SelfAdjointEigenSolver<Eigen::Matrix3d> solver(B);
+        if (solver.info() != Eigen::Success) return NBG_ROW_EIGEN_FAIL;
+        for (int c = 0; c < 3; ++c) ev[c] = solver.eigenvalues()[c];
+        return 0;
+    }
+    // MathUtils.cpp:197-208.  A one-point neighbourhood gives a 0/0 matrix
+    // whose JacobiSVD rank reads an unset count; 0 is returned for it.
+    int rank(const PointIdList& ids, double thresh, int) const {
+        if (ids.size() <= 1) return 0;
+        Eigen::Matrix3d B = covariance(t->cloud, ids);
+        Eigen::JacobiSVD<Eigen::Matrix3d> svd(B);
+        svd.setThreshold((float)thresh);
+        return (int)svd.rank();
+    }
+    bool sym_eigenvalues(const double A[3][3], double ev[3]) const {
+        Eigen::Matrix3d M;
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) M(r, c) = A[r][c];
+        Eigen::SelfAdjointEigenSolver<Eigen::Matrix3d> solver(M);
+        if (solver.info() != Eigen::Success) return false;
+        for (int c = 0; c < 3; ++c) ev[c] = solver.eigenvalues()[c];
+        return true;
+    }
+};
+
 template <class F>
 void parallel_rows(uint64_t n, int threads, F&& fn) {
     if (threads <= 1 || n < 1024) {
@@ -346,6 +407,9 @@ int orc_run_stage(void* hv, const nbg_stage_opts* opts, const double* optimal_kn
     if (mode != 0) return -2;  // the reference has only its own arithmetic
     RefTree* t = (RefTree*)hv;
     const nbg_stage_opts o = *opts;
+    if (o.kind > NBG_STAGE_COVARIANCEFEATURES)
+        return orc_consumers::run_consumer(RefBackend{t}, o, 0, out_cols, status, threads,
+                                           [](uint64_t m, int th, auto&& fn) { parallel_rows(m, th, fn); });
     const uint64_t n = t->cloud.pts.size();
     int nd = o.kind == NBG_STAGE_NORMAL ? 4
              : o.kind == NBG_STAGE_EIGENVALUES ? 3

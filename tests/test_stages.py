@@ -131,3 +131,77 @@ def test_radius_few_report():
     f = Filter("filters.covariancefeatures", {"radius": 1.0, "min_k": 7})
     f.report(_ex([(12, 0, abi.ROW_RADIUS_FEW)]))
     assert f.log()[-1] == "Skipping point 12. Found 0 neighbors but required 7."
+
+
+def test_consumer_defaults_and_dims():
+    # the other consumers' addArgs defaults and addDimensions
+    want = {
+        "filters.approximatecoplanar": (abi.STAGE_APPROXIMATECOPLANAR, 8, ["Coplanar"]),
+        "filters.estimaterank": (abi.STAGE_ESTIMATERANK, 8, ["Rank"]),
+        "filters.nndistance": (abi.STAGE_NNDISTANCE, 10, ["NNDistance"]),
+        "filters.optimalneighborhood": (abi.STAGE_OPTIMALNEIGHBORHOOD, 14,
+                                        ["OptimalKNN", "OptimalRadius"]),
+        "filters.lof": (abi.STAGE_LOF, 10, ["NNDistance", "LocalReachabilityDistance",
+                                            "LocalOutlierFactor"]),
+        "filters.outlier": (abi.STAGE_OUTLIER, 8, ["Classification"]),
+    }
+    for t, (kind, knn, dims) in want.items():
+        f = Filter(t)
+        o, rc = f.options()
+        assert rc == abi.NBG_OK and o.kind == kind and o.knn == knn, t
+        assert f.dims() == dims
+        assert abi.stage_dims(o) == dims
+    o, _ = Filter("filters.approximatecoplanar").options()
+    assert (o.thresh1, o.thresh2) == (25.0, 6.0)
+    o, _ = Filter("filters.estimaterank").options()
+    assert o.thresh1 == 0.01
+    o, _ = Filter("filters.optimalneighborhood").options()
+    assert o.min_k == 10
+    o, _ = Filter("filters.outlier").options()
+    assert (o.mode, o.min_k, o.radius, o.thresh1, o.label) == (0, 2, 1.0, 2.0, 7)
+
+
+def test_consumer_options():
+    o, _ = Filter("filters.nndistance", {"mode": "AVG", "k": 6}).options()
+    assert (o.mode, o.knn) == (1, 6)
+    with pytest.raises(StageError, match="Invalid value 'median' for argument 'mode'"):
+        Filter("filters.nndistance", {"mode": "median"})
+    o, _ = Filter("filters.outlier", {"method": "Radius", "radius": 1.5, "min_k": -1,
+                                      "class": 18}).options()
+    assert (o.mode, o.radius, o.min_k, o.label) == (1, 1.5, -1, 18)
+    f = Filter("filters.outlier", {"method": "sideways"})
+    o, _ = f.options()
+    assert o.mode == 2
+    assert f.log() == ['Requested method is unrecognized. Please choose from "statistical" or '
+                       '"radius".']
+    o, _ = Filter("filters.optimalneighborhood", {"min_k": 4, "max_k": 9}).options()
+    assert (o.min_k, o.knn) == (4, 9)
+    with pytest.raises(StageError, match="Unexpected argument 'knn'"):
+        Filter("filters.lof", {"knn": 4})
+
+
+def test_outlier_outcome_warnings():
+    for outl, inl, line in [(10, 0, "Requested filter would remove all points. Try a larger "
+                                    "radius/smaller minimum neighbors."),
+                            (0, 10, "Filtered cloud has no outliers!")]:
+        f = Filter("filters.outlier")
+        s = abi.RunStats()
+        s.outliers, s.inliers = outl, inl
+        f.outcome(s)
+        assert f.log() == [line]
+    f = Filter("filters.outlier")
+    s = abi.RunStats()
+    s.outliers, s.inliers = 3, 7
+    f.outcome(s)
+    assert f.log() == []
+
+
+def test_consumer_row_reports():
+    f = Filter("filters.approximatecoplanar")
+    f.report(_ex([(4, 0, abi.ROW_ZERO_COV)]))
+    assert f.log()[-1].startswith("Skipping point 4. Covariance matrix is all zeros.")
+    with pytest.raises(StageError, match=r"^filters\.approximatecoplanar: Cannot perform eigen"):
+        f.report(_ex([(1, 0, abi.ROW_EIGEN_FAIL)]))
+    g = Filter("filters.optimalneighborhood")
+    with pytest.raises(StageError, match="Cannot perform eigen decomposition."):
+        g.report(_ex([(2, 0, abi.ROW_EIGEN_FAIL)]))
