@@ -1138,9 +1138,13 @@ int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, i
     }
     int rc = ensure_scratch(ctx, n, 1);
     if (rc) return rc;
+    // sample: runs of 32 consecutive blocks (4096 rows), four waves of 8 blocks
+    // per SM (one wave would time its slowest SM, not the throughput)
     const uint64_t rows_total = (n + 127) / 128;
-    const unsigned blocks = (unsigned)std::min<uint64_t>(rows_total, 512);
-    const uint64_t stride = std::max<uint64_t>(128, (n / blocks) / 128 * 128);
+    const unsigned run = 32;
+    const unsigned blocks = (unsigned)std::min<uint64_t>(rows_total, (uint64_t)ctx->sm_count * 32 / run * run);
+    const unsigned groups = std::max(1u, blocks / run);
+    const uint64_t stride = std::max<uint64_t>((uint64_t)run * 128, (n / groups) / 128 * 128);
     const double scale = (double)n / ((double)blocks * 128.0);
     uint32_t* cnt_dev = ctx->counters + 32;  // scratch block, not the call counters
     float best = candidates[0];
@@ -1168,7 +1172,7 @@ int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, i
         ql.sums = ctx->sums;
         cudaMemsetAsync(cnt_dev, 0, 8 * sizeof(uint32_t), stream);
         cudaEventRecord(ctx->ev[2], stream);
-        rc = launch_select_sample(ctx, ql, stride, blocks, stream);
+        rc = launch_select_sample(ctx, ql, stride, blocks, std::min(run, blocks), stream);
         if (rc) return fail(ctx, rc, "autotune sample launch");
         cudaEventRecord(ctx->ev[3], stream);
         uint32_t cnt[3] = {0, 0, 0};
@@ -1178,9 +1182,9 @@ int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, i
         cudaEventElapsedTime(&build_ms, ctx->ev[0], ctx->ev[1]);
         cudaEventElapsedTime(&sample_ms, ctx->ev[2], ctx->ev[3]);
         // rows the ring search cannot finish go to the search replay: charge
-        // each an estimated 20 us of replay
+        // each an estimated 5 us of replay
         const double deferred = (double)cnt[0] * scale;
-        const double est = build_ms + sample_ms * scale + deferred * 0.02;
+        const double est = build_ms + sample_ms * scale + deferred * 0.005;
         if (est < best_ms) {
             best_ms = est;
             best = cf;

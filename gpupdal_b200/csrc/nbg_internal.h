@@ -137,9 +137,10 @@ struct QueryLaunch {
     const double* row_k = nullptr;  // per-row neighbour count (optimized), device
 };
 int launch_query(Context* ctx, const QueryLaunch& q, cudaStream_t stream);
-// Select pass over a sample of `blocks` blocks of 128 rows, `stride` rows apart.
+// Select pass over a sample of `blocks` blocks of 128 rows, in runs of `run`
+// consecutive blocks whose starts are `stride` rows apart.
 int launch_select_sample(Context* ctx, const QueryLaunch& q, uint64_t stride, unsigned blocks,
-                         cudaStream_t stream);
+                         unsigned run, cudaStream_t stream);
 
 // Tie rows ordered on the KD replica's tree (no search replay).
 struct TieLaunch {

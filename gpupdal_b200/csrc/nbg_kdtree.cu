@@ -796,7 +796,25 @@ __device__ __forceinline__ double kd_sq(double a, double b) {
     return __dmul_rn(d, d);
 }
 
+// Squared FP64 distance from q to replica position i, as the reference forms it.
+__device__ __forceinline__ double kd_point_dist(const KdDev& kd, const Transform& tf,
+                                                const double q[3], uint32_t i) {
+    const double p0 = ref_coord(kd.rx[i], tf.scale[0], tf.offset[0]);
+    const double p1 = ref_coord(kd.ry[i], tf.scale[1], tf.offset[1]);
+    const double p2 = ref_coord(kd.rz[i], tf.scale[2], tf.offset[2]);
+    const double d0 = __dsub_rn(q[0], p0);
+    const double d1 = __dsub_rn(q[1], p1);
+    const double d2 = __dsub_rn(q[2], p2);
+    return __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+}
+
 // Returns false when the explicit stack overflowed (never for sane trees).
+// WARP: the 32 lanes of a warp replay one row together.  Every lane walks the
+// same nodes and keeps the same result list; a leaf's points are measured 32
+// at a time and its candidates (below the worst distance taken at the leaf's
+// start, as the reference's leaf loop takes it) are inserted by every lane in
+// leaf order, so the list is the single-thread replay's exactly.
+template <bool WARP>
 __device__ bool kd_search(const KdDev& kd, const Transform& tf, const double q[3], KdResult& rs) {
     double dists[3] = {0.0, 0.0, 0.0};
     double distsq = 0.0;
@@ -820,16 +838,31 @@ __device__ bool kd_search(const KdDev& kd, const Transform& tf, const double q[3
         const int phase = st[top].phase;
         if (phase == 0 && kd.c1[node] < 0) {
             const double worst = rs.worst();
-            for (uint32_t i = kd.nb[node]; i < kd.ne[node]; ++i) {
-                const double p0 = ref_coord(kd.rx[i], tf.scale[0], tf.offset[0]);
-                const double p1 = ref_coord(kd.ry[i], tf.scale[1], tf.offset[1]);
-                const double p2 = ref_coord(kd.rz[i], tf.scale[2], tf.offset[2]);
-                const double d0 = __dsub_rn(q[0], p0);
-                const double d1 = __dsub_rn(q[1], p1);
-                const double d2 = __dsub_rn(q[2], p2);
-                const double dist = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
-                                              __dmul_rn(d2, d2));
-                if (dist < worst) rs.add(dist, kd.rid[i]);
+            const uint32_t b = kd.nb[node], e = kd.ne[node];
+            if (WARP) {
+                const int lane = threadIdx.x & 31;
+                for (uint32_t base = b; base < e; base += 32) {
+                    const uint32_t i = base + lane;
+                    double dist = 0.0;
+                    uint32_t id = 0;
+                    bool c = false;
+                    if (i < e) {
+                        dist = kd_point_dist(kd, tf, q, i);
+                        id = kd.rid[i];
+                        c = dist < worst;
+                    }
+                    unsigned m = __ballot_sync(0xffffffffu, c);
+                    while (m) {
+                        const int l = __ffs(m) - 1;
+                        m &= m - 1;
+                        rs.add(__shfl_sync(0xffffffffu, dist, l), __shfl_sync(0xffffffffu, id, l));
+                    }
+                }
+            } else {
+                for (uint32_t i = b; i < e; ++i) {
+                    const double dist = kd_point_dist(kd, tf, q, i);
+                    if (dist < worst) rs.add(dist, kd.rid[i]);
+                }
             }
             --top;
             continue;
@@ -868,30 +901,33 @@ __device__ bool kd_search(const KdDev& kd, const Transform& tf, const double q[3
     return true;
 }
 
-// Replays the reference's search for each listed row and writes its K
-// neighbour ids (the reference's order) to nbr[r*K ...].
-__global__ void kd_search_kernel(KdDev kd, Transform tf, const int32_t* __restrict__ x,
+// Replays the reference's search for each listed row, one warp per row, and
+// writes its K neighbour ids (the reference's order) to nbr[r*K ...].
+__global__ void __launch_bounds__(128) kd_search_kernel(KdDev kd, Transform tf, const int32_t* __restrict__ x,
                                  const int32_t* __restrict__ y, const int32_t* __restrict__ z,
                                  const uint32_t* __restrict__ rows, uint32_t nrows, int K,
                                  uint32_t* __restrict__ nbr, uint32_t* __restrict__ counts,
                                  uint32_t* errors, const double* row_k, uint64_t npts) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nrows) return;
+    const uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= nrows) return;  // whole warps leave together
     const uint32_t id = rows[r];
     const int Kr = row_neighbours(row_k, K, npts, id);  // <= K
     const double q[3] = {ref_coord(x[id], tf.scale[0], tf.offset[0]),
                          ref_coord(y[id], tf.scale[1], tf.offset[1]),
                          ref_coord(z[id], tf.scale[2], tf.offset[2])};
     if (Kr <= 0) {
-        counts[r] = 0;
+        if (lane == 0) counts[r] = 0;
         return;
     }
     KdResult rs;
     rs.init(Kr);
-    const bool ok = kd_search(kd, tf, q, rs);
-    for (int s = 0; s < K; ++s) nbr[(uint64_t)r * K + s] = s < rs.count ? rs.idx[s] : 0u;
-    counts[r] = ok ? (uint32_t)rs.count : 0u;
-    if (!ok) atomicAdd(errors, 1u);
+    const bool ok = kd_search<true>(kd, tf, q, rs);
+    for (int s = lane; s < K; s += 32) nbr[(uint64_t)r * K + s] = s < rs.count ? rs.idx[s] : 0u;
+    if (lane == 0) {
+        counts[r] = ok ? (uint32_t)rs.count : 0u;
+        if (!ok) atomicAdd(errors, 1u);
+    }
 }
 
 // Covariance of the replayed neighbour lists and the stage projections.
@@ -1438,7 +1474,7 @@ static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, ui
         return arc;
     }
     cudaMemsetAsync(kd->counters + 2, 0, 4, st);
-    kd_search_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(kd_view(t), t->tf, t->x, t->y, t->z,
+    kd_search_kernel<<<(nrows + 3) / 4, 128, 0, st>>>(kd_view(t), t->tf, t->x, t->y, t->z,
                                                           rows, nrows, K, *nbr, *counts,
                                                           kd->counters + 2, row_k, t->n);
     NBG_LAUNCHED(1);

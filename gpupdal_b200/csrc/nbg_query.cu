@@ -392,10 +392,13 @@ __device__ __forceinline__ void finish_row(const QueryArgs& a, const uint64_t i)
     nbg_finish_row(a.grp, a.tf, a.ex, id, (int)n, M, qraw);
 }
 
-// Autotuning sample: block b answers rows [b*stride, b*stride + 128).
+// Autotuning sample: runs of `run` consecutive blocks of 128 rows, run g
+// starting at row g*stride (neighbouring blocks share cells, as in a full
+// launch, so the sample sees the full launch's cache behaviour).
 template <int KS>
-__global__ void __launch_bounds__(128) knn_select_sample_kernel(const QueryArgs a, uint64_t stride) {
-    const uint64_t i = blockIdx.x * stride + threadIdx.x;
+__global__ void __launch_bounds__(128) knn_select_sample_kernel(const QueryArgs a, uint64_t stride,
+                                                                unsigned run) {
+    const uint64_t i = (blockIdx.x / run) * stride + (blockIdx.x % run) * 128ull + threadIdx.x;
     if (i < a.n) select_row<KS>(a, i);
 }
 
@@ -1148,6 +1151,7 @@ struct SampleArgs {
     QueryArgs q;
     uint64_t stride;
     unsigned blocks;
+    unsigned run;
     cudaStream_t stream;
 };
 
@@ -1156,14 +1160,14 @@ struct SampleLauncher {
     using Args = SampleArgs;
     static int run(const SampleArgs& s) {
         if (!s.blocks) return NBG_OK;
-        knn_select_sample_kernel<KS><<<s.blocks, 128, 0, s.stream>>>(s.q, s.stride);
+        knn_select_sample_kernel<KS><<<s.blocks, 128, 0, s.stream>>>(s.q, s.stride, s.run);
         NBG_LAUNCHED(1);
         return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
     }
 };
 
 int launch_select_sample(Context* ctx, const QueryLaunch& ql, uint64_t stride, unsigned blocks,
-                         cudaStream_t stream) {
+                         unsigned run, cudaStream_t stream) {
     (void)ctx;
     SampleArgs s{};
     s.q.gv = grid_view(ql.tile);
@@ -1182,6 +1186,7 @@ int launch_select_sample(Context* ctx, const QueryLaunch& ql, uint64_t stride, u
     s.q.row_k = ql.row_k;
     s.stride = stride;
     s.blocks = blocks;
+    s.run = std::max(1u, run);
     s.stream = stream;
     return dispatch_slots<SampleLauncher>(ql.K, s);
 }
