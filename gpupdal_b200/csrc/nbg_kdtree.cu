@@ -129,7 +129,6 @@ struct KdForest {
     uint32_t* nt = nullptr;        // per segment tile count, then prefix (seg_cap+1)
     uint32_t* tile_seg = nullptr;
     unsigned long long* tile_cnt = nullptr;  // per tile counts (lt | eq << 32), then prefix
-    int32_t* tile_mm = nullptr;    // per tile extents (6 ints)
     uint32_t tile_cap = 0;
     void* scan_tmp = nullptr;
     size_t scan_bytes = 0;
@@ -190,11 +189,12 @@ __global__ void kd_minmax_init_kernel(KdSplit* sp, uint32_t S) {
     }
 }
 
-// Per-tile extents (block reduction) into tile_mm[6*t]: min x,y,z, max x,y,z.
+// Segment extents: each tile's block reduction folded into its segment's
+// split record with integer atomics (mn/mx start at INT32_MAX/INT32_MIN).
 __global__ void __launch_bounds__(KD_THREADS) kd_minmax_kernel(const KdSeg* segs, const uint32_t* tile_first,
                                                                const uint32_t* tile_seg,
                                                                const int32_t* rx, const int32_t* ry,
-                                                               const int32_t* rz, int32_t* tile_mm) {
+                                                               const int32_t* rz, KdSplit* sp) {
     __shared__ int32_t red[KD_THREADS / 32][6];
     const uint32_t t = blockIdx.x;
     const uint32_t s = tile_seg[t];
@@ -230,42 +230,8 @@ __global__ void __launch_bounds__(KD_THREADS) kd_minmax_kernel(const KdSeg* segs
         int32_t r = red[0][threadIdx.x];
         for (int k = 1; k < KD_THREADS / 32; ++k)
             r = threadIdx.x < 3 ? min(r, red[k][threadIdx.x]) : max(r, red[k][threadIdx.x]);
-        tile_mm[6 * (size_t)t + threadIdx.x] = r;
-    }
-}
-
-// One block per segment folds its tiles' extents.
-__global__ void __launch_bounds__(KD_THREADS) kd_seg_minmax_kernel(uint32_t S, const uint32_t* tile_first,
-                                                                   const int32_t* tile_mm, KdSplit* sp) {
-    __shared__ int32_t red[KD_THREADS / 32][6];
-    const uint32_t s = blockIdx.x;
-    if (s >= S) return;
-    int32_t v[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, w[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
-    for (uint32_t t = tile_first[s] + threadIdx.x; t < tile_first[s + 1]; t += KD_THREADS) {
-        for (int d = 0; d < 3; ++d) {
-            v[d] = min(v[d], tile_mm[6 * (size_t)t + d]);
-            w[d] = max(w[d], tile_mm[6 * (size_t)t + 3 + d]);
-        }
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        v[d] = __reduce_min_sync(0xffffffffu, v[d]);
-        w[d] = __reduce_max_sync(0xffffffffu, w[d]);
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-        for (int d = 0; d < 3; ++d) {
-            red[warp][d] = v[d];
-            red[warp][3 + d] = w[d];
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        int32_t r = red[0][threadIdx.x];
-        for (int k = 1; k < KD_THREADS / 32; ++k)
-            r = threadIdx.x < 3 ? min(r, red[k][threadIdx.x]) : max(r, red[k][threadIdx.x]);
-        if (threadIdx.x < 3) sp[s].mn[threadIdx.x] = r;
-        else sp[s].mx[threadIdx.x - 3] = r;
+        if (threadIdx.x < 3) atomicMin(&sp[s].mn[threadIdx.x], r);
+        else atomicMax(&sp[s].mx[threadIdx.x - 3], r);
     }
 }
 
@@ -1087,13 +1053,10 @@ static int kd_tiles(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, u
         uint32_t cap = std::max<uint32_t>(total + 1, kd->tile_cap * 2);
         if (kd->tile_seg) kd_release(ctx, kd, kd->tile_seg);
         if (kd->tile_cnt) kd_release(ctx, kd, kd->tile_cnt);
-        if (kd->tile_mm) kd_release(ctx, kd, kd->tile_mm);
         kd->tile_seg = nullptr;
         kd->tile_cnt = nullptr;
-        kd->tile_mm = nullptr;
         int rc = kd_alloc(ctx, (void**)&kd->tile_seg, (size_t)cap * 4, kd);
         if (!rc) rc = kd_alloc(ctx, (void**)&kd->tile_cnt, (size_t)(cap + 1) * 8, kd);
-        if (!rc) rc = kd_alloc(ctx, (void**)&kd->tile_mm, (size_t)cap * 24, kd);
         if (rc) return rc;
         kd->tile_cap = cap;
     }
@@ -1103,12 +1066,16 @@ static int kd_tiles(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, u
     return NBG_OK;
 }
 
+// known_tiles: the tile count when the tile map of `segs` is already built
+// (~0u: build it).
 template <int PASS>
 static int kd_pass(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, KdSplit* sp,
-                   cudaStream_t st) {
-    uint32_t ntiles = 0;
-    int rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
-    if (rc) return rc;
+                   cudaStream_t st, uint32_t known_tiles = ~0u) {
+    uint32_t ntiles = known_tiles;
+    if (known_tiles == ~0u) {
+        int rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
+        if (rc) return rc;
+    }
     if (ntiles) {
         kd_count_kernel<PASS><<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg, sp, kd->rx,
                                                              kd->ry, kd->rz, kd->tfs, kd->tile_cnt);
@@ -1228,15 +1195,13 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
         kd_minmax_init_kernel<<<(S + 127) / 128, 128, 0, st>>>(kd->split, S);
         rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
         if (rc) return rc;
-        if (ntiles) {
+        if (ntiles)
             kd_minmax_kernel<<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->rx, kd->ry,
-                                                            kd->rz, kd->tile_mm);
-            kd_seg_minmax_kernel<<<S, KD_THREADS, 0, st>>>(S, kd->nt, kd->tile_mm, kd->split);
-            NBG_LAUNCHED(1);
-        }
+                                                            kd->rz, kd->split);
         kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->tfs, kd->bmin, kd->bmax);
         NBG_LAUNCHED(2 + (ntiles ? 1 : 0));
-        rc = kd_pass<1>(ctx, kd, segs, S, kd->split, st);
+        // pass 1 runs on the same segments: their tile map is already built
+        rc = kd_pass<1>(ctx, kd, segs, S, kd->split, st, ntiles);
         if (rc) return rc;
         // pass 2 only where points equal the cut value
         cudaMemsetAsync(kd->counters + 5, 0, 4, st);
