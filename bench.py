@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--served-rate", type=float, default=20.0)
     ap.add_argument("--served-slots", type=int, default=4)
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--served-sweep", default="",
+                    help="comma-separated request rates (req/s, 0: all at once): run only the "
+                         "served stream (--served-requests requests) at each rate, one JSON "
+                         "line per rate")
     ap.add_argument("--batch-tiles", type=int, default=256)
     ap.add_argument("--no-batched", action="store_true")
     return ap.parse_args()
@@ -238,6 +242,38 @@ def served_leg(ctx, args):
     }
 
 
+def served_sweep(ctx, args):
+    """The served stream at each rate of --served-sweep: p50/p99 latency from
+    submission to results and Mpts/s, beside the plain per-tile calls' Mpts/s
+    on the same stream (requests materialised one at a time)."""
+    from gpupdal_b200 import served
+    from gpupdal_b200.native import Server
+    reqs = served.make_stream(args.served_requests, seed=1000, lazy=True)
+    pts = reqs.points()
+    warm = served.make_stream(24, seed=999)
+    served.run_plain(ctx, warm)
+    plain_s = sum(served.run_plain(ctx, reqs))
+    stream = (f"{len(reqs)} requests, sizes log-uniform 10k-8M of the mixture (subsamples of one "
+              "8M cloud, seed 1000), knn in {8,16,32,64}, normal/eigenvalues/"
+              "covariancefeatures(all) in equal shares; host buffers in and out; Poisson arrivals")
+    srv = Server(0, slots=args.served_slots, hbm_budget=120 * 10**9)
+    try:
+        served.run_served(srv, warm)
+        for rate in [float(r) for r in args.served_sweep.split(",") if r]:
+            # rate 0: every request at once (the server's capacity)
+            span_s, lat, _ = served.run_served(srv, reqs, rate=rate or None, seed=int(rate))
+            lat_ms = np.sort(np.array(lat) * 1e3)
+            print(json.dumps({
+                "metric": "served stream latency and throughput", "rate_req_s": rate,
+                "requests": len(reqs), "points": pts, "slots": args.served_slots,
+                "hbm_budget_gb": 120, "p50_ms": float(np.percentile(lat_ms, 50)),
+                "p99_ms": float(np.percentile(lat_ms, 99)), "max_ms": float(lat_ms[-1]),
+                "served_mpts_s": pts / span_s / 1e6, "plain_mpts_s": pts / plain_s / 1e6,
+                "stream": stream}), flush=True)
+    finally:
+        srv.close()
+
+
 def dist_setup():
     """One process per GPU (torchrun env); NCCL on GPUs, gloo without (host-logic tests)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -303,6 +339,9 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.served_sweep:
+        served_sweep(Context(local), args)
+        return
     x, y, z = workload(args.points, 2 + rank)
     n = len(x)
     ctx = Context(local)

@@ -5,7 +5,8 @@ log-uniform in [10k, 8M] points of the building/vegetation/terrain mixture,
 knn uniform in {8, 16, 32, 64}, and the stage normal, eigenvalues or
 covariancefeatures (feature_set=all, with OptimalKNN/OptimalRadius columns)
 in equal shares.  Requests are uniform subsamples of one pre-generated,
-pre-shuffled mixture cloud (so a bounded stream generates in seconds).
+pre-shuffled mixture cloud, handed out as views of it (so a stream of any
+length generates in seconds and submitting a request copies nothing).
 
 run_plain() answers the requests one after another with the plain per-tile
 call (upload, nbg_run, free; host buffers in and out).  run_served() submits
@@ -25,30 +26,60 @@ from . import synthetic as syn
 KNNS = (8, 16, 32, 64)
 
 
+class Stream:
+    """The requests of a stream as views of one cloud: each request is a
+    contiguous slice of the (doubled) pool, its OptimalKNN / OptimalRadius
+    columns slices of pre-built columns, so taking a request copies nothing
+    and a long stream costs host memory only for the pool."""
+
+    def __init__(self, pool, specs, seed, max_points):
+        x, y, z = pool
+        m = min(max_points, len(x))
+        self.x, self.y, self.z = (np.concatenate([v, v[:m]]) for v in (x, y, z))
+        rng = np.random.default_rng(seed + 7919)
+        self.ropt = rng.uniform(0.3, 1.5, len(self.x))
+        self.kopt = {k: np.full(m, float(k)) for k in KNNS}
+        self.specs = specs
+
+    def __len__(self):
+        return len(self.specs)
+
+    def __getitem__(self, i):
+        s0, n, knn, kind = self.specs[i]
+        if kind == abi.STAGE_COVARIANCEFEATURES:
+            st = abi.make_opts(kind, knn=knn, feature_mask=abi.FEAT_ALL)
+            kopt, ropt = self.kopt[knn][:n], self.ropt[s0:s0 + n]
+        else:
+            st = abi.make_opts(kind, knn=knn)
+            kopt = ropt = None
+        return dict(x=self.x[s0:s0 + n], y=self.y[s0:s0 + n], z=self.z[s0:s0 + n], stages=[st],
+                    kopt=kopt, ropt=ropt, knn=knn, kind=kind)
+
+    def __iter__(self):
+        return (self[i] for i in range(len(self)))
+
+    def points(self):
+        return sum(s[1] for s in self.specs)
+
+
 def make_stream(count, seed=1000, pool_points=8_000_000, min_points=10_000,
-                max_points=8_000_000):
+                max_points=8_000_000, lazy=False):
+    """`count` requests (a list, or with lazy=True the Stream itself, which
+    hands out each request when it is taken)."""
     rng = np.random.default_rng(seed)
     x, y, z = syn.mixture(pool_points, seed)
     perm = rng.permutation(pool_points)
     x, y, z = x[perm], y[perm], z[perm]
     sizes = np.exp(rng.uniform(np.log(min_points), np.log(min(max_points, pool_points)), count))
-    reqs = []
+    specs = []
     for i in range(count):
         n = int(sizes[i])
         s0 = int(rng.integers(0, pool_points))
-        idx = (s0 + np.arange(n)) % pool_points
         knn = int(rng.choice(KNNS))
         kind = (abi.STAGE_NORMAL, abi.STAGE_EIGENVALUES, abi.STAGE_COVARIANCEFEATURES)[i % 3]
-        if kind == abi.STAGE_COVARIANCEFEATURES:
-            st = abi.make_opts(kind, knn=knn, feature_mask=abi.FEAT_ALL)
-            kopt, ropt = syn.optimal_columns(n, seed + i, knn=knn)
-        else:
-            st = abi.make_opts(kind, knn=knn)
-            kopt = ropt = None
-        reqs.append(dict(x=np.ascontiguousarray(x[idx]), y=np.ascontiguousarray(y[idx]),
-                         z=np.ascontiguousarray(z[idx]), stages=[st], kopt=kopt, ropt=ropt,
-                         knn=knn, kind=kind))
-    return reqs
+        specs.append((s0, n, knn, kind))
+    stream = Stream((x, y, z), specs, seed, max_points)
+    return stream if lazy else list(stream)
 
 
 def run_plain(ctx, reqs):
@@ -70,10 +101,13 @@ def run_served(server, reqs, rate=None, seed=0):
     gaps = rng.exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
     arrivals = np.cumsum(gaps) - gaps[0]
     tickets = [None] * len(reqs)
+    held = [None] * len(reqs)
     t0 = time.perf_counter()
 
     def client():
-        for i, r in enumerate(reqs):
+        for i in range(len(reqs)):
+            r = reqs[i]
+            held[i] = r
             delay = arrivals[i] - (time.perf_counter() - t0)
             if delay > 0:
                 time.sleep(delay)
@@ -87,6 +121,7 @@ def run_served(server, reqs, rate=None, seed=0):
         while tickets[i] is None:
             time.sleep(0.0005)
         results[i] = server.wait(tickets[i])[2]
+        held[i] = None  # the request's host buffers may go once its result is back
     th.join()
     first = min(r.submit_us for r in results)
     last = max(r.end_us for r in results)
