@@ -226,3 +226,36 @@ def test_consumer_options_refused(nbg):
     o.mode = 2
     outs, _, stats = nbg.run(tile, [o])
     assert (outs[0][0] == 0).all() and stats.outliers == 0
+
+
+def test_pipeline_json_runs_the_consumers(nbg):
+    """An existing pipeline naming the consumers runs through the stage layer
+    with the filters' own names and options; each dimension equals the
+    direct nbg_run of the same options, and filters.outlier's warning is
+    logged when no row is an outlier."""
+    from gpupdal_b200.stages import run_pipeline
+    x, y, z = _cloud("mixture")
+    pipe = ["in.las",
+            {"type": "filters.nndistance", "mode": "avg", "k": 6},
+            {"type": "filters.lof", "minpts": 12},
+            {"type": "filters.approximatecoplanar", "knn": 10, "thresh1": 20},
+            {"type": "filters.estimaterank", "knn": 9},
+            {"type": "filters.outlier", "method": "radius", "radius": 5.0, "min_k": 0},
+            "out.las"]
+    dims, log = run_pipeline(nbg, pipe, x, y, z)
+    assert log[0] == "not run: file" and log[-1] == "not run: file"
+    assert any("Filtered cloud has no outliers!" in l for l in log)
+    tile = nbg.tile(x, y, z)
+    direct = {
+        "LocalOutlierFactor": (abi.consumer_opts(abi.STAGE_LOF, minpts=12), 2),
+        "Coplanar": (abi.consumer_opts(abi.STAGE_APPROXIMATECOPLANAR, knn=10, thresh1=20.0), 0),
+        "Rank": (abi.consumer_opts(abi.STAGE_ESTIMATERANK, knn=9), 0),
+        "Classification": (abi.consumer_opts(abi.STAGE_OUTLIER, method="radius", radius=5.0,
+                                             min_k=0), 0),
+    }
+    for name, (o, d) in direct.items():
+        outs, _, _ = nbg.run(tile, [o])
+        assert np.array_equal(dims[name], outs[0][d], equal_nan=True), name
+    # NNDistance was written by nndistance, then by lof (the later stage wins, as in PDAL)
+    outs, _, _ = nbg.run(tile, [abi.consumer_opts(abi.STAGE_LOF, minpts=12)])
+    assert np.array_equal(dims["NNDistance"], outs[0][0])
