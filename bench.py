@@ -63,6 +63,8 @@ def parse():
                          "line per rate")
     ap.add_argument("--batch-tiles", type=int, default=256)
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the extra stages / consumers / LAS ingest leg")
     return ap.parse_args()
 
 
@@ -166,6 +168,109 @@ def cpu_reference(x, y, z, knn, sample, kind=None):
                                     f"{side / 100:.0f} m) of the same tile: KD build + "
                                     f"eigenvalues + normal, {threads} threads",
             "seconds": dt}
+
+
+def extras_cases():
+    """The stage options beyond the main path (radius, stride, optimized) and
+    the other consumers of the index, each as one stage on the 4M mixture."""
+    from gpupdal_b200 import abi
+    c = abi.consumer_opts
+    return [
+        ("normal radius=0.5", abi.make_opts(abi.STAGE_NORMAL, radius=0.5)),
+        ("eigenvalues knn=8 stride=2", abi.make_opts(abi.STAGE_EIGENVALUES, knn=8, stride=2)),
+        ("covariancefeatures optimized all", abi.make_opts(abi.STAGE_COVARIANCEFEATURES,
+                                                           optimized=True, feature_mask=abi.FEAT_ALL)),
+        ("approximatecoplanar knn=8", c(abi.STAGE_APPROXIMATECOPLANAR)),
+        ("estimaterank knn=8", c(abi.STAGE_ESTIMATERANK)),
+        ("nndistance k=10 avg", c(abi.STAGE_NNDISTANCE, mode="avg")),
+        ("optimalneighborhood 10..14", c(abi.STAGE_OPTIMALNEIGHBORHOOD)),
+        ("lof minpts=10", c(abi.STAGE_LOF)),
+        ("outlier statistical mean_k=8", c(abi.STAGE_OUTLIER)),
+        ("outlier radius=1 min_k=2", c(abi.STAGE_OUTLIER, method="radius")),
+    ]
+
+
+def cpu_reference_stage(x, y, z, st, kopt, ropt, sample=250_000):
+    """The reference's CPU loop of one stage (oracle/_ref, all host threads) on
+    a spatially contiguous window of about `sample` points of the tile."""
+    from gpupdal_b200 import synthetic as syn
+    from oracle import oracle as orc
+    kind = "reference" if orc.available("reference") else "port"
+    o = orc.Oracle(kind)
+    side = int(round(np.sqrt(sample / len(x)) * (x.max() + 1)))
+    m = (x < side) & (y < side)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    t = o.tree(*(syn.to_double(v) for v in (x[m], y[m], z[m])))
+    t.run_stage(st, mode=0, threads=threads,
+                optimal_knn=None if kopt is None else kopt[m],
+                optimal_radius=None if ropt is None else ropt[m])
+    dt = time.perf_counter() - t0
+    return {"value": int(m.sum()) / dt / 1e6, "unit": "Mpts/s", "cores": threads, "kind": kind,
+            "sample": f"{int(m.sum())}-point window of the same tile: KD build + the stage"}
+
+
+def extras_leg(ctx, args):
+    """The §8f rows measured: each extra stage on the 4M mixture (device
+    inputs, one fresh tile per step), and LAS ingest of the same points."""
+    import tempfile
+    import torch
+    from gpupdal_b200 import las
+    from gpupdal_b200 import synthetic as syn
+    x, y, z = syn.mixture(4_000_000, 1)
+    n = len(x)
+    kopt, ropt = syn.optimal_columns(n, 1, knn=10)
+    dev = torch.device("cuda", ctx.device)
+    dx, dy, dz = (torch.from_numpy(v).to(dev) for v in (x, y, z))
+    dk, dr = torch.from_numpy(kopt).to(dev), torch.from_numpy(ropt).to(dev)
+    out = {"workload": f"mixture tile {n} points (seed 1), one stage per entry, device inputs "
+                       "and outputs, a fresh tile (upload + grid + KD replica) every step"}
+
+    def timed_ms(fn, steps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    for label, st in extras_cases():
+        def step():
+            tile = ctx.tile(dx, dy, dz)
+            ctx.run(tile, [st], optimal_knn=dk, optimal_radius=dr, device_out=True)
+            tile.free()
+        try:
+            ms = timed_ms(step)
+            e = {"ms": ms, "mpts_s": n / ms / 1e3}
+            if not args.no_cpu_baseline:
+                cb = cpu_reference_stage(x, y, z, st, kopt, ropt)
+                e["cpu_baseline"] = cb
+                e["vs_cpu"] = e["mpts_s"] / cb["value"]
+        except Exception as exc:  # recorded, not fatal to the main line
+            e = {"error": str(exc)}
+        out[label] = e
+    # LAS ingest: point format 6 records (30 bytes), host-mapped and device-resident
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "tile.las")
+        las.write_las(path, x, y, z, version=(1, 4), point_format=6)
+        f = las.LasFile(path)
+        rec = np.ascontiguousarray(f.records)
+        drec = torch.from_numpy(rec).to(dev)
+        nbytes = rec.nbytes
+
+        def up_host():
+            ctx.tile_from_las(f).free()
+
+        def up_dev():
+            ctx.tile_from_las(f, records=drec).free()
+        for label, fn in (("las ingest host records", up_host), ("las ingest device records", up_dev)):
+            ms = timed_ms(fn)
+            out[label] = {"ms": ms, "mpts_s": n / ms / 1e3, "gb_s": nbytes / ms / 1e6,
+                          "record_bytes": int(f.record_length)}
+    return out
 
 
 def batched_leg(ctx, args):
@@ -438,6 +543,8 @@ def main():
         line["batched"] = batched_leg(ctx, args)
     if ws == 1 and not args.no_served:
         line["served"] = served_leg(ctx, args)
+    if ws == 1 and not args.no_extras:
+        line["extras"] = extras_leg(ctx, args)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(x, y, z, args.knn, args.cpu_sample)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

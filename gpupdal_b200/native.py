@@ -28,6 +28,14 @@ def _dptr(a):
 EXC_DTYPE = [("point_id", np.uint32), ("stage", np.uint8), ("code", np.uint8), ("reserved", np.uint16)]
 
 
+def exceptions_array(buf, count):
+    """The first `count` nbg_row_exception records of a ctypes array as a
+    structured numpy array (the record is EXC_DTYPE byte for byte)."""
+    if count == 0:
+        return np.zeros(0, dtype=EXC_DTYPE)
+    return np.frombuffer(buf, dtype=np.dtype(EXC_DTYPE), count=count).copy()
+
+
 def record_columns(base_ptr, stages, record_bytes, on_device):
     """abi.Columns for `stages` sharing one record per point: the stages'
     dims are laid out one after another from offset 0."""
@@ -150,9 +158,7 @@ class Context:
                               ctypes.c_void_p(stream) if stream else None)
         self._check(rc)
         m = min(nexc.value, cap)
-        ex = np.zeros(m, dtype=EXC_DTYPE)
-        for j in range(m):
-            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code, exc[j].reserved)
+        ex = exceptions_array(exc, m)
         return [o[: len(abi.stage_dims(s))] for o, s in zip(outs, stages)], ex, stats
 
     def run_columns(self, tile, stages, columns, optimal_knn=None, optimal_radius=None,
@@ -176,9 +182,7 @@ class Context:
                               ctypes.c_void_p(stream) if stream else None)
         self._check(rc)
         m = min(nexc.value, cap)
-        ex = np.zeros(m, dtype=EXC_DTYPE)
-        for j in range(m):
-            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code, exc[j].reserved)
+        ex = exceptions_array(exc, m)
         return ex, stats
 
     def run_batch(self, tiles, stages, outputs, optimal=None, graph=True, autotune=False,
@@ -218,9 +222,7 @@ class Context:
         out = []
         for i in range(m):
             k = min(nex[i], exception_capacity)
-            ex = np.zeros(k, dtype=EXC_DTYPE)
-            for j in range(k):
-                ex[j] = (excs[i][j].point_id, excs[i][j].stage, excs[i][j].code, excs[i][j].reserved)
+            ex = exceptions_array(excs[i], k)
             out.append(ex)
         return out, stats
 
@@ -400,9 +402,7 @@ class Server:
         if res.status != abi.NBG_OK:
             raise NbgError(res.status, self.lib.nbg_server_last_error(self.h).decode())
         m = min(res.n_exceptions, len(exc))
-        ex = np.zeros(m, dtype=EXC_DTYPE)
-        for j in range(m):
-            ex[j] = (exc[j].point_id, exc[j].stage, exc[j].code, exc[j].reserved)
+        ex = exceptions_array(exc, m)
         return [o[: len(abi.stage_dims(s))] for o, s in zip(outs, stages)], ex, res
 
     def close(self):

@@ -57,10 +57,15 @@ class Filter:
     def report(self, exceptions, stage_index=0):
         n = len(exceptions)
         arr = (abi.RowException * max(n, 1))()
-        for i, e in enumerate(exceptions):
-            arr[i].point_id, arr[i].stage, arr[i].code = int(e["point_id"]), int(e["stage"]), int(e["code"])
-            if "reserved" in e.dtype.names:
-                arr[i].reserved = int(e["reserved"])
+        from .native import EXC_DTYPE
+        if n and exceptions.dtype == np.dtype(EXC_DTYPE):
+            ctypes.memmove(arr, np.ascontiguousarray(exceptions).ctypes.data, n * ctypes.sizeof(abi.RowException))
+        else:
+            for i, e in enumerate(exceptions):
+                arr[i].point_id, arr[i].stage, arr[i].code = (int(e["point_id"]), int(e["stage"]),
+                                                              int(e["code"]))
+                if "reserved" in e.dtype.names:
+                    arr[i].reserved = int(e["reserved"])
         err = ctypes.create_string_buffer(1024)
         rc = self.lib.nbg_filter_report(self.h, arr, n, int(stage_index), err, len(err))
         if rc != abi.NBG_OK:
