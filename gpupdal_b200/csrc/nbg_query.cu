@@ -748,14 +748,15 @@ int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream) {
 // search meets them on the KD replica's tree); positions 0, stride, 2*stride,
 // ... give the neighbourhood.  Rows the ring search cannot finish, or whose
 // group exceeds the collection, go to the search replay.
-static constexpr int STRIDE_LIST = 66;
-
+// The list holds K <= KS - 1 entries (fewer than K points are strictly
+// closer than D), so its arrays are sized by the launch's slot count.
+template <int KS>
 struct StrideFn {
     float qx, qy, qz;
     uint32_t kk;
     int less, gcnt;
-    uint32_t id[STRIDE_LIST + TIE_CAP];  // [0, less): closer than D; then the group
-    int off[STRIDE_LIST + TIE_CAP][3];
+    uint32_t id[KS];  // [0, less): closer than D; then the group's chosen members
+    int off[KS][3];
     uint32_t gid[TIE_CAP];
     int goff[TIE_CAP][3];
     __device__ __forceinline__ unsigned long long limit() const {
@@ -765,7 +766,7 @@ struct StrideFn {
         const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
         const uint32_t key = dist_key(dx, dy, dz);
         if (key < kk) {
-            if (less < STRIDE_LIST) {
+            if (less < KS) {
                 id[less] = __float_as_uint(p.w);
                 off[less][0] = small_int(dx);
                 off[less][1] = small_int(dy);
@@ -817,7 +818,7 @@ __global__ void __launch_bounds__(128) knn_stride_kernel(const StrideArgs sa) {
         a.exact_rows[slot] = rid;
         return;
     }
-    StrideFn f;
+    StrideFn<KS> f;
     f.qx = q.x;
     f.qy = q.y;
     f.qz = q.z;
@@ -826,7 +827,7 @@ __global__ void __launch_bounds__(128) knn_stride_kernel(const StrideArgs sa) {
     f.gcnt = 0;
     for (int r = 0; r <= R; ++r) scan_shell(a.gv, g, qc, r, f);
     const int m = K - f.less;
-    if (f.gcnt > TIE_CAP || f.less > STRIDE_LIST || m <= 0 || m > f.gcnt) {
+    if (f.gcnt > TIE_CAP || f.less >= KS || m <= 0 || m > f.gcnt) {
         const uint32_t slot = atomicAdd(&a.counters[0], 1u);
         a.exact_rows[slot] = rid;
         return;
@@ -856,7 +857,7 @@ __global__ void __launch_bounds__(128) knn_stride_kernel(const StrideArgs sa) {
         f.off[f.less + j][2] = f.goff[best][2];
     }
     // the list in the reference's order: FP64 distance, then visiting order
-    double d[STRIDE_LIST + TIE_CAP];
+    double d[KS];
     for (int t = 0; t < K; ++t) d[t] = ref_dist2(q64, qraw, f.off[t], a.tf);
     for (int t = 1; t < K; ++t) {
         const double dv = d[t];
