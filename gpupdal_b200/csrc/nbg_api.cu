@@ -408,6 +408,7 @@ int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const in
                     void* stream_v, nbg_tile** out) {
     if (!h || !out) return NBG_ERR_INVALID;
     Context* ctx = &h->c;
+    std::lock_guard<std::mutex> lock(ctx->mu);
     *out = nullptr;
     if (n > 0 && (!x || !y || !z)) return fail(ctx, NBG_ERR_INVALID, "null coordinate array");
     nbg_tile* th = nullptr;
@@ -513,6 +514,7 @@ int nbg_tile_tune(nbg_context* h, nbg_tile* th, float cell_factor, int32_t fixed
 
 int nbg_tile_free(nbg_context* h, nbg_tile* th) {
     if (!h || !th) return NBG_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(h->c.mu);
     cudaSetDevice(h->c.device);
     tile_release(&h->c, &th->t);
     delete th;

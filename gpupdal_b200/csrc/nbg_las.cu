@@ -84,6 +84,7 @@ extern "C" int nbg_tile_upload_las(nbg_context* h, const void* records, uint64_t
                                    const double offset[3], void* stream_v, nbg_tile** out) {
     if (!h || !out) return NBG_ERR_INVALID;
     Context* ctx = &h->c;
+    std::lock_guard<std::mutex> lock(ctx->mu);
     *out = nullptr;
     if (n && !records) return fail(ctx, NBG_ERR_INVALID, "null record buffer");
     if (record_length < 12) return fail(ctx, NBG_ERR_INVALID, "LAS point records hold at least X, Y, Z");

@@ -201,7 +201,12 @@ int nbg_device_count(void);
 
 /* Context: owns device scratch, resident tiles and the HBM budget.
  * Replaces the fork's resident neighbourhood lifetime
- * (src/pdal/PdgNeighborhood.cpp:1383-1550). */
+ * (src/pdal/PdgNeighborhood.cpp:1383-1550).
+ * Threads: the calls that take a context serialise on it (uploads, runs,
+ * tuning and frees of its tiles wait for one another), so a context may be
+ * shared; for work that overlaps on the GPU use one context per thread, or
+ * the served form below, whose slots each own one.  nbg_last_error reports
+ * the context's most recent failure, whichever thread made it. */
 int nbg_create(nbg_context** ctx, int device, uint64_t hbm_budget_bytes);
 int nbg_destroy(nbg_context* ctx);
 const char* nbg_last_error(const nbg_context* ctx);
