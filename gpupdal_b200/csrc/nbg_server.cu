@@ -8,6 +8,7 @@
 // arrival starts as soon as a slot and memory are free (continuous batching),
 // never waiting for a batch boundary.  Every request runs the same code path
 // as the plain per-tile call, so its results do not depend on the mix.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -62,9 +63,17 @@ extern "C" uint64_t nbg_request_bytes(const nbg_request* r) {
     // grid (coordinates, sorted copy, keys, cell table and column directory),
     // query scratch (row sums, tie and replay lists), KD replica (point order,
     // inverse, partition scratch, nodes), plus host-output staging per dim
-    uint64_t dims = 0;
-    for (int s = 0; s < r->n_stages; ++s) dims += (uint64_t)r->outputs[s].ndims;
-    return r->n * (200 + 8 * dims) + (64ull << 20);
+    uint64_t dims = 0, extra = 0;
+    if (r->n_stages > 0 && (!r->stages || !r->outputs)) return 0;
+    for (int s = 0; s < r->n_stages; ++s) {
+        dims += (uint64_t)r->outputs[s].ndims;
+        const nbg_stage_opts& o = r->stages[s];
+        // lof keeps its ordered lists (ids and distances) and two row arrays;
+        // the outlier stages a row value and a flag per point
+        if (o.kind == NBG_STAGE_LOF) extra = std::max<uint64_t>(extra, 12ull * (o.knn + 1) + 16);
+        if (o.kind == NBG_STAGE_OUTLIER) extra = std::max<uint64_t>(extra, 16);
+    }
+    return r->n * (200 + 8 * dims + extra) + (64ull << 20);
 }
 
 void nbg_server::worker(int slot) {
