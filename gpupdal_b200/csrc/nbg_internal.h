@@ -157,6 +157,8 @@ struct TieLaunch {
     const double* row_k = nullptr;
 };
 int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream);
+// The tie rows of several tiles in one launch (returns after it completed).
+int launch_ties_many(Context* ctx, const TieLaunch* tls, int count, cudaStream_t stream);
 
 // Radius neighbourhoods of one stage (no tie order: every point within the
 // radius belongs to the set).

@@ -470,6 +470,7 @@ struct QueueArgs {
     unsigned long long* head;
     int sms;
     cudaStream_t stream;
+    int reserve;  // resident blocks per SM left to kernels of other streams
 };
 
 template <int KS>
@@ -478,7 +479,8 @@ struct QueueLauncher {
     static int run(const QueueArgs& q) {
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_select_queue_kernel<KS>, 128, 0);
-        const uint64_t grid = std::min<uint64_t>(q.items, (uint64_t)q.sms * std::max(per_sm, 1));
+        const uint64_t grid =
+            std::min<uint64_t>(q.items, (uint64_t)q.sms * std::max(per_sm - q.reserve, 1));
         if (!grid) return NBG_OK;
         knn_select_queue_kernel<KS><<<(unsigned)grid, 128, 0, q.stream>>>(q.jobs, q.njobs, q.items,
                                                                            q.head);
@@ -623,9 +625,8 @@ struct TieArgs {
     uint32_t* ids_out;
 };
 
-__global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= a.nties) return;
+// One tie row r of a.ties.
+__device__ __forceinline__ void tie_row(const TieArgs& a, uint32_t r) {
     const uint2 e = a.ties[r];
     const uint32_t id = e.x;
     const uint32_t kk = KEY_BASE + (e.y & 0xFFFFFFu);
@@ -711,9 +712,28 @@ __global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
     nbg_finish_row(a.grp, a.tf, a.ex, id, (int)n, M, qraw);
 }
 
-int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream) {
-    (void)ctx;
-    if (!tl.nties) return NBG_OK;
+__global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < a.nties) tie_row(a, r);
+}
+
+// The tie rows of many tiles in one launch: jobs[j] is tile j's arguments,
+// its rows are entries first[j] .. first[j+1]-1 of the launch.
+__global__ void __launch_bounds__(128) knn_tie_batch_kernel(const TieArgs* __restrict__ jobs,
+                                                            const uint64_t* __restrict__ first,
+                                                            int njobs) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t >= first[njobs]) return;
+    int lo = 0, hi = njobs;  // the job whose range holds t
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (first[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    tie_row(jobs[lo], (uint32_t)(t - first[lo]));
+}
+
+static TieArgs tie_args(const TieLaunch& tl) {
     TieArgs a;
     a.gv = grid_view(tl.tile);
     a.gp = tl.tile->gp;
@@ -732,9 +752,46 @@ int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream) {
     a.exact_rows = tl.exact_rows;
     a.counters = tl.counters;
     a.ids_out = tl.ids_out;
-    knn_tie_kernel<<<(tl.nties + 127) / 128, 128, 0, stream>>>(a);
+    return a;
+}
+
+int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream) {
+    (void)ctx;
+    if (!tl.nties) return NBG_OK;
+    knn_tie_kernel<<<(tl.nties + 127) / 128, 128, 0, stream>>>(tie_args(tl));
     NBG_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+}
+
+int launch_ties_many(Context* ctx, const TieLaunch* tls, int count, cudaStream_t stream) {
+    std::vector<TieArgs> jobs;
+    std::vector<uint64_t> first(1, 0);
+    for (int i = 0; i < count; ++i) {
+        if (!tls[i].nties) continue;
+        jobs.push_back(tie_args(tls[i]));
+        first.push_back(first.back() + tls[i].nties);
+    }
+    if (jobs.empty()) return NBG_OK;
+    TieArgs* djobs = nullptr;
+    uint64_t* dfirst = nullptr;
+    const size_t jb = jobs.size() * sizeof(TieArgs), fb = first.size() * sizeof(uint64_t);
+    int rc = ctx_alloc(ctx, (void**)&djobs, jb);
+    if (!rc) rc = ctx_alloc(ctx, (void**)&dfirst, fb);
+    // pageable sources: both copies complete before they return
+    if (!rc) rc = host_to_device(ctx, djobs, jobs.data(), jb, stream);
+    if (!rc) rc = host_to_device(ctx, dfirst, first.data(), fb, stream);
+    if (!rc) {
+        const uint64_t total = first.back();
+        knn_tie_batch_kernel<<<(unsigned)((total + 127) / 128), 128, 0, stream>>>(djobs, dfirst,
+                                                                               (int)jobs.size());
+        NBG_LAUNCHED(1);
+        if (cudaGetLastError() != cudaSuccess) rc = NBG_ERR_CUDA;
+    }
+    // the job table is read by the kernel: return it to the cache only after
+    if (cudaStreamSynchronize(stream) != cudaSuccess && !rc) rc = NBG_ERR_CUDA;
+    if (djobs) ctx_free(ctx, djobs, jb);
+    if (dfirst) ctx_free(ctx, dfirst, fb);
+    return rc;
 }
 
 // ---------------------------------------------------------------------------
@@ -1193,15 +1250,17 @@ int launch_select_sample(Context* ctx, const QueryLaunch& ql, uint64_t stride, u
 }
 
 int launch_select_queue(Context* ctx, int K, const BatchJob* jobs, int njobs, uint64_t items,
-                        unsigned long long* head, cudaStream_t stream) {
-    return dispatch_slots<QueueLauncher>(K, QueueArgs{jobs, njobs, items, head, ctx->sm_count, stream});
+                        unsigned long long* head, cudaStream_t stream, int reserve) {
+    return dispatch_slots<QueueLauncher>(
+        K, QueueArgs{jobs, njobs, items, head, ctx->sm_count, stream, reserve});
 }
 
 int launch_finish_queue(Context* ctx, const BatchJob* jobs, int njobs, uint64_t items,
-                        unsigned long long* head, cudaStream_t stream) {
+                        unsigned long long* head, cudaStream_t stream, int reserve) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_finish_queue_kernel, 128, 0);
-    const uint64_t grid = std::min<uint64_t>(items, (uint64_t)ctx->sm_count * std::max(per_sm, 1));
+    const uint64_t grid =
+        std::min<uint64_t>(items, (uint64_t)ctx->sm_count * std::max(per_sm - reserve, 1));
     if (!grid) return NBG_OK;
     knn_finish_queue_kernel<<<(unsigned)grid, 128, 0, stream>>>(jobs, njobs, items, head);
     NBG_LAUNCHED(1);
