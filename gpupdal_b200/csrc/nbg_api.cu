@@ -23,8 +23,14 @@ namespace nbg {
 
 int slots_for_k(int K);
 
+void set_err(Context* c, const std::string& msg) {
+    if (!c) return;
+    std::lock_guard<std::mutex> lock(c->emu);
+    c->err = msg;
+}
+
 int fail(Context* c, int code, const std::string& msg) {
-    if (c) c->err = msg;
+    set_err(c, msg);
     return code;
 }
 
@@ -52,11 +58,16 @@ static size_t size_class(size_t bytes) {
     return ((bytes + step - 1) / step) * step;
 }
 
-void ctx_trim(Context* ctx) {
+static void trim_locked(Context* ctx) {
     for (auto& kv : ctx->cache) cudaFree(kv.second);
     ctx->used -= std::min<uint64_t>(ctx->used, ctx->cached);
     ctx->cache.clear();
     ctx->cached = 0;
+}
+
+void ctx_trim(Context* ctx) {
+    std::lock_guard<std::mutex> lock(ctx->amu);
+    trim_locked(ctx);
 }
 
 // Device allocation through the context's cache: the smallest cached block
@@ -64,6 +75,7 @@ void ctx_trim(Context* ctx) {
 // calls of varying sizes (a request stream) recycle their blocks.
 int ctx_alloc(Context* ctx, void** p, size_t bytes) {
     bytes = size_class(bytes);
+    std::lock_guard<std::mutex> lock(ctx->amu);
     auto it = ctx->cache.lower_bound(bytes);
     if (it != ctx->cache.end() && it->first <= 2 * bytes) {
         *p = it->second;
@@ -72,13 +84,13 @@ int ctx_alloc(Context* ctx, void** p, size_t bytes) {
         ctx->cache.erase(it);
         return NBG_OK;
     }
-    if (ctx->budget && ctx->used + bytes > ctx->budget) ctx_trim(ctx);
+    if (ctx->budget && ctx->used + bytes > ctx->budget) trim_locked(ctx);
     if (ctx->budget && ctx->used + bytes > ctx->budget)
         return fail(ctx, NBG_ERR_BUDGET, "HBM budget exceeded");
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        ctx_trim(ctx);
+        trim_locked(ctx);
         e = cudaMalloc(p, bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -93,6 +105,7 @@ int ctx_alloc(Context* ctx, void** p, size_t bytes) {
 
 void ctx_free(Context* ctx, void* p, size_t bytes) {
     if (!p) return;
+    std::lock_guard<std::mutex> lock(ctx->amu);
     auto it = ctx->live.find(p);
     if (it != ctx->live.end()) {
         bytes = it->second;
@@ -275,7 +288,7 @@ namespace nbg {
 // Grows the cell table (cstart, cursor) and the scan storage to `entries`.
 int grid_grow_table(Context* ctx, Tile* t, uint64_t entries) {
     if (t->fixed_storage) {
-        ctx->err = "cell table exceeds the fixed storage";
+        set_err(ctx, "cell table exceeds the fixed storage");
         return NBG_ERR_UNSUPPORTED;
     }
     const uint64_t cap = std::max<uint64_t>(entries, 2 * t->table_cap);
@@ -399,7 +412,11 @@ int nbg_destroy(nbg_context* h) {
     return NBG_OK;
 }
 
-const char* nbg_last_error(const nbg_context* h) { return h ? h->c.err.c_str() : "no context"; }
+const char* nbg_last_error(const nbg_context* h) {
+    if (!h) return "no context";
+    std::lock_guard<std::mutex> lock(const_cast<nbg_context*>(h)->c.emu);
+    return h->c.err.c_str();
+}
 
 uint64_t nbg_tile_size(const nbg_tile* t) { return t ? t->t.n : 0; }
 

@@ -30,7 +30,9 @@ struct Context {
     uint64_t budget = 0;   // HBM budget in bytes (0 = no limit)
     uint64_t used = 0;     // bytes held by tiles and scratch
     std::string err;
-    std::mutex mu;
+    std::mutex mu;   // held by every entry point that takes the context
+    std::mutex amu;  // the block cache below (the batched form's KD helper thread allocates too)
+    std::mutex emu;  // err
     // per-call scratch (grown on demand)
     uint32_t* exact_rows = nullptr;
     uint64_t exact_cap = 0;
@@ -114,7 +116,10 @@ int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream);
 // Grid for neighbour count k1 (or a fixed cell edge), rebuilt only when needed.
 int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream, int32_t cell = 0);
 int build_grid_async(Context* ctx, Tile* t, int k1, cudaStream_t stream);
+
 int fail(Context* c, int code, const std::string& msg);
+// Sets the context's error message (thread-safe).
+void set_err(Context* c, const std::string& msg);
 int validate_stages(Context* ctx, const nbg_stage_opts* stages, int n_stages,
                     const nbg_columns* outputs, bool* need_aux);
 void fill_stage(StageDev& d, const nbg_stage_opts& o, const nbg_columns& c);

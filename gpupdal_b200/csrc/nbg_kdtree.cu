@@ -1046,7 +1046,7 @@ static int kd_tiles(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, u
     uint32_t total = 0;
     cudaMemcpyAsync(&total, kd->nt + S, 4, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
-        ctx->err = "KD tile scan failed";
+        set_err(ctx, "KD tile scan failed");
         return NBG_ERR_CUDA;
     }
     if (total + 1 > kd->tile_cap) {
@@ -1137,12 +1137,12 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
                                                          kd->rz + b, kd->rid + b);
         // root: the tile's actual bounding box, as calculateBounds
         const GridParams& g = t->host_gp;
+        const int32_t mn[3] = {g.minx, g.miny, g.minz}, mx[3] = {g.maxx, g.maxy, g.maxz};
         KdSeg root;
         root.begin = (uint32_t)b;
         root.end = (uint32_t)(b + n);
         root.node = k;
         root.pad = k;
-        const int32_t mn[3] = {g.minx, g.miny, g.minz}, mx[3] = {g.maxx, g.maxy, g.maxz};
         for (int d = 0; d < 3; ++d) {
             root.lo[d] = (double)mn[d] * t->tf.scale[d] + t->tf.offset[d];
             root.hi[d] = (double)mx[d] * t->tf.scale[d] + t->tf.offset[d];
@@ -1158,7 +1158,7 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
     }
     NBG_LAUNCHED(T);
     if (level0.size() > kd->seg_cap || small0.size() > kd->seg_cap || leaves0.size() > kd->leaf_cap) {
-        ctx->err = "KD replica: too many trees for the segment lists";
+        set_err(ctx, "KD replica: too many trees for the segment lists");
         return NBG_ERR_UNSUPPORTED;
     }
     // root nodes 0..T-1 (host arrays outlive the copies: the stream is synchronised below)
@@ -1178,7 +1178,7 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
     uint32_t cnt[5] = {0, (uint32_t)T, 0, (uint32_t)small0.size(), (uint32_t)leaves0.size()};
     cudaMemcpyAsync(kd->counters, cnt, sizeof(cnt), cudaMemcpyHostToDevice, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
-        ctx->err = "KD replica init failed";
+        set_err(ctx, "KD replica init failed");
         return NBG_ERR_CUDA;
     }
     uint32_t node_count = (uint32_t)T;
@@ -1211,7 +1211,7 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
         uint32_t S2 = 0;
         cudaMemcpyAsync(&S2, kd->counters + 5, 4, cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) {
-            ctx->err = "KD replica pass-2 plan failed";
+            set_err(ctx, "KD replica pass-2 plan failed");
             return NBG_ERR_CUDA;
         }
         NBG_LAUNCHED(1);
@@ -1233,11 +1233,11 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
         cudaError_t be = cudaGetLastError();
         if (be == cudaSuccess) be = cudaStreamSynchronize(st);
         if (be != cudaSuccess) {
-            ctx->err = std::string("KD replica build failed: ") + cudaGetErrorString(be);
+            set_err(ctx, std::string("KD replica build failed: ") + cudaGetErrorString(be));
             return NBG_ERR_CUDA;
         }
         if (cnt[2]) {
-            ctx->err = "KD replica build ran out of node or segment capacity";
+            set_err(ctx, "KD replica build ran out of node or segment capacity");
             return NBG_ERR_UNSUPPORTED;
         }
         node_count = cnt[1];
@@ -1263,7 +1263,7 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
     cudaError_t we = cudaGetLastError();
     if (we == cudaSuccess) we = cudaStreamSynchronize(st);
     if (we != cudaSuccess) {
-        ctx->err = std::string("KD replica subtree build failed: ") + cudaGetErrorString(we);
+        set_err(ctx, std::string("KD replica subtree build failed: ") + cudaGetErrorString(we));
         return NBG_ERR_CUDA;
     }
     if (cnt[2]) return KD_RETRY;
@@ -1291,7 +1291,7 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
                                                                       kd->npts[k], kd->kpos);
     NBG_LAUNCHED(1 + T + (nleaves ? 1 : 0));
     if (cudaStreamSynchronize(st) != cudaSuccess) {
-        ctx->err = "KD replica extents failed";
+        set_err(ctx, "KD replica extents failed");
         return NBG_ERR_CUDA;
     }
     return NBG_OK;
@@ -1315,7 +1315,7 @@ int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t st)
     }
     if (n >= (1ull << 32) - 1) {
         delete kd;
-        ctx->err = "KD replica: more than 2^32 points in one forest";
+        set_err(ctx, "KD replica: more than 2^32 points in one forest");
         return NBG_ERR_UNSUPPORTED;
     }
     kd->n = n;
@@ -1357,7 +1357,7 @@ int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t st)
             rc = kd_grow_nodes(ctx, kd, (uint32_t)std::min<uint64_t>(2 * n + 64 + 2 * (uint64_t)T, UINT32_MAX), st);
             if (!rc) rc = kd_build(ctx, kd, todo.data(), 0, st);
             if (rc == KD_RETRY) {
-                ctx->err = "KD replica build ran out of node capacity";
+                set_err(ctx, "KD replica build ran out of node capacity");
                 rc = NBG_ERR_UNSUPPORTED;
             }
         }
@@ -1448,11 +1448,11 @@ static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, ui
     if (le == cudaSuccess) le = cudaMemcpyAsync(&err, kd->counters + 2, 4, cudaMemcpyDeviceToHost, st);
     if (le == cudaSuccess) le = cudaStreamSynchronize(st);
     if (le != cudaSuccess) {
-        ctx->err = std::string("exact KD rows: ") + cudaGetErrorString(le);
+        set_err(ctx, std::string("exact KD rows: ") + cudaGetErrorString(le));
         return NBG_ERR_CUDA;
     }
     if (err) {
-        ctx->err = "KD search stack overflow";
+        set_err(ctx, "KD search stack overflow");
         return NBG_ERR_UNSUPPORTED;
     }
     return NBG_OK;
@@ -1472,7 +1472,7 @@ int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const Excep
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
-            ctx->err = std::string("exact KD finish: ") + cudaGetErrorString(e);
+            set_err(ctx, std::string("exact KD finish: ") + cudaGetErrorString(e));
             rc = NBG_ERR_CUDA;
         }
     }
@@ -1493,7 +1493,7 @@ int kd_list_rows(Context* ctx, Tile* t, int K, const ListArgs& L, const Exceptio
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
-            ctx->err = std::string("exact KD list: ") + cudaGetErrorString(e);
+            set_err(ctx, std::string("exact KD list: ") + cudaGetErrorString(e));
             rc = NBG_ERR_CUDA;
         }
     }
@@ -1514,7 +1514,7 @@ int kd_neighbor_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, uint32_
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
-            ctx->err = std::string("exact KD ids: ") + cudaGetErrorString(e);
+            set_err(ctx, std::string("exact KD ids: ") + cudaGetErrorString(e));
             rc = NBG_ERR_CUDA;
         }
     }

@@ -64,9 +64,10 @@ extern "C" uint64_t nbg_request_bytes(const nbg_request* r) {
     // query scratch (row sums, tie and replay lists), KD replica (point order,
     // inverse, partition scratch, nodes), plus host-output staging per dim
     uint64_t dims = 0, extra = 0;
-    if (r->n_stages > 0 && (!r->stages || !r->outputs)) return 0;
+    if (r->n_stages > 0 && !r->outputs) return 0;
     for (int s = 0; s < r->n_stages; ++s) {
         dims += (uint64_t)r->outputs[s].ndims;
+        if (!r->stages) continue;
         const nbg_stage_opts& o = r->stages[s];
         // lof keeps its ordered lists (ids and distances) and two row arrays;
         // the outlier stages a row value and a flag per point

@@ -7,6 +7,7 @@ library; a missing library raises instead of falling back to the CPU.
 from __future__ import annotations
 
 import ctypes
+import threading
 
 import numpy as np
 
@@ -65,7 +66,16 @@ class Context:
             raise NbgError(rc, "nbg_create failed (no sm_100 device?)")
         self.h = h
         self.device = device
-        self._exc_buf = {}
+        self._tls = threading.local()
+
+    def _exceptions(self, cap):
+        """This thread's row-exception buffer of `cap` records (a context may
+        be shared by threads; each reads its own call's exceptions)."""
+        buf = getattr(self._tls, "exc", None)
+        if buf is None or len(buf) != cap:
+            buf = (abi.RowException * cap)()
+            self._tls.exc = buf
+        return buf
 
     def close(self):
         if getattr(self, "h", None):
@@ -138,10 +148,7 @@ class Context:
             for d in range(nd):
                 c.offset[d] = d * n * 8
         cap = exception_capacity if exception_capacity is not None else max(1024, n)
-        exc = self._exc_buf.get(cap)
-        if exc is None:
-            exc = (abi.RowException * cap)()
-            self._exc_buf = {cap: exc}
+        exc = self._exceptions(cap)
         nexc = ctypes.c_uint32(0)
         stats = abi.RunStats()
         kp = rp = None
@@ -169,10 +176,7 @@ class Context:
         opts = (abi.StageOpts * max(ns, 1))(*stages)
         cols = (abi.Columns * max(ns, 1))(*columns)
         cap = exception_capacity
-        exc = self._exc_buf.get(cap)
-        if exc is None:
-            exc = (abi.RowException * cap)()
-            self._exc_buf = {cap: exc}
+        exc = self._exceptions(cap)
         nexc = ctypes.c_uint32(0)
         stats = abi.RunStats()
         kp = None if optimal_knn is None else _dptr(optimal_knn)
@@ -390,7 +394,9 @@ class Server:
         cols = (abi.Columns * len(stages))()
         for i, st in enumerate(stages):
             cols[i].ndims = len(abi.stage_dims(st))
+        opts = (abi.StageOpts * len(stages))(*stages)
         r.outputs = cols
+        r.stages = opts
         return int(self.lib.nbg_request_bytes(ctypes.byref(r)))
 
     def wait(self, ticket, timeout_ms=-1):
