@@ -142,9 +142,24 @@ def stages(knn):
             abi.make_opts(abi.STAGE_NORMAL, knn=knn, always_up=True)]
 
 
-def cpu_reference(x, y, z, knn, sample, kind=None):
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_reference(x, y, z, knn, sample, kind=None, single_thread=False):
     """Times the reference's CPU path (KD build + eigenvalues + normal) on a
-    spatially contiguous window of `sample` points; all host threads."""
+    spatially contiguous window of `sample` points: all host threads for the
+    rows in fixed contiguous chunks, and the KD build on min(8, cores)
+    threads.  With `single_thread`, also one thread for both (the stage's
+    own semantics: one thread per view) on a window of a quarter of the
+    points."""
     from gpupdal_b200 import synthetic as syn
     from oracle import oracle as orc
     if kind is None:
@@ -152,22 +167,40 @@ def cpu_reference(x, y, z, knn, sample, kind=None):
     if not orc.available(kind):
         orc.build()
     o = orc.Oracle(kind)
-    # square window from the tile's corner holding about `sample` points
-    frac = min(1.0, sample / len(x))
-    side = int(round(50000 * np.sqrt(frac)))
-    m = (x < side) & (y < side)
-    xs, ys, zs = x[m], y[m], z[m]
+
+    def window(count):
+        # square window from the tile's corner holding about `count` points
+        side = int(round(50000 * np.sqrt(min(1.0, count / len(x)))))
+        m = (x < side) & (y < side)
+        return side, tuple(syn.to_double(v[m]) for v in (x, y, z))
+
+    def timed_run(xyz, threads):
+        t0 = time.perf_counter()
+        t = o.tree(*xyz, build_threads=threads if threads == 1 else 0)
+        for st in stages(knn):
+            t.run_stage(st, mode=0, threads=threads)
+        return time.perf_counter() - t0
+
     threads = os.cpu_count() or 1
-    t0 = time.perf_counter()
-    t = o.tree(*(syn.to_double(v) for v in (xs, ys, zs)))
-    for st in stages(knn):
-        t.run_stage(st, mode=0, threads=threads)
-    dt = time.perf_counter() - t0
-    return {"value": len(xs) / dt / 1e6, "unit": "Mpts/s", "cores": threads,
-            "kind": kind, "sample": f"{len(xs)}-point window ({side / 100:.0f} x "
-                                    f"{side / 100:.0f} m) of the same tile: KD build + "
-                                    f"eigenvalues + normal, {threads} threads",
-            "seconds": dt}
+    side, xyz = window(sample)
+    dt = timed_run(xyz, threads)
+    n = len(xyz[0])
+    out = {"value": n / dt / 1e6, "unit": "Mpts/s", "cores": threads,
+           "kind": kind, "sample": f"{n}-point window ({side / 100:.0f} x "
+                                   f"{side / 100:.0f} m) of the same tile: KD build "
+                                   f"(min(8, cores) threads) + eigenvalues + normal, "
+                                   f"{threads} threads",
+           "seconds": dt, "cpu_model": cpu_model(), "nproc": threads}
+    if single_thread:
+        side1, xyz1 = window(sample // 4)
+        dt1 = timed_run(xyz1, 1)
+        n1 = len(xyz1[0])
+        out["single_thread"] = {"value": n1 / dt1 / 1e6, "unit": "Mpts/s", "cores": 1,
+                                "seconds": dt1,
+                                "sample": f"{n1}-point window ({side1 / 100:.0f} x "
+                                          f"{side1 / 100:.0f} m): KD build + eigenvalues "
+                                          f"+ normal, one thread"}
+    return out
 
 
 def extras_cases():
@@ -423,7 +456,8 @@ def run_reference(args, ws, rank):
             "config": {"workload": f"stress tile {args.points} points (seed 2), eigenvalues "
                                    f"knn={args.knn} then normal knn={args.knn}",
                        "sample": base["sample"]},
-            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                  "cpu_model", "nproc")},
             "e2e": {"value": v, "unit": "Mpts/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -527,6 +561,7 @@ def main():
                    "points_per_gpu": n, "knn": args.knn, "form": "plain per-tile launch",
                    "l2": "inputs larger than L2 (tile 384 MB + sorted copy 512 MB per step)",
                    "tie_rows": int(last.tie_rows), "deferred_rows": int(last.deferred_rows),
+                   "resolved_rows": int(last.resolved_rows), "replay_rows": int(last.replay_rows),
                    "grid_ms": last.grid_ms, "query_ms": last.query_ms, "tree_ms": last.tree_ms},
         "e2e": {"value": e2e_value, "unit": "Mpts/s", "h2d_bytes_per_step": 12 * n,
                 "d2h_bytes_per_step": 8 * sum(nd) * n},
@@ -546,8 +581,9 @@ def main():
     if ws == 1 and not args.no_extras:
         line["extras"] = extras_leg(ctx, args)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cb = cpu_reference(x, y, z, args.knn, args.cpu_sample)
-        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cb = cpu_reference(x, y, z, args.knn, args.cpu_sample, single_thread=True)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                   "cpu_model", "nproc", "single_thread")}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -853,6 +853,11 @@ void* orc_tree_build(const double* x, const double* y, const double* z, uint64_t
     return h;
 }
 
+// the port's build is serial: the thread count changes nothing
+void* orc_tree_build_t(const double* x, const double* y, const double* z, uint64_t n, int) {
+    return orc_tree_build(x, y, z, n);
+}
+
 void orc_tree_free(void* h) { delete (OrcTree*)h; }
 
 // KD3ImplT::neighbors; writes min(n,k) ids, returns that count.

@@ -39,6 +39,8 @@ class Oracle:
         lib.orc_impl_name.restype = ctypes.c_char_p
         lib.orc_tree_build.argtypes = [dp, dp, dp, u64]
         lib.orc_tree_build.restype = vp
+        lib.orc_tree_build_t.argtypes = [dp, dp, dp, u64, ctypes.c_int]
+        lib.orc_tree_build_t.restype = vp
         lib.orc_tree_free.argtypes = [vp]
         lib.orc_tree_neighbors.argtypes = [vp, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_double, u64, u64,
@@ -56,8 +58,9 @@ class Oracle:
         lib.orc_run_stage.restype = ctypes.c_int
         self.lib = lib
 
-    def tree(self, x, y, z) -> "Tree":
-        return Tree(self, x, y, z)
+    def tree(self, x, y, z, build_threads=0) -> "Tree":
+        """build_threads 0 leaves the KD build its own thread count."""
+        return Tree(self, x, y, z, build_threads)
 
     def eigen_chain(self, a):
         a = np.ascontiguousarray(a, dtype=np.float64).reshape(9)
@@ -72,15 +75,15 @@ class Oracle:
 class Tree:
     """A KD3-style index over double coordinates (x, y, z in metres)."""
 
-    def __init__(self, orc: Oracle, x, y, z):
+    def __init__(self, orc: Oracle, x, y, z, build_threads=0):
         self.orc = orc
         self.x = np.ascontiguousarray(x, dtype=np.float64)
         self.y = np.ascontiguousarray(y, dtype=np.float64)
         self.z = np.ascontiguousarray(z, dtype=np.float64)
         self.n = len(self.x)
         dp = ctypes.POINTER(ctypes.c_double)
-        self.h = orc.lib.orc_tree_build(self.x.ctypes.data_as(dp), self.y.ctypes.data_as(dp),
-                                        self.z.ctypes.data_as(dp), self.n)
+        self.h = orc.lib.orc_tree_build_t(self.x.ctypes.data_as(dp), self.y.ctypes.data_as(dp),
+                                          self.z.ctypes.data_as(dp), self.n, int(build_threads))
 
     def __del__(self):
         h = getattr(self, "h", None)

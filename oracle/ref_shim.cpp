@@ -348,15 +348,22 @@ extern "C" {
 
 const char* orc_impl_name(void) { return "reference"; }
 
-void* orc_tree_build(const double* x, const double* y, const double* z, uint64_t n) {
+// build_threads 0: the KD3 build's own choice, up to eight threads (the
+// threaded build yields the serial tree); n > 0 caps it at n threads
+void* orc_tree_build_t(const double* x, const double* y, const double* z, uint64_t n,
+                       int build_threads) {
     RefTree* t = new RefTree();
     t->cloud.pts.resize(n);
     for (uint64_t i = 0; i < n; ++i) t->cloud.pts[i] = {x[i], y[i], z[i]};
-    // the KD3 build uses up to eight threads and yields the serial tree
     int threads = n < 256 ? 1 : (int)std::min<unsigned>(8u, std::max(1u, std::thread::hardware_concurrency()));
+    if (build_threads > 0) threads = std::min(threads, build_threads);
     t->index.set_build_threads(threads);
     t->index.buildIndex();
     return t;
+}
+
+void* orc_tree_build(const double* x, const double* y, const double* z, uint64_t n) {
+    return orc_tree_build_t(x, y, z, n, 0);
 }
 
 void orc_tree_free(void* h) { delete (RefTree*)h; }

@@ -2,8 +2,10 @@
 
     python tests/golden/make_golden.py
 
-Inputs are seeded windows of the benchmark workloads plus small tie-heavy and
-edge-case clouds.  Outputs come from oracle/_ref/libnbg_ref.so, i.e. the
+Inputs are seeded windows of the benchmark workloads, small tie-heavy and
+edge-case clouds, and two of the reference's own test fixtures (read where they
+lie in the reference tree, NBG_REFERENCE, default /root/reference): the fork's
+tie / duplicate points and the simple.las tile.  Outputs come from oracle/_ref/libnbg_ref.so, i.e. the
 reference's own vendored nanoflann 1.3.1 and Eigen 3.4 compiled here (see
 oracle/Makefile); this script must run where that library was built.  Each
 fixture stores raw int32 coordinates (scale 0.01, offset 0), the
@@ -39,7 +41,10 @@ def stage_set(kind_list):
     return out
 
 
-def record(ref, name, x, y, z, knns, stages, kopt=None, ropt=None):
+REF = os.environ.get("NBG_REFERENCE", "/root/reference")
+
+
+def record(ref, name, x, y, z, knns, stages, kopt=None, ropt=None, extra=None):
     X, Y, Z = (syn.to_double(v) for v in (x, y, z))
     t = ref.tree(X, Y, Z)
     data = dict(x=x.astype(np.int32), y=y.astype(np.int32), z=z.astype(np.int32))
@@ -53,6 +58,8 @@ def record(ref, name, x, y, z, knns, stages, kopt=None, ropt=None):
     if kopt is not None:
         data["optimal_knn"] = kopt
         data["optimal_radius"] = ropt
+    if extra:
+        data.update(extra)
     path = os.path.join(OUT, f"{name}.npz")
     np.savez_compressed(path, **data)
     print(path, len(x), os.path.getsize(path))
@@ -111,6 +118,31 @@ def main():
         "dups": ([5] * 12 + [7], [5] * 12 + [9], [1] * 12 + [2]),
         "line45": (list(range(0, 2000, 100)), list(range(0, 2000, 100)), [0] * 20),
     }
+    # the fork's own tie / duplicate fixture (test/data/pdg/neighborhood-points.csv,
+    # metres, read as raw = 100 * value at scale 0.01) with the stages of its
+    # deterministic-ties pipeline (test/data/pdg/hybrid-neighborhood-deterministic-ties.json)
+    pts = np.loadtxt(os.path.join(REF, "test/data/pdg/neighborhood-points.csv"), delimiter=",",
+                     skiprows=1)[:, :3]
+    raw = np.rint(pts * 100).astype(np.int32)
+    record(ref, "fork_neighborhood_points", raw[:, 0], raw[:, 1], raw[:, 2], [1, 2, 3, 7],
+           [("normal3free", A.make_opts(A.STAGE_NORMAL, knn=3, always_up=False)),
+            ("eig3n", A.make_opts(A.STAGE_EIGENVALUES, knn=3, normalize=True)),
+            ("cov3", A.make_opts(A.STAGE_COVARIANCEFEATURES, knn=3,
+                                 feature_mask=A.FEAT_ALL & ~A.FEAT_BIT["Density"]))])
+    # a real LAS tile, the reference's test/data/las/simple.las (LAS 1.2, point
+    # format 3, scale 0.01, offset -0): its raw X/Y/Z, and its header block and
+    # point records for the LAS ingest tests
+    from gpupdal_b200 import las
+    lf = las.LasFile(os.path.join(REF, "test/data/las/simple.las"))
+    assert lf.scale == (0.01, 0.01, 0.01) and all(o == 0 for o in lf.offset)
+    lx, ly, lz = lf.raw_xyz()
+    hdr = np.asarray(lf.map[:lf.info["offset_to_points"]]).copy()
+    record(ref, "las_simple", lx, ly, lz, [8, 16],
+           [("normal8", A.make_opts(A.STAGE_NORMAL, knn=8)),
+            ("eig16", A.make_opts(A.STAGE_EIGENVALUES, knn=16)),
+            ("cov10", A.make_opts(A.STAGE_COVARIANCEFEATURES, knn=10,
+                                  feature_mask=A.FEAT_ALL & ~A.FEAT_BIT["Density"]))],
+           extra={"las_header": hdr, "las_records": np.asarray(lf.records).copy()})
     for cname, (cx, cy, cz) in cases.items():
         cx, cy, cz = (np.array(v, dtype=np.int32) for v in (cx, cy, cz))
         record(ref, f"edge_{cname}", cx, cy, cz, [3, 8],

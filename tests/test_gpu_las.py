@@ -92,3 +92,27 @@ def test_las_rejects_short_records(nbg):
     rc = nbg.lib.nbg_tile_upload_las(nbg.h, buf.ctypes.data, 4, 11, 0, sc, sc, None,
                                      ctypes.byref(h))
     assert rc == abi.NBG_ERR_INVALID and not h.value
+
+
+def test_reference_las_fixture_matches_reference_outputs(nbg, tmp_path):
+    # the reference's simple.las through LAS ingest: neighbour sets bit-exact
+    # against the reference's, and stage outputs identical to the array tile's
+    # (which the golden parity tests hold to the reference's own outputs)
+    g = U.golden("las_simple")
+    p = tmp_path / "simple.las"
+    p.write_bytes(g["las_header"].tobytes() + g["las_records"].tobytes())
+    t = nbg.tile_from_las(las.LasFile(p))
+    t_arr = nbg.tile(g["x"], g["y"], g["z"])
+    assert t.n == 1065
+    for k in (8, 16):
+        ids, _ = nbg.neighbor_sets(t, k)
+        assert np.array_equal(U.sorted_rows(ids), U.sorted_rows(g[f"nbr_k{k}"]))
+    stages = [U.opts_from_bytes(g[f"{s}_opts"]) for s in ("normal8", "eig16", "cov10")]
+    got, ex, _ = nbg.run(t, stages)
+    want, want_ex, _ = nbg.run(t_arr, stages)
+    for i, (a, b) in enumerate(zip(got, want)):
+        assert np.array_equal(a, b, equal_nan=True)
+        assert np.array_equal(U.status_from_exceptions(t.n, ex, i), g[[
+            "normal8_status", "eig16_status", "cov10_status"][i]])
+    assert np.array_equal(np.sort(ex, order=["stage", "point_id"]),
+                          np.sort(want_ex, order=["stage", "point_id"]))

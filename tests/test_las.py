@@ -80,3 +80,22 @@ def test_compressed_and_truncated_files(tmp_path):
     t.write_bytes(bytes(raw[:-5]))
     with pytest.raises(las.LasError, match="exceed"):
         las.LasFile(t)
+
+
+def test_reference_las_fixture(tmp_path):
+    # the reference's test/data/las/simple.las (LAS 1.2, format 3), stored as
+    # its header block and point records: the header fields, and the raw
+    # X/Y/Z the golden outputs were made from
+    from tests import _util as U
+    g = U.golden("las_simple")
+    p = tmp_path / "simple.las"
+    p.write_bytes(g["las_header"].tobytes() + g["las_records"].tobytes())
+    f = las.LasFile(p)
+    h = f.info
+    assert (h["version_major"], h["version_minor"], h["point_format"]) == (1, 2, 3)
+    assert h["point_record_length"] == 34 and h["point_count"] == 1065
+    assert f.scale == (0.01, 0.01, 0.01) and all(o == 0 for o in f.offset)
+    rx, ry, rz = f.raw_xyz()
+    assert np.array_equal(rx, g["x"]) and np.array_equal(ry, g["y"]) and np.array_equal(rz, g["z"])
+    assert h["min"][0] == pytest.approx(g["x"].min() * 0.01)
+    assert h["max"][1] == pytest.approx(g["y"].max() * 0.01)
