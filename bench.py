@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--knn", type=int, default=16)
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true",
+                    help="skip the plain FP64 eigensolve comparison leg")
     ap.add_argument("--served-requests", type=int, default=64)
     ap.add_argument("--served-rate", type=float, default=20.0)
     ap.add_argument("--served-slots", type=int, default=4)
@@ -203,6 +205,56 @@ def cpu_reference(x, y, z, knn, sample, kind=None, single_thread=False):
     return out
 
 
+def fp64_leg(ctx, args, dxyz, drec, sts, steps):
+    """The main workload with every row solved by the FP64 Eigen chain alone
+    (eigen_fp64: a plain FP64 eigensolve) against the FP32 Jacobi + FP64
+    polish path whose outputs `drec` holds: device time per step, and the
+    largest difference of the two outputs (eigenvalues relative to the row's
+    largest, normals on rows whose relative eigen-gap is at least 1e-4)."""
+    import ctypes
+    import torch
+    from gpupdal_b200.native import record_columns
+    s64 = []
+    for o in sts:
+        c = type(o)()
+        ctypes.memmove(ctypes.addressof(c), ctypes.addressof(o), ctypes.sizeof(o))
+        c.eigen_fp64 = 1
+        s64.append(c)
+    n = drec.shape[0]
+    rec64 = torch.empty_like(drec)
+    cols64 = record_columns(rec64.data_ptr(), s64, 64, 1)
+
+    def step():
+        tile = ctx.tile(*dxyz)
+        ex, st = ctx.run_columns(tile, s64, cols64)
+        tile.free()
+        return st
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        st = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    lam, lam64 = drec[:, 0:3], rec64[:, 0:3]
+    lmax = lam.abs().amax(dim=1).clamp_min(1e-300)
+    ok = torch.isfinite(lam).all(dim=1) & torch.isfinite(lam64).all(dim=1)
+    dl = ((lam - lam64).abs().amax(dim=1) / lmax)[ok]
+    gap = ((lam[:, 1] - lam[:, 0]) / lmax) >= 1e-4
+    nv, nv64 = drec[:, 3:6], rec64[:, 3:6]
+    okn = ok & gap & torch.isfinite(nv).all(dim=1) & torch.isfinite(nv64).all(dim=1)
+    dn = (nv - nv64).abs().amax(dim=1)[okn]
+    return {"ms_per_step": ms, "value": n / (ms / 1e3) / 1e6, "unit": "Mpts/s",
+            "resolved_rows": int(st.resolved_rows),
+            "max_rel_diff_eigenvalues": float(dl.max()) if dl.numel() else 0.0,
+            "max_abs_diff_normal": float(dn.max()) if dn.numel() else 0.0,
+            "rows_compared": int(ok.sum()), "normal_rows_compared": int(okn.sum())}
+
+
 def extras_cases():
     """The stage options beyond the main path (radius, stride, optimized) and
     the other consumers of the index, each as one stage on the 4M mixture."""
@@ -285,10 +337,11 @@ def extras_leg(ctx, args):
         except Exception as exc:  # recorded, not fatal to the main line
             e = {"error": str(exc)}
         out[label] = e
-    # LAS ingest: point format 6 records (30 bytes), host-mapped and device-resident
+    # LAS ingest: point format 7 records (36 bytes, scale 0.01), host-mapped and
+    # device-resident
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, "tile.las")
-        las.write_las(path, x, y, z, version=(1, 4), point_format=6)
+        las.write_las(path, x, y, z, version=(1, 4), point_format=7)
         f = las.LasFile(path)
         rec = np.ascontiguousarray(f.records)
         drec = torch.from_numpy(rec).to(dev)
@@ -551,6 +604,11 @@ def main():
     ms_e2e = max_over_ranks(ms_e2e)
     e2e_value = ws * n / (ms_e2e / args.steps / 1e3) / 1e6
     last = stats[-1]
+    fp64 = None
+    if ws == 1 and not args.no_fp64:
+        step_device()  # drec: the FP32 + FP64-polish outputs
+        fp64 = fp64_leg(ctx, args, (dx, dy, dz), drec, sts, args.steps)
+        fp64["speedup_of_default"] = fp64["ms_per_step"] / per_step
     line = {
         "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step,
@@ -574,6 +632,8 @@ def main():
                      "bytes_per_point": BYTES_PER_POINT},
         "clocks": clk,
     }
+    if fp64 is not None:
+        line["eigen_fp64"] = fp64
     if ws == 1 and not args.no_batched:
         line["batched"] = batched_leg(ctx, args)
     if ws == 1 and not args.no_served:

@@ -96,7 +96,7 @@ class StageOpts(ctypes.Structure):
         ("thresh1", ctypes.c_double),
         ("thresh2", ctypes.c_double),
         ("label", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("eigen_fp64", ctypes.c_int32),
     ]
 
 
@@ -220,7 +220,7 @@ def stage_dims(opts: StageOpts) -> list:
 def make_opts(kind, knn=8, always_up=True, viewpoint=None, refine=False,
               normalize=False, feature_mask=FEAT_DIMENSIONALITY, mode=MODE_SQRT,
               stride=1, optimized=False, radius=None, min_k=3, thresh1=0.0, thresh2=0.0,
-              label=0) -> StageOpts:
+              label=0, eigen_fp64=False) -> StageOpts:
     o = StageOpts()
     o.kind = int(kind)
     o.knn = int(knn)
@@ -241,6 +241,7 @@ def make_opts(kind, knn=8, always_up=True, viewpoint=None, refine=False,
     o.thresh1 = float(thresh1)
     o.thresh2 = float(thresh2)
     o.label = int(label)
+    o.eigen_fp64 = int(bool(eigen_fp64))
     return o
 
 

@@ -911,7 +911,8 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             const nbg_stage_opts& o = stages[s];
             g.stage_index[i] = s;
             fill_stage(g.st[i], o, dcols[s]);
-            if (o.kind == NBG_STAGE_NORMAL && !o.always_up && !o.has_viewpoint) g.sign_exact = 1;
+            if ((o.kind == NBG_STAGE_NORMAL && !o.always_up && !o.has_viewpoint) || o.eigen_fp64)
+                g.sign_exact = 1;
         }
         g.resolve_count = ctx->counters + 5;
         if (cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(uint32_t), stream) ||

@@ -157,7 +157,8 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
             g.stage_index[s] = s;
             fill_stage(g.st[s], it.stages[s], it.outputs[s]);
             const nbg_stage_opts& o = it.stages[s];
-            if (o.kind == NBG_STAGE_NORMAL && !o.always_up && !o.has_viewpoint) g.sign_exact = 1;
+            if ((o.kind == NBG_STAGE_NORMAL && !o.always_up && !o.has_viewpoint) || o.eigen_fp64)
+                g.sign_exact = 1;
         }
         live.push_back(i);
         rows += t->n;

@@ -52,7 +52,8 @@ struct StageDev {
 
 struct StageGroup {
     int32_t nstages;
-    int32_t sign_exact;  // a stage exposes the eigenvector sign: use the Eigen chain
+    int32_t sign_exact;  // a stage exposes the eigenvector sign, or asks for the plain
+                         // FP64 eigensolve: every row through the Eigen chain
     int32_t stage_index[NBG_MAX_STAGES];  // index in the caller's array
     StageDev st[NBG_MAX_STAGES];
     const double* optimal_knn;     // device, may be null

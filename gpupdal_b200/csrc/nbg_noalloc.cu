@@ -189,7 +189,8 @@ extern "C" int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32
     d.base = (char*)out->base;
     d.point_stride = out->point_stride;
     for (int k = 0; k < NBG_MAX_DIMS; ++k) d.offset[k] = out->offset[k];
-    g.sign_exact = opts->kind == NBG_STAGE_NORMAL && !opts->always_up && !opts->has_viewpoint;
+    g.sign_exact = (opts->kind == NBG_STAGE_NORMAL && !opts->always_up && !opts->has_viewpoint) ||
+                   opts->eigen_fp64;
     QueryLaunch ql;
     ql.tile = &t;
     ql.K = K;

@@ -143,7 +143,11 @@ typedef struct nbg_stage_opts {
                               thresh, outlier multiplier                     */
     double thresh2;        /* approximatecoplanar thresh2                    */
     int32_t label;         /* outlier: class written to outlier rows         */
-    int32_t reserved0;
+    int32_t eigen_fp64;    /* 1: every row of the stage's neighbourhood group
+                              is solved by the FP64 Eigen chain alone (a plain
+                              FP64 eigensolve); 0: FP32 Jacobi + FP64 polish,
+                              the chain only where the polish does not settle
+                              or a sign needs it.  Both meet the same bars.  */
 } nbg_stage_opts;
 
 /* Output placement: dimension d of point id is the double at

@@ -111,3 +111,37 @@ def test_error_statistics(nbg, port, tmp_path, name):
     os.makedirs(out_dir, exist_ok=True)
     with open(os.path.join(out_dir, f"accuracy_{name}.json"), "w") as f:
         json.dump(report, f, indent=1)
+
+
+def test_plain_fp64_eigensolve(nbg, port):
+    # eigen_fp64: every row through the FP64 Eigen chain alone.  Same bars
+    # against the FP64 oracle as the default FP32 Jacobi + FP64 polish path,
+    # no row counted as handed from the fast solver to the chain, and the
+    # eigenvalues of both forms agree to FP64 rounding.
+    x, y, z = syn.stress(2_000_000, 2)
+    m = (x < 20000) & (y < 20000)
+    x, y, z = x[m], y[m], z[m]
+    X, Y, Z = (syn.to_double(v) for v in (x, y, z))
+    tile = nbg.tile(x, y, z)
+    fast = [abi.make_opts(abi.STAGE_EIGENVALUES, knn=16),
+            abi.make_opts(abi.STAGE_NORMAL, knn=16),
+            abi.make_opts(abi.STAGE_COVARIANCEFEATURES, knn=10, feature_mask=abi.FEAT_ALL
+                          & ~abi.FEAT_DENSITY)]
+    plain = [abi.make_opts(abi.STAGE_EIGENVALUES, knn=16, eigen_fp64=True),
+             abi.make_opts(abi.STAGE_NORMAL, knn=16, eigen_fp64=True),
+             abi.make_opts(abi.STAGE_COVARIANCEFEATURES, knn=10, feature_mask=abi.FEAT_ALL
+                           & ~abi.FEAT_DENSITY, eigen_fp64=True)]
+    got_fast, ex_fast, _ = nbg.run(tile, fast)
+    got, ex, stats = nbg.run(tile, plain)
+    assert int(stats.resolved_rows) == 0
+    tree = port.tree(X, Y, Z)
+    for i, o in enumerate(plain):
+        lam, _ = tree.run_stage(abi.make_opts(abi.STAGE_EIGENVALUES, knn=o.knn), mode=1)
+        want, st = tree.run_stage(o, mode=1)
+        got_st = U.status_from_exceptions(len(x), ex, i)
+        assert np.array_equal(got_st, st)
+        assert np.array_equal(got_st, U.status_from_exceptions(len(x), ex_fast, i))
+        U.compare_stage(o, got[i], want, st, got_st, lam=lam, label=f"eigen_fp64/{i} vs f64")
+    ok = U.status_from_exceptions(len(x), ex, 0) == 0
+    lmax = np.abs(got_fast[0][:, ok]).max(axis=0)
+    assert np.all(np.abs(got[0][:, ok] - got_fast[0][:, ok]) <= 1e-12 * lmax)
