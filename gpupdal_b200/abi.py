@@ -134,6 +134,7 @@ class RunStats(ctypes.Structure):
         ("kd_build_ms", ctypes.c_double),
         ("outliers", ctypes.c_uint64),
         ("inliers", ctypes.c_uint64),
+        ("output_chunks", ctypes.c_uint64),
     ]
 
 

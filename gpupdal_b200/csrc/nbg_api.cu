@@ -687,6 +687,151 @@ struct HostOut {
     size_t bytes = 0;
 };
 
+// Host records of a plain kNN group copied back while the rows are still
+// being answered.  The rows are taken in `C` chunks of the point-id range
+// (each chunk's sorted positions in cell order).  Every chunk's select +
+// finish is queued on `stream` at once; the KD replica builds on the side
+// stream beside them (its build waits on the host, which has nothing else to
+// queue), and then, chunk by chunk as each one's queries complete, the side
+// stream orders and replays its tie rows and a copy stream copies its
+// records -- one contiguous byte range of the caller's pinned buffer -- back
+// while the later chunks are still being answered.  Every chunk has its own
+// counters, tie list and replay list (disjoint slices of the context's), so
+// chunks share no mutable state; the outputs equal the unchunked path's bit
+// for bit.
+struct PipeStats {
+    float query_ms = 0, tree_ms = 0, build_ms = 0;
+    uint64_t tie_rows = 0, deferred_rows = 0, replay_rows = 0;
+};
+
+static int run_pipelined(Context* ctx, Tile* t, int K, const StageGroup& g, const ExceptionSink& sink,
+                         const char* dev_records, char* host_records, size_t record_bytes, int C,
+                         cudaStream_t stream, PipeStats& ps) {
+    const uint64_t n = t->n;
+    // chunk c counts in counters[8c .. 8c+4]: at most four chunks stay below
+    // the word build_id_chunks writes (counters[48])
+    if (C < 1 || C > 4) return fail(ctx, NBG_ERR_INVALID, "pipeline chunk count");
+    uint64_t b[9];
+    for (int c = 0; c <= C; ++c) b[c] = n * (uint64_t)c / (uint64_t)C;
+    uint32_t* rows = nullptr;
+    int rc = ctx_alloc(ctx, (void**)&rows, n * 4);
+    if (rc) return rc;
+    cudaStream_t cs = nullptr;
+    cudaEvent_t sel[8] = {}, t0[8] = {}, t1[8] = {}, done = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    for (int c = 0; c < C && !e; ++c) {
+        e = cudaEventCreate(&sel[c]);
+        if (!e) e = cudaEventCreate(&t0[c]);
+        if (!e) e = cudaEventCreate(&t1[c]);
+    }
+    if (!e) e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+    if (e) rc = fail(ctx, NBG_ERR_CUDA, std::string("pipeline setup: ") + cudaGetErrorString(e));
+    if (!rc) rc = build_id_chunks(ctx, t, b, C, rows, ctx->counters + 48, stream);
+    const bool speculative = !(t->kd && kd_built(t));
+    auto finish_chunk = [&](int c) -> int {
+        const uint32_t rows_c = (uint32_t)(b[c + 1] - b[c]);
+        uint32_t* cnt_dev = ctx->counters + 8 * c;
+        uint32_t cnt[5] = {0, 0, 0, 0, 0};
+        cudaError_t e = cudaStreamWaitEvent(ctx->side, sel[c], 0);
+        if (!e) e = cudaMemcpyAsync(cnt, cnt_dev, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->side);
+        if (!e) e = cudaStreamSynchronize(ctx->side);
+        if (e) return fail(ctx, NBG_ERR_CUDA, std::string("query kernel: ") + cudaGetErrorString(e));
+        ps.tie_rows += cnt[1];
+        ps.deferred_rows += cnt[2];
+        cudaEventRecord(t0[c], ctx->side);
+        const uint32_t nties = std::min(cnt[4], rows_c);
+        if (nties) {
+            TieLaunch tl;
+            tl.tile = t;
+            tl.K = K;
+            tl.grp = g;
+            tl.ex = sink;
+            tl.ties = ctx->ties + b[c];
+            tl.nties = nties;
+            tl.kd = kd_order(t);
+            tl.exact_rows = ctx->exact_rows + b[c];
+            tl.counters = cnt_dev;
+            tl.ids_out = nullptr;
+            tl.row_k = nullptr;
+            int r = launch_ties(ctx, tl, ctx->side);
+            if (r) return fail(ctx, r, "tie-order resolver launch failed");
+            e = cudaMemcpyAsync(cnt, cnt_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->side);
+            if (!e) e = cudaStreamSynchronize(ctx->side);
+            if (e) return fail(ctx, NBG_ERR_CUDA, std::string("tie-order resolver: ") + cudaGetErrorString(e));
+        }
+        ps.replay_rows += cnt[0];
+        int r = kd_run_rows(ctx, t, K, g, sink, ctx->exact_rows + b[c], cnt[0], ctx->side, nullptr);
+        if (r) return r;
+        cudaEventRecord(t1[c], ctx->side);
+        e = cudaStreamWaitEvent(cs, t1[c], 0);
+        if (!e) e = cudaMemcpyAsync(host_records + b[c] * record_bytes, dev_records + b[c] * record_bytes,
+                                    rows_c * record_bytes, cudaMemcpyDeviceToHost, cs);
+        if (e) return fail(ctx, NBG_ERR_CUDA, std::string("output copy: ") + cudaGetErrorString(e));
+        return NBG_OK;
+    };
+    int launched = 0;
+    if (!rc && speculative) {
+        cudaEventRecord(ctx->xev[0], stream);
+        cudaStreamWaitEvent(ctx->side, ctx->xev[0], 0);
+    }
+    for (int c = 0; c < C && !rc; ++c) {
+        QueryLaunch ql;
+        ql.tile = t;
+        ql.K = K;
+        ql.rmax = 8;
+        ql.grp = g;
+        ql.ex = sink;
+        ql.exact_rows = ctx->exact_rows + b[c];
+        ql.counters = ctx->counters + 8 * c;
+        ql.ties = ctx->ties + b[c];
+        ql.tie_cap = (uint32_t)(b[c + 1] - b[c]);
+        ql.sums = ctx->sums;
+        ql.row_k = nullptr;
+        ql.rows = rows + b[c];
+        ql.nrows = b[c + 1] - b[c];
+        rc = launch_query(ctx, ql, stream);
+        if (rc) {
+            rc = fail(ctx, rc, std::string("query launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        cudaEventRecord(sel[c], stream);
+        ++launched;
+    }
+    if (!rc && speculative) {
+        // the KD replica (needed by the tie rows) builds beside the queries
+        cudaEventRecord(ctx->ev[8], ctx->side);
+        rc = kd_ensure(ctx, t, ctx->side);
+        cudaEventRecord(ctx->ev[9], ctx->side);
+    }
+    for (int c = 0; c < launched && !rc; ++c) rc = finish_chunk(c);
+    // every queued kernel and copy completes before the buffers are released
+    if (cs && done) {
+        cudaEventRecord(done, cs);
+        cudaStreamWaitEvent(stream, done, 0);
+    }
+    e = cudaStreamSynchronize(stream);
+    if (cs && !e) e = cudaStreamSynchronize(cs);
+    cudaError_t e2 = cudaStreamSynchronize(ctx->side);
+    if (!rc && (e || e2))
+        rc = fail(ctx, NBG_ERR_CUDA, std::string("pipelined query: ") + cudaGetErrorString(e ? e : e2));
+    if (!rc) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, ctx->ev[2], sel[C - 1]) == cudaSuccess) ps.query_ms += ms;
+        for (int c = 0; c < C; ++c)
+            if (cudaEventElapsedTime(&ms, t0[c], t1[c]) == cudaSuccess) ps.tree_ms += ms;
+        if (speculative && cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]) == cudaSuccess) ps.build_ms += ms;
+    }
+    for (int c = 0; c < C; ++c) {
+        if (sel[c]) cudaEventDestroy(sel[c]);
+        if (t0[c]) cudaEventDestroy(t0[c]);
+        if (t1[c]) cudaEventDestroy(t1[c]);
+    }
+    if (done) cudaEventDestroy(done);
+    if (cs) cudaStreamDestroy(cs);
+    ctx_free(ctx, rows, n * 4);
+    return rc;
+}
+
 }  // namespace nbg
 
 extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stages,
@@ -882,6 +1027,13 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         if (!placed) groups.push_back({s});
     }
 
+    // pinned host records of one plain kNN group on a large tile: copied back
+    // chunk by chunk while the later chunks are answered (run_pipelined)
+    const bool pipelined = packed && host_pinned(outputs[0].base) && groups.size() == 1 &&
+                           consumers.empty() && n >= (1ull << 22) && !by_radius(groups[0][0]) &&
+                           !strided(groups[0][0]) && !stages[groups[0][0]].optimized;
+    const int pipe_chunks = n >= (8ull << 20) ? 4 : 2;
+    bool packed_copied = false;
     cudaEventRecord(ctx->ev[0], stream);
     float grid_ms = 0, query_ms = 0, tree_ms = 0;
     uint64_t tie_rows = 0, deferred_rows = 0, replay_rows = 0;
@@ -974,6 +1126,23 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             grid_ms += ms;
             cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
             query_ms += ms;
+            continue;
+        }
+        if (pipelined) {
+            PipeStats ps;
+            rc = run_pipelined(ctx, t, K, g, sink, packed_dev, (char*)outputs[0].base,
+                               (size_t)outputs[0].point_stride, pipe_chunks, stream, ps);
+            if (rc) { cleanup(); return rc; }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+            grid_ms += ms;
+            query_ms += ps.query_ms;
+            tree_ms += ps.tree_ms;
+            build_ms += ps.build_ms;
+            tie_rows += ps.tie_rows;
+            deferred_rows += ps.deferred_rows;
+            replay_rows += ps.replay_rows;
+            packed_copied = true;
             continue;
         }
         QueryLaunch ql;
@@ -1072,7 +1241,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     tie_rows += cc.tie_rows;
     replay_rows += cc.replay_rows;
     // results back to host layouts
-    if (packed) {
+    if (packed && !packed_copied) {
         rc = device_to_host(ctx, outputs[0].base, packed_dev, packed_bytes, stream);
         if (rc) { cleanup(); return rc; }
     }
@@ -1119,6 +1288,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         stats->query_ms = query_ms;
         stats->tree_ms = tree_ms;
         stats->kd_build_ms = build_ms;
+        stats->output_chunks = packed_copied ? (uint64_t)pipe_chunks : 0;
         float ms = 0;
         cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[6]);
         stats->total_ms = ms;

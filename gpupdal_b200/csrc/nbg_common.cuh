@@ -115,6 +115,8 @@ struct QueryArgs {
     uint32_t tie_cap;
     RowSums* sums;       // split form: per sorted position, read by knn_finish_kernel
     const double* row_k; // covariancefeatures optimized: per-point k = OptimalKNN (null: K)
+    const uint32_t* rows = nullptr;  // split form: the sorted positions to answer (null: all n)
+    uint64_t nq = 0;                 // entries of `rows`
 };
 
 // Neighbour count of a row: K, or the point's OptimalKNN rounded half away

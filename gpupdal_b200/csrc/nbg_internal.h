@@ -140,8 +140,16 @@ struct QueryLaunch {
     uint32_t tie_cap = 0;
     RowSums* sums = nullptr;  // split select/finish kernels (null: one fused kernel)
     const double* row_k = nullptr;  // per-row neighbour count (optimized), device
+    const uint32_t* rows = nullptr;  // split form only: sorted positions to answer (null: all)
+    uint64_t nrows = 0;
 };
 int launch_query(Context* ctx, const QueryLaunch& q, cudaStream_t stream);
+// rows + bounds[c] receives, in ascending order, the sorted positions whose
+// point id lies in [bounds[c], bounds[c+1]), for c < nchunks (bounds[nchunks]
+// = n); `dnum` is one device word the selection writes its count to.
+// Returns after the selection completed.
+int build_id_chunks(Context* ctx, const Tile* t, const uint64_t* bounds, int nchunks,
+                    uint32_t* rows, uint32_t* dnum, cudaStream_t st);
 // Select pass over a sample of `blocks` blocks of 128 rows, in runs of `run`
 // consecutive blocks whose starts are `stride` rows apart.
 int launch_select_sample(Context* ctx, const QueryLaunch& q, uint64_t stride, unsigned blocks,

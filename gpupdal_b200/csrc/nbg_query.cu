@@ -24,6 +24,9 @@
 // row with no boundary tie has exactly the reference's neighbour set.
 #include <algorithm>
 
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
+
 #include "nbg_common.cuh"
 #include "nbg_internal.h"
 
@@ -367,8 +370,10 @@ __device__ __forceinline__ void select_row(const QueryArgs& a, const uint64_t i)
 
 template <int KS>
 __global__ void __launch_bounds__(128) knn_select_kernel(const QueryArgs a) {
-    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i < a.n) select_row<KS>(a, i);
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= (a.rows ? a.nq : a.n)) return;
+    if (a.rows) i = __ldg(&a.rows[i]);
+    select_row<KS>(a, i);
 }
 
 // Split form, finish: covariance, eigensolve and stage projections of the
@@ -403,8 +408,10 @@ __global__ void __launch_bounds__(128) knn_select_sample_kernel(const QueryArgs 
 }
 
 __global__ void __launch_bounds__(128) knn_finish_kernel(const QueryArgs a) {
-    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i < a.n) finish_row(a, i);
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= (a.rows ? a.nq : a.n)) return;
+    if (a.rows) i = __ldg(&a.rows[i]);
+    finish_row(a, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -1132,7 +1139,8 @@ struct KnnLauncher {
     using Args = LaunchArgs;
     static int run(const LaunchArgs& la) {
         const int threads = 128;
-        const uint64_t blocks = (la.q.n + threads - 1) / threads;
+        const uint64_t rows = la.q.rows ? la.q.nq : la.q.n;
+        const uint64_t blocks = (rows + threads - 1) / threads;
         if (blocks == 0) return NBG_OK;
         if (la.ids) {
             knn_ids_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
@@ -1175,6 +1183,8 @@ int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
     la.q.tie_cap = ql.tie_cap;
     la.q.sums = ql.sums;
     la.q.row_k = ql.row_k;
+    la.q.rows = ql.sums ? ql.rows : nullptr;  // the fused kernel answers every row
+    la.q.nq = ql.sums ? ql.nrows : 0;
     la.stream = stream;
     la.ids = false;
     return dispatch_slots<KnnLauncher>(ql.K, la);
@@ -1204,6 +1214,39 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
 }
 
 int slots_for_k(int K) { return slots_for(K); }
+
+// Sorted positions whose point id lies in [lo, hi).
+struct InIdRange {
+    const float4* sorted;
+    uint32_t lo, hi;
+    __device__ __forceinline__ bool operator()(const uint32_t i) const {
+        const uint32_t id = __float_as_uint(__ldg(&sorted[i]).w);
+        return id >= lo && id < hi;
+    }
+};
+
+int build_id_chunks(Context* ctx, const Tile* t, const uint64_t* bounds, int nchunks,
+                    uint32_t* rows, uint32_t* dnum, cudaStream_t st) {
+    const uint64_t n = t->n;
+    cub::CountingInputIterator<uint32_t> first(0);
+    size_t tmp_bytes = 0;
+    cudaError_t e = cub::DeviceSelect::If(nullptr, tmp_bytes, first, rows, dnum, (int64_t)n,
+                                          InIdRange{t->sorted, 0, 0}, st);
+    if (e) return fail(ctx, NBG_ERR_CUDA, std::string("row chunks: ") + cudaGetErrorString(e));
+    void* tmp = nullptr;
+    int rc = ctx_alloc(ctx, &tmp, std::max<size_t>(tmp_bytes, 16));
+    if (rc) return rc;
+    for (int c = 0; c < nchunks && !e; ++c) {
+        e = cub::DeviceSelect::If(tmp, tmp_bytes, first, rows + bounds[c], dnum, (int64_t)n,
+                                  InIdRange{t->sorted, (uint32_t)bounds[c], (uint32_t)bounds[c + 1]},
+                                  st);
+        NBG_LAUNCHED(1);
+    }
+    // the temporary storage goes back to the cache only after the selects ran
+    if (!e) e = cudaStreamSynchronize(st);
+    ctx_free(ctx, tmp, std::max<size_t>(tmp_bytes, 16));
+    return e ? fail(ctx, NBG_ERR_CUDA, std::string("row chunks: ") + cudaGetErrorString(e)) : NBG_OK;
+}
 
 struct SampleArgs {
     QueryArgs q;

@@ -194,6 +194,9 @@ typedef struct nbg_run_stats {
     uint64_t outliers;        /* outlier stages: rows found to be outliers
                                  (written only when inliers remain)             */
     uint64_t inliers;         /* outlier stages: rows found to be inliers       */
+    uint64_t output_chunks;   /* host records copied back in this many chunks of
+                                 the point-id range, each while the later chunks
+                                 were answered (0: one copy at the end)         */
 } nbg_run_stats;
 
 typedef struct nbg_context nbg_context;
