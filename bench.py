@@ -622,7 +622,13 @@ def main():
                    "resolved_rows": int(last.resolved_rows), "replay_rows": int(last.replay_rows),
                    "grid_ms": last.grid_ms, "query_ms": last.query_ms, "tree_ms": last.tree_ms},
         "e2e": {"value": e2e_value, "unit": "Mpts/s", "h2d_bytes_per_step": 12 * n,
-                "d2h_bytes_per_step": 8 * sum(nd) * n},
+                "d2h_bytes_per_step": 8 * sum(nd) * n, "ms_per_step": ms_e2e / args.steps,
+                "output_chunks": int(stats_e2e[-1].output_chunks),
+                "run_device_ms": statistics.mean(s.total_ms for s in stats_e2e),
+                "run_query_ms": statistics.mean(s.query_ms for s in stats_e2e),
+                "form": "tile upload from pinned host arrays + nbg_run writing one pinned "
+                        "56-byte host record per point (copied back chunk by chunk while "
+                        "later chunks run when output_chunks > 0)"},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": TRAFFIC_PER_POINT * n,
