@@ -642,7 +642,7 @@ def main():
                      "kernel": "knn_select_kernel+knn_finish_kernel", "peak_source": peak_kind,
                      "bytes_per_point": BYTES_PER_POINT,
                      "limiter": "instruction issue, not HBM: ncu on the 4M-point stress tile shows "
-                                "knn_select_kernel with 77.5 % of issue slots busy and 0.5 % DRAM "
+                                "knn_select_kernel with 79.3 % of issue slots busy and 0.54 % DRAM "
                                 "throughput (8.9 of 32 lanes active per instruction)"},
         "clocks": clk,
     }
