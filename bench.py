@@ -255,6 +255,49 @@ def fp64_leg(ctx, args, dxyz, drec, sts, steps):
             "rows_compared": int(ok.sum()), "normal_rows_compared": int(okn.sum())}
 
 
+def target_leg(ctx, dxyz, seed, steps):
+    """filters.normal knn=16 + filters.covariancefeatures knn=16 feature_set=all on the main
+    tile (one grid, one fused pass for both stages): device inputs, one 128-byte device
+    record per point (4 + 11 dims), OptimalKNN / OptimalRadius input columns as in the
+    4M-point covariancefeatures configuration."""
+    import torch
+    from gpupdal_b200 import abi
+    from gpupdal_b200 import synthetic as syn
+    from gpupdal_b200.native import record_columns
+    n = int(dxyz[0].shape[0])
+    dev = dxyz[0].device
+    sts = [abi.make_opts(abi.STAGE_NORMAL, knn=16),
+           abi.make_opts(abi.STAGE_COVARIANCEFEATURES, knn=16, feature_mask=abi.FEAT_ALL)]
+    kopt, ropt = syn.optimal_columns(n, seed, knn=16)
+    dk, dr = (torch.from_numpy(v).to(dev) for v in (kopt, ropt))
+    rec = torch.empty((n, 16), dtype=torch.float64, device=dev)
+    cols = record_columns(rec.data_ptr(), sts, 128, 1)
+
+    def step():
+        tile = ctx.tile(*dxyz)
+        _, st = ctx.run_columns(tile, sts, cols, optimal_knn=dk, optimal_radius=dr,
+                                aux_on_device=True)
+        tile.free()
+        return st
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    stats = [step() for _ in range(steps)]
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    q = statistics.mean(s.query_ms for s in stats)
+    bpp = 16 + 4 + 8 * 15 + 1
+    hbm, _ = peaks()
+    return {"workload": f"stress tile {n} points, normal knn=16 + covariancefeatures knn=16 "
+                        "feature_set=all, one fused pass",
+            "ms_per_step": ms, "value": n / ms / 1e3, "unit": "Mpts/s", "query_ms": q,
+            "bytes_per_point": bpp, "query_hbm_frac": n * bpp / (q / 1e3) / 1e9 / hbm}
+
+
 def extras_cases():
     """The stage options beyond the main path (radius, stride, optimized) and
     the other consumers of the index, each as one stage on the 4M mixture."""
@@ -648,6 +691,11 @@ def main():
     }
     if fp64 is not None:
         line["eigen_fp64"] = fp64
+    if ws == 1 and not args.no_extras:
+        try:
+            line["normal_plus_features"] = target_leg(ctx, (dx, dy, dz), 2 + rank, args.steps)
+        except Exception as exc:  # recorded, not fatal to the main line
+            line["normal_plus_features"] = {"error": str(exc)}
     if ws == 1 and not args.no_batched:
         line["batched"] = batched_leg(ctx, args)
     if ws == 1 and not args.no_served:
