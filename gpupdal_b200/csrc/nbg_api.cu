@@ -164,6 +164,7 @@ static void par_memcpy(void* dst, const void* src, size_t bytes) {
 }
 
 int host_to_device(Context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    NBG_RANGE("nbg copy in");
     if (!bytes) return NBG_OK;
     if (bytes < ((size_t)1 << 20) || host_pinned(src)) {
         cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
@@ -186,6 +187,7 @@ int host_to_device(Context* ctx, void* dst, const void* src, size_t bytes, cudaS
 }
 
 int device_to_host(Context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    NBG_RANGE("nbg copy back");
     if (!bytes) return NBG_OK;
     if (bytes < ((size_t)1 << 20) || host_pinned(dst)) {
         cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream);
@@ -423,6 +425,7 @@ uint64_t nbg_tile_size(const nbg_tile* t) { return t ? t->t.n : 0; }
 int nbg_tile_upload(nbg_context* h, const int32_t* x, const int32_t* y, const int32_t* z,
                     uint64_t n, const double scale[3], const double offset[3], int32_t on_device,
                     void* stream_v, nbg_tile** out) {
+    NBG_RANGE("nbg tile upload");
     if (!h || !out) return NBG_ERR_INVALID;
     Context* ctx = &h->c;
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -547,6 +550,7 @@ namespace nbg {
 // (radius stages); rebuilt when k1 moves far from the build's or the edge rule
 // changes.
 int ensure_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream, int32_t cell) {
+    NBG_RANGE("nbg grid build");
     const int32_t fixed = cell ? cell : t->fixed_cell;
     if (t->grid_valid && t->grid_fixed == fixed &&
         (fixed || (k1 <= 2 * t->grid_k1 && 2 * k1 >= t->grid_k1)))
@@ -707,6 +711,7 @@ struct PipeStats {
 static int run_pipelined(Context* ctx, Tile* t, int K, const StageGroup& g, const ExceptionSink& sink,
                          const char* dev_records, char* host_records, size_t record_bytes, int C,
                          cudaStream_t stream, PipeStats& ps) {
+    NBG_RANGE("nbg pipelined query");
     const uint64_t n = t->n;
     // chunk c counts in counters[8c .. 8c+4]: at most four chunks stay below
     // the word build_id_chunks writes (counters[48])
@@ -839,6 +844,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
                        const double* optimal_radius, int32_t aux_on_device,
                        nbg_row_exception* exceptions, uint32_t exception_capacity,
                        uint32_t* n_exceptions, nbg_run_stats* stats, void* stream_v) {
+    NBG_RANGE("nbg_run");
     if (!h || !th) return NBG_ERR_INVALID;
     Context* ctx = &h->c;
     Tile* t = &th->t;

@@ -107,6 +107,7 @@ using namespace nbg;
 
 extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_t n_items,
                              uint32_t flags, nbg_run_stats* stats, void* stream_v) {
+    NBG_RANGE("nbg_run_batch");
     if (!h || n_items < 0 || (n_items && !items)) return NBG_ERR_INVALID;
     Context* ctx = &h->c;
     std::lock_guard<std::mutex> lock(ctx->mu);

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <atomic>
 #include <cstdint>
@@ -23,6 +24,19 @@ struct KdReplica;  // exact nanoflann replica (nbg_kdtree.cu)
 // Kernels launched by this library (all contexts), for the per-call count.
 extern std::atomic<uint64_t> g_launches;
 #define NBG_LAUNCHED(n) ::nbg::g_launches.fetch_add((n), std::memory_order_relaxed)
+
+// NVTX range over a host-side phase (grid build, KD replica build, search
+// replay, copies, whole calls), seen by Nsight tools; without a tool attached
+// a push/pop is a no-op call.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+#define NBG_RANGE_CAT2(a, b) a##b
+#define NBG_RANGE_CAT(a, b) NBG_RANGE_CAT2(a, b)
+#define NBG_RANGE(name) ::nbg::NvtxRange NBG_RANGE_CAT(nbg_range_, __LINE__)(name)
 
 struct Context {
     int device = 0;

@@ -1299,6 +1299,7 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
 
 // Builds one forest holding the replicas of every listed tile that has none.
 int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t st) {
+    NBG_RANGE("nbg kd replica build");
     std::vector<Tile*> todo;
     for (int i = 0; i < count; ++i)
         if (!(tiles[i]->kd && tiles[i]->kd->built) && tiles[i]->n > 0) todo.push_back(tiles[i]);
@@ -1461,6 +1462,7 @@ static int kd_search_rows(Context* ctx, Tile* t, int K, const uint32_t* rows, ui
 int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const ExceptionSink& ex,
                 const uint32_t* rows, uint32_t nrows, cudaStream_t st, const double* row_k,
                 int stride, int kpick) {
+    NBG_RANGE("nbg search replay");
     if (!nrows) return NBG_OK;
     uint32_t *nbr = nullptr, *counts = nullptr;
     int rc = kd_search_rows(ctx, t, K, rows, nrows, &nbr, &counts, st, row_k);
