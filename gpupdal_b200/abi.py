@@ -190,6 +190,15 @@ class RequestResult(ctypes.Structure):
     ]
 
 
+class TuneEntry(ctypes.Structure):
+    _fields_ = [
+        ("size_class", ctypes.c_int32),
+        ("slots", ctypes.c_int32),
+        ("cell_factor", ctypes.c_float),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 class LasInfo(ctypes.Structure):
     _fields_ = [
         ("version_major", ctypes.c_uint8),
@@ -313,6 +322,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_tile_autotune.argtypes = [vp, vp, i32, ctypes.POINTER(ctypes.c_float), i32, i32,
                                       ctypes.POINTER(ctypes.c_float), vp]
     lib.nbg_tile_autotune.restype = ctypes.c_int
+    lib.nbg_autotune_cache_get.argtypes = [vp, ctypes.POINTER(TuneEntry), i32,
+                                           ctypes.POINTER(ctypes.c_int32)]
+    lib.nbg_autotune_cache_get.restype = ctypes.c_int
+    lib.nbg_autotune_cache_set.argtypes = [vp, ctypes.POINTER(TuneEntry), i32]
+    lib.nbg_autotune_cache_set.restype = ctypes.c_int
     lib.nbg_tile_size.argtypes = [vp]
     lib.nbg_tile_size.restype = u64
     lib.nbg_run.argtypes = [vp, vp, ctypes.POINTER(StageOpts), i32, ctypes.POINTER(Columns),

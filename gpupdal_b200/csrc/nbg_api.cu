@@ -1406,6 +1406,41 @@ extern "C" int nbg_tile_autotune(nbg_context* h, nbg_tile* th, int32_t knn, cons
                          (cudaStream_t)stream_v);
 }
 
+extern "C" int nbg_autotune_cache_get(nbg_context* h, nbg_tune_entry* entries, int32_t capacity,
+                                      int32_t* count) {
+    if (!h || !count || capacity < 0 || (capacity > 0 && !entries)) return NBG_ERR_INVALID;
+    Context* ctx = &h->c;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    int32_t i = 0;
+    for (const auto& kv : ctx->tuned) {
+        if (i < capacity) {
+            entries[i].size_class = kv.first.first;
+            entries[i].slots = kv.first.second;
+            entries[i].cell_factor = kv.second;
+            entries[i].reserved = 0;
+        }
+        ++i;
+    }
+    *count = i;
+    return NBG_OK;
+}
+
+extern "C" int nbg_autotune_cache_set(nbg_context* h, const nbg_tune_entry* entries, int32_t count) {
+    if (!h || count < 0 || (count > 0 && !entries)) return NBG_ERR_INVALID;
+    Context* ctx = &h->c;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    for (int32_t i = 0; i < count; ++i) {
+        const nbg_tune_entry& e = entries[i];
+        if (e.size_class < 0 || e.size_class > 63 || e.slots < 1 || e.slots > 128 ||
+            !std::isfinite(e.cell_factor) || !(e.cell_factor > 0.0f))
+            return fail(ctx, NBG_ERR_INVALID, "bad tuning-cache entry");
+    }
+    for (int32_t i = 0; i < count; ++i)
+        ctx->tuned[std::make_pair((int)entries[i].size_class, (int)entries[i].slots)] =
+            entries[i].cell_factor;
+    return NBG_OK;
+}
+
 extern "C" int nbg_neighbor_sets(nbg_context* h, nbg_tile* th, int32_t knn, uint32_t* ids_out,
                                  int32_t ids_on_device, nbg_run_stats* stats, void* stream_v) {
     if (!h || !th || !ids_out) return NBG_ERR_INVALID;

@@ -77,6 +77,47 @@ class Context:
             self._tls.exc = buf
         return buf
 
+    def tuning_cache(self):
+        """The autotuner's cached choices: a list of
+        {"size_class", "slots", "cell_factor"} (nbg_autotune_cache_get)."""
+        count = ctypes.c_int32(0)
+        self._check(self.lib.nbg_autotune_cache_get(self.h, None, 0, ctypes.byref(count)))
+        buf = (abi.TuneEntry * max(count.value, 1))()
+        self._check(self.lib.nbg_autotune_cache_get(self.h, buf, count.value, ctypes.byref(count)))
+        return [{"size_class": int(e.size_class), "slots": int(e.slots),
+                 "cell_factor": float(e.cell_factor)} for e in buf[:count.value]]
+
+    def set_tuning_cache(self, entries):
+        """Adds or replaces autotuner choices (nbg_autotune_cache_set)."""
+        buf = (abi.TuneEntry * max(len(entries), 1))()
+        for e, d in zip(buf, entries):
+            e.size_class = int(d["size_class"])
+            e.slots = int(d["slots"])
+            e.cell_factor = float(d["cell_factor"])
+        self._check(self.lib.nbg_autotune_cache_set(self.h, buf, len(entries)))
+
+    def save_tuning(self, path):
+        """Writes the autotuner's choices to a JSON tuning file, keyed by the
+        device's name (a file tuned on one GPU model is not applied to another)."""
+        import json
+        with open(path, "w") as f:
+            json.dump({"device": self.device_name(), "entries": self.tuning_cache()}, f, indent=1)
+
+    def load_tuning(self, path):
+        """Applies a tuning file written by save_tuning on the same GPU model;
+        returns the number of entries applied (0 for another model)."""
+        import json
+        with open(path) as f:
+            d = json.load(f)
+        if d.get("device") != self.device_name():
+            return 0
+        self.set_tuning_cache(d["entries"])
+        return len(d["entries"])
+
+    def device_name(self):
+        import torch
+        return torch.cuda.get_device_name(self.device)
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.nbg_destroy(self.h)

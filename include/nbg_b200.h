@@ -235,13 +235,30 @@ int nbg_tile_free(nbg_context* ctx, nbg_tile* tile);
  * reference (whose KD tree has no tunable). */
 int nbg_tile_tune(nbg_context* ctx, nbg_tile* tile, float cell_factor, int32_t fixed_cell);
 /* Autotuner: builds the tile's grid with each candidate cell factor (null:
- * 1, 1.5, 2, 3, 4, 6), times the select pass on a 65,536-row sample spread
- * over the tile, and keeps the factor with the least estimated grid + query
- * time (rows the ring search would defer charged at 20 us each).  The choice
- * is cached per (log2 points, neighbour slots) class of the context; with
- * use_cache a cached class is applied without measuring. */
+ * 1, 1.5, 2, 3, 4, 6), times the select pass on a sample of four waves of
+ * blocks taken as runs of 32 consecutive 128-row blocks spread over the tile,
+ * and keeps the factor with the least estimated grid + query time (rows the
+ * ring search would defer charged at 5 us each).  The choice is cached per
+ * (log2 points, neighbour slots) class of the context; with use_cache a
+ * cached class is applied without measuring. */
 int nbg_tile_autotune(nbg_context* ctx, nbg_tile* tile, int32_t knn, const float* candidates,
                       int32_t n_candidates, int32_t use_cache, float* chosen, void* stream);
+
+/* The autotuner's cached choices, to keep them in a tuning file across
+ * processes: one entry per (log2 points, neighbour slots) class.
+ * nbg_autotune_cache_get writes up to `capacity` entries (sorted by class)
+ * and the number the cache holds to *count; nbg_autotune_cache_set adds or
+ * replaces entries (NBG_ERR_INVALID for a class outside [0, 63] x [1, 128]
+ * or a factor that is not finite and positive; nothing is set then). */
+typedef struct nbg_tune_entry {
+    int32_t size_class;    /* floor(log2(points))                            */
+    int32_t slots;         /* neighbour slots of the select kernel           */
+    float cell_factor;
+    int32_t reserved;
+} nbg_tune_entry;
+int nbg_autotune_cache_get(nbg_context* ctx, nbg_tune_entry* entries, int32_t capacity,
+                           int32_t* count);
+int nbg_autotune_cache_set(nbg_context* ctx, const nbg_tune_entry* entries, int32_t count);
 uint64_t nbg_tile_size(const nbg_tile* tile);
 
 /* Run stages over a resident tile.  Stages sharing knn share one fused

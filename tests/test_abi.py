@@ -54,6 +54,8 @@ int main(void) {
          offsetof(nbg_request_result, stats), offsetof(nbg_run_stats, kd_build_ms));
   printf("%zu %zu %zu\n", sizeof(nbg_las_info), offsetof(nbg_las_info, point_count),
          offsetof(nbg_las_info, max));
+  printf("%zu %zu %zu\n", sizeof(nbg_tune_entry), offsetof(nbg_tune_entry, cell_factor),
+         offsetof(nbg_run_stats, output_chunks));
   return 0;
 }
 """
@@ -76,6 +78,9 @@ int main(void) {
     las = [int(v) for v in lines[3].split()]
     assert las == [ctypes.sizeof(abi.LasInfo), abi.LasInfo.point_count.offset,
                    abi.LasInfo.max.offset]
+    tune = [int(v) for v in lines[4].split()]
+    assert tune == [ctypes.sizeof(abi.TuneEntry), abi.TuneEntry.cell_factor.offset,
+                    abi.RunStats.output_chunks.offset]
 
 
 def test_loader_fails_loudly_without_the_library(tmp_path):
