@@ -716,8 +716,13 @@ static int run_pipelined(Context* ctx, Tile* t, int K, const StageGroup& g, cons
     // chunk c counts in counters[8c .. 8c+4]: at most four chunks stay below
     // the word build_id_chunks writes (counters[48])
     if (C < 1 || C > 4) return fail(ctx, NBG_ERR_INVALID, "pipeline chunk count");
+    // four chunks of 30, 30, 25 and 15 % of the id range: the copy of the last
+    // chunk is the only one left after the queries end, so it is the smallest
+    // (the earlier, larger copies still finish while later chunks run)
+    static const uint64_t w4[5] = {0, 300, 600, 850, 1000};
     uint64_t b[9];
-    for (int c = 0; c <= C; ++c) b[c] = n * (uint64_t)c / (uint64_t)C;
+    for (int c = 0; c <= C; ++c)
+        b[c] = C == 4 ? n * w4[c] / 1000 : n * (uint64_t)c / (uint64_t)C;
     uint32_t* rows = nullptr;
     int rc = ctx_alloc(ctx, (void**)&rows, n * 4);
     if (rc) return rc;
