@@ -99,3 +99,29 @@ def test_reference_las_fixture(tmp_path):
     assert np.array_equal(rx, g["x"]) and np.array_equal(ry, g["y"]) and np.array_equal(rz, g["z"])
     assert h["min"][0] == pytest.approx(g["x"].min() * 0.01)
     assert h["max"][1] == pytest.approx(g["y"].max() * 0.01)
+
+
+def test_header_parser_survives_mutations():
+    # every truncation of the reference's simple.las header block, and every
+    # byte of it set to 0x00, 0xFF and a random value: the parser rejects the
+    # header or returns one whose fields hold together
+    from tests import _util as U
+    hdr = bytes(U.golden("las_simple")["las_header"])
+    rng = np.random.default_rng(11)
+
+    def check(b):
+        try:
+            h = las.header(b)
+        except las.LasError:
+            return
+        assert h["point_record_length"] >= 12
+        assert h["point_format"] <= 10
+        assert h["compressed"] in (0, 1)
+
+    for n in range(len(hdr) + 1):
+        check(hdr[:n])
+    for i in range(len(hdr)):
+        for v in (0x00, 0xFF, int(rng.integers(0, 256))):
+            b = bytearray(hdr)
+            b[i] = v
+            check(bytes(b))
