@@ -39,8 +39,8 @@ sys.path.insert(0, ROOT)
 METRIC = "Mpts/s k=16 normals+eigen, served vs plain @<=1e-5 rel err; p50/p99 latency"
 BYTES_PER_POINT = 20 + 8 * 7 + 1  # sorted xyz+id, id permutation, 7 f64 outputs, status
 # DRAM bytes per point of knn_select_kernel + knn_finish_kernel (read + write) from one
-# ncu capture of the same workload at 4M points: (178.4 + 691.4) MB / 4e6
-TRAFFIC_PER_POINT = 217.5
+# ncu capture of the same workload at 4M points: (182.3 + 628.9) MB / 4e6
+TRAFFIC_PER_POINT = 202.8
 
 
 def parse():
