@@ -44,7 +44,7 @@ def stage_set(kind_list):
 REF = os.environ.get("NBG_REFERENCE", "/root/reference")
 
 
-def record(ref, name, x, y, z, knns, stages, kopt=None, ropt=None, extra=None):
+def record(ref, name, x, y, z, knns, stages, kopt=None, ropt=None, extra=None, out=None):
     X, Y, Z = (syn.to_double(v) for v in (x, y, z))
     t = ref.tree(X, Y, Z)
     data = dict(x=x.astype(np.int32), y=y.astype(np.int32), z=z.astype(np.int32))
@@ -60,7 +60,8 @@ def record(ref, name, x, y, z, knns, stages, kopt=None, ropt=None, extra=None):
         data["optimal_radius"] = ropt
     if extra:
         data.update(extra)
-    path = os.path.join(OUT, f"{name}.npz")
+    os.makedirs(out or OUT, exist_ok=True)
+    path = os.path.join(out or OUT, f"{name}.npz")
     np.savez_compressed(path, **data)
     print(path, len(x), os.path.getsize(path))
 
@@ -143,6 +144,25 @@ def main():
             ("cov10", A.make_opts(A.STAGE_COVARIANCEFEATURES, knn=10,
                                   feature_mask=A.FEAT_ALL & ~A.FEAT_BIT["Density"]))],
            extra={"las_header": hdr, "las_records": np.asarray(lf.records).copy()})
+    # the fork's approximatecoplanar fixtures (test/data/pdg/approximatecoplanar-
+    # boundary.csv: six points on the axes whose spectrum puts the thresholds
+    # exactly on the boundary, with the options of hybrid-approximatecoplanar-
+    # boundary.json and -ties.json; approximatecoplanar-widened.csv: four
+    # coincident points).  Kept in fixtures/, outside the device parity sets:
+    # the oracle is pinned to them on the CPU.
+    fx = os.path.join(OUT, "fixtures")
+    for fname, gname, runs in [
+            ("approximatecoplanar-boundary.csv", "fork_coplanar_boundary",
+             [("cop6", A.consumer_opts(A.STAGE_APPROXIMATECOPLANAR, knn=6, thresh1=25.0, thresh2=5.0)),
+              ("cop3", A.consumer_opts(A.STAGE_APPROXIMATECOPLANAR, knn=3, thresh1=25.0, thresh2=6.0)),
+              ("rank6", A.consumer_opts(A.STAGE_ESTIMATERANK, knn=6)),
+              ("eig5", A.make_opts(A.STAGE_EIGENVALUES, knn=5))]),
+            ("approximatecoplanar-widened.csv", "fork_coplanar_coincident",
+             [("cop3", A.consumer_opts(A.STAGE_APPROXIMATECOPLANAR, knn=3)),
+              ("rank3", A.consumer_opts(A.STAGE_ESTIMATERANK, knn=3))])]:
+        pts = np.loadtxt(os.path.join(REF, "test/data/pdg", fname), delimiter=",", skiprows=1)[:, :3]
+        raw = np.rint(pts * 100).astype(np.int32)
+        record(ref, gname, raw[:, 0], raw[:, 1], raw[:, 2], [1, 2, 3], runs, out=fx)
     for cname, (cx, cy, cz) in cases.items():
         cx, cy, cz = (np.array(v, dtype=np.int32) for v in (cx, cy, cz))
         record(ref, f"edge_{cname}", cx, cy, cz, [3, 8],

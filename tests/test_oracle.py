@@ -9,6 +9,8 @@
 """
 import math
 
+import os
+
 import numpy as np
 import pytest
 
@@ -19,7 +21,19 @@ from tests import _util as U
 
 @pytest.mark.parametrize("name", U.golden_names())
 def test_port_matches_golden(port, name):
-    g = U.golden(name)
+    _port_matches(port, U.golden(name), name)
+
+
+FIXTURES = os.path.join(U.GOLDEN, "fixtures")
+
+
+@pytest.mark.parametrize("name", sorted(f[:-4] for f in os.listdir(FIXTURES) if f.endswith(".npz")))
+def test_port_matches_fork_fixtures(port, name):
+    # the reference's own approximatecoplanar fixtures (tests/golden/fixtures)
+    _port_matches(port, dict(np.load(os.path.join(FIXTURES, name + ".npz"))), name)
+
+
+def _port_matches(port, g, name):
     X, Y, Z = U.doubles(g)
     t = port.tree(X, Y, Z)
     for key in [k for k in g if k.startswith("nbr_k")]:
