@@ -33,6 +33,17 @@ def test_port_matches_fork_fixtures(port, name):
     _port_matches(port, dict(np.load(os.path.join(FIXTURES, name + ".npz"))), name)
 
 
+def test_fork_boundary_fixture_known_answer():
+    # six points at (+-1,0,0), (0,+-5,0), (0,0,+-10): with every point in the
+    # neighbourhood the covariance is diag(0.4, 10, 40), so thresh1 = 25 sits
+    # exactly on the boundary (10 > 25 * 0.4 is false: not coplanar) and the
+    # rank is 3
+    g = dict(np.load(os.path.join(FIXTURES, "fork_coplanar_boundary.npz")))
+    assert np.array_equal(g["eig5_out"], np.tile([[0.4], [10.0], [40.0]], (1, 6)))
+    assert np.array_equal(g["cop6_out"], np.zeros((1, 6)))
+    assert np.array_equal(g["rank6_out"], np.full((1, 6), 3.0))
+
+
 def _port_matches(port, g, name):
     X, Y, Z = U.doubles(g)
     t = port.tree(X, Y, Z)
