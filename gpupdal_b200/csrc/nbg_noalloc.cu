@@ -19,7 +19,11 @@
 //
 // The array is shared by every call in the process on a given device and
 // keeps the last call's contents; the entry point clears what must start at
-// zero.  Calls whose work overlaps on the same device race on it.
+// zero.  Calls whose work overlaps on the same device race on it, so calls on
+// one device must be serialised (for example, all issued on one stream).
+// Every call looks up the array's device address with the device current;
+// the first call on a device also loads the library's device code there, so
+// make it outside any stream capture.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -52,10 +56,6 @@ constexpr size_t kArenaBytes = kOffTmp + kTmpReserve;
 // device that loads this library until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_arena[kArenaBytes];
 
-// Device address of g_noalloc_arena per device, looked up once per device.
-constexpr int kMaxDevices = 64;
-unsigned char* g_arena_ptr[kMaxDevices] = {nullptr};
-
 int set_msg(char* buf, size_t len, int code, const char* msg) {
     if (buf && len) {
         std::strncpy(buf, msg, len - 1);
@@ -86,10 +86,21 @@ extern "C" int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32
                        "tile larger than NBG_NOALLOC_MAX_POINTS; use nbg_tile_upload + nbg_run");
     if (n > 0 && (!x || !y || !z || !unresolved))
         return set_msg(err_msg, err_len, NBG_ERR_INVALID, "null device array");
+    if (exception_capacity > 0 && !exceptions)
+        return set_msg(err_msg, err_len, NBG_ERR_INVALID, "null exception array with a capacity");
     if (scale[0] != scale[1] || scale[0] != scale[2] || !(scale[0] > 0.0))
         return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "needs one positive scale for x, y, z");
-    if (opts->kind < 1 || opts->kind > 3 || opts->knn < 0 || opts->knn > 64)
-        return set_msg(err_msg, err_len, NBG_ERR_INVALID, "invalid stage options");
+    {
+        // the regular path's option checks first (same codes and messages)
+        Context vctx;
+        bool need_aux = false;
+        const int vrc = validate_stages(&vctx, opts, 1, out, &need_aux);
+        if (vrc) return set_msg(err_msg, err_len, vrc, vctx.err.c_str());
+    }
+    // then what this entry point does not run
+    if (opts->kind > NBG_STAGE_COVARIANCEFEATURES)
+        return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED,
+                       "only normal, eigenvalues and covariancefeatures run without allocation");
     if (opts->kind != NBG_STAGE_NORMAL && opts->stride > 1)
         return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED, "stride > 1 is not supported");
     if (opts->kind == NBG_STAGE_COVARIANCEFEATURES && opts->optimized)
@@ -97,12 +108,9 @@ extern "C" int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32
     if (opts->use_radius)
         return set_msg(err_msg, err_len, NBG_ERR_UNSUPPORTED,
                        "radius neighbourhoods are not supported by this entry point");
-    const int ndims = opts->kind == NBG_STAGE_NORMAL ? 4
-                      : opts->kind == NBG_STAGE_EIGENVALUES
-                          ? 3
-                          : __builtin_popcount(opts->feature_mask & NBG_FEAT_ALL);
-    if (out->ndims != ndims || out->on_device != 1)
-        return set_msg(err_msg, err_len, NBG_ERR_INVALID, "outputs must be device columns of the stage");
+    const int ndims = out->ndims;
+    if (out->on_device != 1)
+        return set_msg(err_msg, err_len, NBG_ERR_INVALID, "outputs must be device columns");
     if (opts->kind == NBG_STAGE_COVARIANCEFEATURES && (opts->feature_mask & NBG_FEAT_DENSITY) &&
         (!optimal_knn || !optimal_radius))
         return set_msg(err_msg, err_len, NBG_ERR_INVALID, "Density needs OptimalKNN and OptimalRadius");
@@ -110,21 +118,22 @@ extern "C" int nbg_stage_noalloc(const int32_t* x, const int32_t* y, const int32
     cudaStream_t stream = (cudaStream_t)stream_v;
 
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0)
         return set_msg(err_msg, err_len, NBG_ERR_NO_DEVICE, "no current device");
-    // First call on this device: look up the array's device address (the
-    // host-side symbol is not a device address).  Make this first call
-    // outside any stream capture.
-    if (!g_arena_ptr[dev]) {
+    // The array's device address on the current device (the host-side symbol
+    // is not a device address).  Looked up on every call: a cached address
+    // would go stale after cudaDeviceReset or a new primary context, and the
+    // lookup is a cheap host query once the device code is loaded.
+    unsigned char* arena = nullptr;
+    {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_arena);
         if (e != cudaSuccess || !p) {
             cudaGetLastError();
             return set_msg(err_msg, err_len, NBG_ERR_CUDA, "cudaGetSymbolAddress failed");
         }
-        g_arena_ptr[dev] = (unsigned char*)p;
+        arena = (unsigned char*)p;
     }
-    unsigned char* arena = g_arena_ptr[dev];
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 

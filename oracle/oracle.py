@@ -18,8 +18,10 @@ PORT_PATH = os.path.join(HERE, "_build", "libnbg_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libnbg_ref.so")
 
 
-def build(ref_root: str = "/root/reference") -> None:
-    """Compile the port (always) and the reference shim (when the tree exists)."""
+def build(ref_root: str | None = None) -> None:
+    """Compile the port (always) and the reference shim when a reference tree
+    is given (`ref_root`, else the NBG_REFERENCE environment variable)."""
+    ref_root = ref_root or os.environ.get("NBG_REFERENCE", "")
     subprocess.check_call(["make", "-s", "-C", HERE, "all", f"REF={ref_root}"])
 
 

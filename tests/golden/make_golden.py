@@ -4,7 +4,8 @@
 
 Inputs are seeded windows of the benchmark workloads, small tie-heavy and
 edge-case clouds, and two of the reference's own test fixtures (read where they
-lie in the reference tree, NBG_REFERENCE, default /root/reference): the fork's
+lie in the reference tree named by the NBG_REFERENCE environment variable,
+which must be set): the fork's
 tie / duplicate points and the simple.las tile.  Outputs come from oracle/_ref/libnbg_ref.so, i.e. the
 reference's own vendored nanoflann 1.3.1 and Eigen 3.4 compiled here (see
 oracle/Makefile); this script must run where that library was built.  Each
@@ -41,7 +42,9 @@ def stage_set(kind_list):
     return out
 
 
-REF = os.environ.get("NBG_REFERENCE", "/root/reference")
+REF = os.environ.get("NBG_REFERENCE", "")
+if __name__ == "__main__" and not os.path.isdir(REF):
+    sys.exit("set NBG_REFERENCE to the reference tree's root")
 
 
 def record(ref, name, x, y, z, knns, stages, kopt=None, ropt=None, extra=None, out=None):
