@@ -16,6 +16,7 @@ and the reference's own loops (oracle/_ref):
   covariance) of a threshold, relative to the largest eigenvalue.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -259,3 +260,34 @@ def test_pipeline_json_runs_the_consumers(nbg):
     # NNDistance was written by nndistance, then by lof (the later stage wins, as in PDAL)
     outs, _, _ = nbg.run(tile, [abi.consumer_opts(abi.STAGE_LOF, minpts=12)])
     assert np.array_equal(dims["NNDistance"], outs[0][0])
+
+
+FIXTURES = os.path.join(U.GOLDEN, "fixtures")
+
+
+@pytest.mark.parametrize("name", sorted(f[:-4] for f in os.listdir(FIXTURES) if f.endswith(".npz")))
+def test_fork_coplanar_fixtures_on_device(nbg, name):
+    # the fork's own approximatecoplanar fixtures, recorded from the reference:
+    # six axis points whose spectrum (0.4, 10, 40) puts thresh1 = 25 exactly on
+    # the boundary (knn 6, and knn 3 with a distance tie at the k-th
+    # neighbour), and four coincident points
+    g = dict(np.load(os.path.join(FIXTURES, name + ".npz")))
+    tile = nbg.tile(g["x"], g["y"], g["z"])
+    n = len(g["x"])
+    for key in [k for k in g if k.startswith("nbr_k")]:
+        ids, _ = nbg.neighbor_sets(tile, int(key[5:]))
+        assert np.array_equal(U.sorted_rows(ids), U.sorted_rows(g[key])), f"{name} {key}"
+    for key in [k for k in g if k.endswith("_opts")]:
+        sname = key[:-5]
+        o = U.opts_from_bytes(g[key])
+        outs, ex, _ = nbg.run(tile, [o])
+        status = U.status_from_exceptions(n, ex)
+        assert np.array_equal(status, g[sname + "_status"]), f"{name}/{sname} status"
+        ok = status == 0
+        want = g[sname + "_out"][:, ok]
+        got = outs[0][:, ok]
+        if o.kind in (abi.STAGE_APPROXIMATECOPLANAR, abi.STAGE_ESTIMATERANK):
+            assert np.array_equal(got, want), f"{name}/{sname}: {got} vs {want}"
+        else:
+            lmax = np.abs(want).max(axis=0)
+            assert np.all(np.abs(got - want) <= 1e-5 * lmax), f"{name}/{sname}: {got} vs {want}"
