@@ -319,6 +319,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_tile_free.restype = ctypes.c_int
     lib.nbg_tile_tune.argtypes = [vp, vp, ctypes.c_float, i32]
     lib.nbg_tile_tune.restype = ctypes.c_int
+    lib.nbg_tile_set_group.argtypes = [vp, vp, i32, ctypes.c_float]
+    lib.nbg_tile_set_group.restype = ctypes.c_int
     lib.nbg_tile_autotune.argtypes = [vp, vp, i32, ctypes.POINTER(ctypes.c_float), i32, i32,
                                       ctypes.POINTER(ctypes.c_float), vp]
     lib.nbg_tile_autotune.restype = ctypes.c_int

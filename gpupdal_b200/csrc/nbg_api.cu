@@ -246,6 +246,14 @@ int ensure_scratch(Context* ctx, uint64_t n, uint64_t ex_cap) {
         if (rc) return rc;
         ctx->tie_cap = std::max<uint64_t>(n, 1024);
     }
+    if (ctx->retry_cap < n) {
+        if (ctx->retry_rows) dev_free(ctx, ctx->retry_rows, ctx->retry_cap * 4);
+        ctx->retry_rows = nullptr;
+        ctx->retry_cap = 0;
+        int rc = dev_alloc(ctx, (void**)&ctx->retry_rows, std::max<uint64_t>(n, 1024) * 4, nullptr);
+        if (rc) return rc;
+        ctx->retry_cap = std::max<uint64_t>(n, 1024);
+    }
     if (ctx->exact_cap < n) {
         if (ctx->exact_rows) dev_free(ctx, ctx->exact_rows, ctx->exact_cap * 4);
         ctx->exact_rows = nullptr;
@@ -393,6 +401,7 @@ int nbg_destroy(nbg_context* h) {
     Context* ctx = &h->c;
     cudaSetDevice(ctx->device);
     dev_free(ctx, ctx->exact_rows, ctx->exact_cap * 4);
+    if (ctx->retry_rows) dev_free(ctx, ctx->retry_rows, ctx->retry_cap * 4);
     if (ctx->ties) dev_free(ctx, ctx->ties, ctx->tie_cap * sizeof(uint2));
     if (ctx->sums) dev_free(ctx, ctx->sums, ctx->sums_cap * sizeof(RowSums));
     dev_free(ctx, ctx->ex_rows, ctx->ex_cap * sizeof(nbg_row_exception));
@@ -529,6 +538,20 @@ int nbg_tile_tune(nbg_context* h, nbg_tile* th, float cell_factor, int32_t fixed
     th->t.cell_factor = cell_factor;
     th->t.fixed_cell = fixed_cell;
     th->t.grid_valid = false;
+    return NBG_OK;
+}
+
+extern "C" int nbg_tile_set_group(nbg_context* h, nbg_tile* th, int32_t queries_per_group,
+                                  float first_margin) {
+    if (!h || !th) return NBG_ERR_INVALID;
+    if (queries_per_group != 0 && queries_per_group != 8 && queries_per_group != 16 &&
+        queries_per_group != 32)
+        return fail(&h->c, NBG_ERR_INVALID, "queries per group must be 0, 8, 16 or 32");
+    if (!(first_margin > 0.0f && first_margin <= 16.0f))
+        return fail(&h->c, NBG_ERR_INVALID, "first margin must be in (0, 16] cell edges");
+    std::lock_guard<std::mutex> lock(h->c.mu);
+    th->t.group = queries_per_group;
+    th->t.margin0 = first_margin;
     return NBG_OK;
 }
 
@@ -799,6 +822,9 @@ static int run_pipelined(Context* ctx, Tile* t, int K, const StageGroup& g, cons
         ql.row_k = nullptr;
         ql.rows = rows + b[c];
         ql.nrows = b[c + 1] - b[c];
+        ql.retry_rows = ctx->retry_rows + b[c];
+        ql.group = t->group;
+        ql.margin0 = t->margin0;
         rc = launch_query(ctx, ql, stream);
         if (rc) {
             rc = fail(ctx, rc, std::string("query launch failed: ") + cudaGetErrorString(cudaGetLastError()));
@@ -1168,6 +1194,9 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         ql.tie_cap = (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX);
         ql.sums = ctx->sums;
         ql.row_k = row_k;
+        ql.retry_rows = ctx->retry_rows;
+        ql.group = t->group;
+        ql.margin0 = t->margin0;
         // the KD replica does not depend on the query: build it on the side
         // stream while the query kernel runs (tie rows almost always need it)
         const bool speculative = !(t->kd && kd_built(t)) && n > 100;
@@ -1471,7 +1500,8 @@ extern "C" int nbg_neighbor_sets(nbg_context* h, nbg_tile* th, int32_t knn, uint
     }
     cudaMemsetAsync(ctx->counters, 0, 64 * sizeof(uint32_t), stream);
     rc = launch_neighbor_sets(ctx, t, K, 8, dev_ids, ctx->exact_rows, ctx->counters, ctx->ties,
-                              (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX), stream);
+                              (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX), stream,
+                              ctx->retry_rows);
     uint32_t cnt[5] = {0, 0, 0, 0, 0};
     cudaError_t e = cudaSuccess;
     if (!rc) {

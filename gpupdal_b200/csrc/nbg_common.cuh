@@ -117,6 +117,8 @@ struct QueryArgs {
     const double* row_k; // covariancefeatures optimized: per-point k = OptimalKNN (null: K)
     const uint32_t* rows = nullptr;  // split form: the sorted positions to answer (null: all n)
     uint64_t nq = 0;                 // entries of `rows`
+    const uint32_t* nq_dev = nullptr;  // entries of `rows` read on the device (retry launches)
+    uint32_t* retry_rows = nullptr;    // group select: rows it hands to the per-thread select
 };
 
 // Neighbour count of a row: K, or the point's OptimalKNN rounded half away

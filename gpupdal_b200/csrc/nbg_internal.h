@@ -52,10 +52,12 @@ struct Context {
     uint64_t exact_cap = 0;
     uint2* ties = nullptr;          // tie list of the query kernels
     uint64_t tie_cap = 0;
+    uint32_t* retry_rows = nullptr; // rows the group select hands to the per-thread select
+    uint64_t retry_cap = 0;
     RowSums* sums = nullptr;        // select -> finish hand-over
     uint64_t sums_cap = 0;
     uint32_t* counters = nullptr;   // [0] exact rows, [1] tie rows, [2] deferred, [3] exceptions,
-                                    // [4] tie list, [5] eigen re-solves
+                                    // [4] tie list, [5] eigen re-solves, [6] group select retries
     nbg_row_exception* ex_rows = nullptr;
     uint64_t ex_cap = 0;
     cudaEvent_t ev[10];
@@ -117,6 +119,10 @@ struct Tile {
     bool fixed_storage = false;  // storage provided by the caller: never grow
     float cell_factor = 4.0f;
     int32_t fixed_cell = 0;
+    // select kernel: queries sharing one candidate list (8, 16, 32), or 0 for
+    // the per-thread ring search; first box margin in cell edges
+    int group = 32;
+    float margin0 = 0.25f;
     int grid_k1 = 0;
     int32_t grid_fixed = 0;      // fixed cell edge the current grid was built with (0: density)
     bool grid_valid = false;
@@ -156,6 +162,11 @@ struct QueryLaunch {
     const double* row_k = nullptr;  // per-row neighbour count (optimized), device
     const uint32_t* rows = nullptr;  // split form only: sorted positions to answer (null: all)
     uint64_t nrows = 0;
+    // group select (split form): rows handed back to the per-thread select
+    // (capacity: the rows answered; null: the per-thread select for every row)
+    uint32_t* retry_rows = nullptr;
+    int group = 0;
+    float margin0 = 0.25f;
 };
 int launch_query(Context* ctx, const QueryLaunch& q, cudaStream_t stream);
 // rows + bounds[c] receives, in ascending order, the sorted positions whose
@@ -228,7 +239,7 @@ int kd_export(Context* ctx, Tile* t, uint32_t* vind, uint32_t* nnodes, int32_t* 
 // neighbour-set export of the grid path
 int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
                          uint32_t* exact_rows, uint32_t* counters, uint2* ties, uint32_t tie_cap,
-                         cudaStream_t stream);
+                         cudaStream_t stream, uint32_t* retry_rows = nullptr);
 
 // Autotuner (nbg_tile_autotune without the context lock).
 int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, int32_t n_candidates,

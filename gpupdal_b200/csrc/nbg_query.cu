@@ -29,126 +29,9 @@
 
 #include "nbg_common.cuh"
 #include "nbg_internal.h"
+#include "nbg_query.cuh"
 
 namespace nbg {
-
-static constexpr uint32_t KEY_BASE = 0x4B000000u;    // bits of 2^23f
-static constexpr uint32_t KEY_EXACT_END = 0x4B800000u;  // bits of 2^24f
-
-__device__ __forceinline__ uint32_t dist_key(float dx, float dy, float dz) {
-    return __float_as_uint(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 8388608.0f))));
-}
-
-// integer value of an exact small float (|v| < 2^22)
-__device__ __forceinline__ int small_int(float v) {
-    return __float_as_int(v + 12582912.0f) - 0x4B400000;
-}
-
-struct QueryCell {
-    int qx, qy, qz;     // raw, relative to tile min
-    int cx, cy, cz;     // cell coords
-};
-
-// Calls f(float4) for the points of cells zl..zh of a column (inclusive).
-template <class F>
-__device__ __forceinline__ void scan_cells(const GridView& gv, const int4 ci, int zl, int zh, F& f) {
-    zl = max(zl, ci.y);
-    zh = min(zh, ci.z);
-    if (zl > zh) return;
-    const uint32_t e0 = (uint32_t)ci.x + (uint32_t)(zl - ci.y);
-    const uint32_t e1 = (uint32_t)ci.x + (uint32_t)(zh - ci.y) + 1;
-    const uint32_t pe = __ldg(&gv.cstart[e1]);
-    for (uint32_t j = __ldg(&gv.cstart[e0]); j < pe; ++j) f(__ldg(&gv.sorted[j]));
-}
-
-// Distance (raw units) from coordinate q to the cell slab [k*c, (k+1)*c - 1].
-__device__ __forceinline__ int slab_gap(int q, int k, int c) {
-    const int lo = k * c, hi = lo + c - 1;
-    return q < lo ? lo - q : (q > hi ? q - hi : 0);
-}
-
-// Calls f(float4) for every point of the cells at Chebyshev distance R that
-// can hold a point within the functor's current squared-distance limit
-// f.limit(): boundary columns contribute their cells with z in [cz-R, cz+R],
-// interior columns only the two cells at z = cz-R and z = cz+R; a column whose
-// horizontal gap already exceeds the limit, and cells beyond the ball's
-// z-reach, are skipped (they cannot hold a point at or below the limit).
-template <class F>
-__device__ __forceinline__ void scan_shell(const GridView& gv, const GridParams& g,
-                                           const QueryCell& qc, int R, F& f) {
-    const int zlo = qc.cz - R, zhi = qc.cz + R;
-    const int c = g.cell;
-    for (int dy = -R; dy <= R; ++dy) {
-        const int y = qc.cy + dy;
-        if (y < 0 || y >= g.gy) continue;
-        const int ady = dy < 0 ? -dy : dy;
-        const int gy_ = slab_gap(qc.qy, y, c);
-        for (int dx = -R; dx <= R; ++dx) {
-            const int x = qc.cx + dx;
-            if (x < 0 || x >= g.gx) continue;
-            const int gx_ = slab_gap(qc.qx, x, c);
-            const long long h2 = (long long)gx_ * gx_ + (long long)gy_ * gy_;
-            const unsigned long long lim = f.limit();
-            if ((unsigned long long)h2 > lim) continue;
-            const int4 ci = __ldg(&gv.colinfo[(uint32_t)y * (uint32_t)g.gx + (uint32_t)x]);
-            if (ci.z < ci.y) continue;
-            // z-cells within reach of the ball of squared radius lim
-            int zr0 = zlo, zr1 = zhi;
-            if (lim < (1ull << 46)) {
-                const float s = sqrtf((float)(lim - (unsigned long long)h2)) + 1.0f;
-                zr0 = max(zr0, (int)floorf(((float)qc.qz - s) / (float)c));
-                zr1 = min(zr1, (int)floorf(((float)qc.qz + s) / (float)c));
-            }
-            const int adx = dx < 0 ? -dx : dx;
-            if (max(ady, adx) == R) {
-                scan_cells(gv, ci, zr0, zr1, f);
-            } else {
-                if (zlo >= zr0 && zlo <= zr1) scan_cells(gv, ci, zlo, zlo, f);
-                if (zhi >= zr0 && zhi <= zr1) scan_cells(gv, ci, zhi, zhi, f);
-            }
-        }
-    }
-}
-
-// Squared raw gap from the query to any point outside the scanned cube of
-// radius R; UINT64_MAX when the cube covers the whole grid.
-__device__ __forceinline__ unsigned long long outside_gap2(const GridParams& g,
-                                                           const QueryCell& qc, int R) {
-    long long gap = LLONG_MAX;
-    const int c = g.cell;
-    if (qc.cx - R > 0) gap = min(gap, (long long)qc.qx - (long long)(qc.cx - R) * c + 1);
-    if (qc.cx + R < g.gx - 1) gap = min(gap, (long long)(qc.cx + R + 1) * c - qc.qx);
-    if (qc.cy - R > 0) gap = min(gap, (long long)qc.qy - (long long)(qc.cy - R) * c + 1);
-    if (qc.cy + R < g.gy - 1) gap = min(gap, (long long)(qc.cy + R + 1) * c - qc.qy);
-    if (qc.cz - R > 0) gap = min(gap, (long long)qc.qz - (long long)(qc.cz - R) * c + 1);
-    if (qc.cz + R < g.gz - 1) gap = min(gap, (long long)(qc.cz + R + 1) * c - qc.qz);
-    if (gap == LLONG_MAX) return ~0ull;
-    return (unsigned long long)gap * (unsigned long long)gap;
-}
-
-template <int KS>
-struct TopK {
-    uint32_t k[KS];
-    __device__ __forceinline__ void init(int off) {
-#pragma unroll
-        for (int s = 0; s < KS; ++s) k[s] = s < off ? 0u : 0xFFFFFFFFu;
-    }
-    __device__ __forceinline__ void insert(uint32_t key) {
-#pragma unroll
-        for (int s = 0; s < KS; ++s) {
-            const uint32_t lo = min(k[s], key);
-            key = max(k[s], key);
-            k[s] = lo;
-        }
-    }
-    __device__ __forceinline__ uint32_t at(int i) const {
-        uint32_t v = 0xFFFFFFFFu;
-#pragma unroll
-        for (int s = 0; s < KS; ++s)
-            if (s == i) v = k[s];
-        return v;
-    }
-};
 
 struct Pass1 {
     float qx, qy, qz;
@@ -214,21 +97,6 @@ struct CollectFn {
 };
 
 
-// A row that cannot finish on the grid: a boundary tie goes to the tie list
-// (its K-th distance and final ring kept for the order resolver), everything
-// else, and ties beyond the list's capacity, to the full search replay.
-__device__ __forceinline__ void defer_row(const QueryArgs& a, uint32_t id, bool tie, uint32_t kk,
-                                          int R) {
-    if (tie && a.ties) {
-        const uint32_t slot = atomicAdd(&a.counters[4], 1u);
-        if (slot < a.tie_cap) {
-            a.ties[slot] = make_uint2(id, (kk - KEY_BASE) | ((uint32_t)R << 24));
-            return;
-        }
-    }
-    const uint32_t slot = atomicAdd(&a.counters[0], 1u);
-    a.exact_rows[slot] = id;
-}
 
 // Pass 1 + completeness/tie decision.  Returns true when the row is exact on
 // the grid path; `R` is the final ring and `kk` the K-th key.
@@ -497,9 +365,7 @@ struct QueueLauncher {
 };
 
 template <int KS>
-__global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
-    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
+__device__ __forceinline__ void ids_row(const QueryArgs& a, const uint64_t i) {
     const GridParams g = *a.gp;
     const float4 q = __ldg(&a.gv.sorted[i]);
     const uint32_t id = __float_as_uint(q.w);
@@ -530,6 +396,24 @@ __global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
             --t;
         }
         row[t + 1] = v;
+    }
+}
+
+template <int KS>
+__global__ void __launch_bounds__(128) knn_ids_kernel(const QueryArgs a) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < a.n) ids_row<KS>(a, i);
+}
+
+// Rows the group select handed back (a.rows, a.nq_dev entries), answered by
+// the per-thread ring search: neighbour sums, or the neighbour-set export.
+template <int KS>
+__global__ void __launch_bounds__(128) knn_retry_kernel(const QueryArgs a) {
+    const uint32_t nr = *a.nq_dev;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += gridDim.x * blockDim.x) {
+        const uint32_t i = __ldg(&a.rows[r]);
+        if (a.ids_out) ids_row<KS>(a, i);
+        else select_row<KS>(a, i);
     }
 }
 
@@ -1132,7 +1016,13 @@ struct LaunchArgs {
     QueryArgs q;
     cudaStream_t stream;
     bool ids;
+    int group = 0;        // queries per group of the group select (0: per-thread select)
+    float margin0 = 0.25f;
+    int sms = 148;
 };
+
+int launch_group_select(const QueryArgs& q, int slots, int group, float margin0,
+                        cudaStream_t stream);
 
 template <int KS>
 struct KnnLauncher {
@@ -1142,6 +1032,25 @@ struct KnnLauncher {
         const uint64_t rows = la.q.rows ? la.q.nq : la.q.n;
         const uint64_t blocks = (rows + threads - 1) / threads;
         if (blocks == 0) return NBG_OK;
+        if (la.group && (la.ids || la.q.sums)) {
+            // group select, then the rows it handed back through the per-thread
+            // select (count read on the device), then the finish pass
+            if (cudaMemsetAsync(la.q.counters + 6, 0, sizeof(uint32_t), la.stream))
+                return NBG_ERR_CUDA;
+            int rc = launch_group_select(la.q, KS, la.group, la.margin0, la.stream);
+            if (rc) return rc;
+            QueryArgs r = la.q;
+            r.rows = la.q.retry_rows;
+            r.nq_dev = la.q.counters + 6;
+            knn_retry_kernel<KS><<<(unsigned)std::min<uint64_t>(blocks, (uint64_t)la.sms * 4), threads,
+                                   0, la.stream>>>(r);
+            NBG_LAUNCHED(1);
+            if (!la.ids) {
+                knn_finish_kernel<<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
+                NBG_LAUNCHED(1);
+            }
+            return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+        }
         if (la.ids) {
             knn_ids_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
             NBG_LAUNCHED(1);
@@ -1185,16 +1094,23 @@ int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
     la.q.row_k = ql.row_k;
     la.q.rows = ql.sums ? ql.rows : nullptr;  // the fused kernel answers every row
     la.q.nq = ql.sums ? ql.nrows : 0;
+    la.q.retry_rows = ql.retry_rows;
     la.stream = stream;
     la.ids = false;
+    la.group = ql.retry_rows ? ql.group : 0;
+    la.margin0 = ql.margin0;
+    la.sms = ctx ? ctx->sm_count : 148;
     return dispatch_slots<KnnLauncher>(ql.K, la);
 }
 
 int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
                          uint32_t* exact_rows, uint32_t* counters, uint2* ties, uint32_t tie_cap,
-                         cudaStream_t stream) {
-    (void)ctx;
+                         cudaStream_t stream, uint32_t* retry_rows) {
     LaunchArgs la{};
+    la.group = retry_rows ? t->group : 0;
+    la.margin0 = t->margin0;
+    la.sms = ctx ? ctx->sm_count : 148;
+    la.q.retry_rows = retry_rows;
     la.q.gv = grid_view(t);
     la.q.gp = t->gp;
     la.q.n = t->n;

@@ -234,6 +234,14 @@ int nbg_tile_free(nbg_context* ctx, nbg_tile* tile);
  * (the grid is rebuilt).  Used by the autotuner; no counterpart in the
  * reference (whose KD tree has no tunable). */
 int nbg_tile_tune(nbg_context* ctx, nbg_tile* tile, float cell_factor, int32_t fixed_cell);
+/* Select kernel of a tile: queries_per_group 8, 16 or 32 lets that many
+ * neighbouring queries (a block-local Morton order makes them compact) share
+ * one candidate list, gathered box ring by box ring with a first margin of
+ * first_margin cell edges (default 32 and 0.25); 0 selects the per-thread
+ * ring search.  Results are identical for every setting.  Used by the
+ * autotuner; no counterpart in the reference. */
+int nbg_tile_set_group(nbg_context* ctx, nbg_tile* tile, int32_t queries_per_group,
+                       float first_margin);
 /* Autotuner: builds the tile's grid with each candidate cell factor (null:
  * 1, 1.5, 2, 3, 4, 6), times the select pass on a sample of four waves of
  * blocks taken as runs of 32 consecutive 128-row blocks spread over the tile,
