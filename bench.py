@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the extra stages / consumers / LAS ingest leg")
+    ap.add_argument("--cpu-only", action="store_true",
+                    help="(internal) time the CPU baselines in this fresh process and print them "
+                         "as one JSON object")
     return ap.parse_args()
 
 
@@ -338,9 +341,21 @@ def cpu_reference_stage(x, y, z, st, kopt, ropt, sample=250_000):
             "sample": f"{int(m.sum())}-point window of the same tile: KD build + the stage"}
 
 
-def extras_leg(ctx, args):
-    """The §8f rows measured: each extra stage on the 4M mixture (device
-    inputs, one fresh tile per step), and LAS ingest of the same points."""
+def extras_cpu(sample=250_000):
+    """The reference's CPU loop of every extra stage on its window of the 4M
+    mixture (run in the CPU-only process)."""
+    from gpupdal_b200 import synthetic as syn
+    x, y, z = syn.mixture(4_000_000, 1)
+    kopt, ropt = syn.optimal_columns(len(x), 1, knn=10)
+    return {label: cpu_reference_stage(x, y, z, st, kopt, ropt, sample)
+            for label, st in extras_cases()}
+
+
+def extras_leg(ctx, args, cpu=None):
+    """The remaining stage options and the other kNN consumers measured: each
+    extra stage on the 4M mixture (device inputs, one fresh tile per step),
+    beside the reference's CPU loop timed in the CPU-only process (`cpu`),
+    and LAS ingest of the same points."""
     import tempfile
     import torch
     from gpupdal_b200 import las
@@ -352,7 +367,8 @@ def extras_leg(ctx, args):
     dx, dy, dz = (torch.from_numpy(v).to(dev) for v in (x, y, z))
     dk, dr = torch.from_numpy(kopt).to(dev), torch.from_numpy(ropt).to(dev)
     out = {"workload": f"mixture tile {n} points (seed 1), one stage per entry, device inputs "
-                       "and outputs, a fresh tile (upload + grid + KD replica) every step"}
+                       "and outputs, a fresh tile every step; cpu: oracle/_ref on a 250k-point "
+                       "window, all host threads"}
 
     def timed_ms(fn, steps=3):
         fn()
@@ -372,11 +388,11 @@ def extras_leg(ctx, args):
             tile.free()
         try:
             ms = timed_ms(step)
-            e = {"ms": ms, "mpts_s": n / ms / 1e3}
-            if not args.no_cpu_baseline:
-                cb = cpu_reference_stage(x, y, z, st, kopt, ropt)
-                e["cpu_baseline"] = cb
-                e["vs_cpu"] = e["mpts_s"] / cb["value"]
+            e = {"ms": round(ms, 3), "mpts_s": round(n / ms / 1e3, 1)}
+            cb = (cpu or {}).get(label)
+            if cb:
+                e["cpu_mpts_s"] = round(cb["value"], 3)
+                e["vs_cpu"] = round(e["mpts_s"] / cb["value"], 1)
         except Exception as exc:  # recorded, not fatal to the main line
             e = {"error": str(exc)}
         out[label] = e
@@ -397,8 +413,8 @@ def extras_leg(ctx, args):
             ctx.tile_from_las(f, records=drec).free()
         for label, fn in (("las ingest host records", up_host), ("las ingest device records", up_dev)):
             ms = timed_ms(fn)
-            out[label] = {"ms": ms, "mpts_s": n / ms / 1e3, "gb_s": nbytes / ms / 1e6,
-                          "record_bytes": int(f.record_length)}
+            out[label] = {"ms": round(ms, 3), "mpts_s": round(n / ms / 1e3, 1),
+                          "gb_s": round(nbytes / ms / 1e6, 1), "record_bytes": int(f.record_length)}
     return out
 
 
@@ -409,6 +425,7 @@ def batched_leg(ctx, args):
     from gpupdal_b200 import batched
     tset = batched.make_set(args.batch_tiles, seed=100)
     pts = sum(t["n"] for t in tset)
+    torch.cuda.synchronize()
 
     def timed(fn, steps):
         torch.cuda.synchronize()
@@ -426,20 +443,16 @@ def batched_leg(ctx, args):
     fixed_ms, st_fixed = timed(lambda: batched.step_batched(ctx, tset), steps)
     batched.step_batched(ctx, tset, autotune=True)  # tunes each size/knn class once
     tuned_ms, st_tuned = timed(lambda: batched.step_batched(ctx, tset, autotune=True), steps)
-    sizes = np.array([t["n"] for t in tset])
     return {
-        "set": (f"{len(tset)} tiles, sizes log-normal (median 200k, sigma 1.0) clipped to "
-                f"[20k, 4M] ({int(sizes.min())}-{int(sizes.max())}), subsamples of one 8M "
-                "mixture cloud (seed 100), knn in {8,16,32}, normal + covariancefeatures(all); "
-                "device-resident inputs and outputs, tiles re-uploaded every step"),
+        "set": (f"{len(tset)} compact mixture tiles, seeds 100-{99 + len(tset)}, sizes "
+                "log-normal (median 200k, sigma 1) in [20k, 4M], knn in {8,16,32}, "
+                "normal + covariancefeatures(all), device-resident, one graph-captured launch"),
         "points": int(pts),
-        "plain_mpts_s": pts / plain_ms / 1e3,
-        "batched_mpts_s": pts / fixed_ms / 1e3,
-        "batched_autotuned_mpts_s": pts / tuned_ms / 1e3,
-        "batched_vs_plain": plain_ms / fixed_ms,
-        "graph": True,
-        "query_ms": st_fixed[-1].query_ms, "kd_build_ms": st_fixed[-1].kd_build_ms,
-        "tree_ms": st_fixed[-1].tree_ms, "grid_ms": st_fixed[-1].grid_ms,
+        "plain": round(pts / plain_ms / 1e3, 1),
+        "batched": round(pts / fixed_ms / 1e3, 1),
+        "autotuned": round(pts / tuned_ms / 1e3, 1),
+        "batched_vs_plain": round(plain_ms / fixed_ms, 2),
+        "query_ms": round(st_fixed[-1].query_ms, 2), "kd_build_ms": round(st_fixed[-1].kd_build_ms, 2),
     }
 
 
@@ -449,7 +462,7 @@ def served_leg(ctx, args):
     arrivals (latency)."""
     from gpupdal_b200 import served
     from gpupdal_b200.native import Server
-    reqs = served.make_stream(args.served_requests, seed=1000)
+    reqs = served.make_requests(args.served_requests, seed=1000)
     pts = sum(len(r["x"]) for r in reqs)
     served.run_plain(ctx, reqs)  # warm-up pass: the plain context's block cache
     plain_s = sum(served.run_plain(ctx, reqs))
@@ -466,17 +479,18 @@ def served_leg(ctx, args):
         srv.close()
     lat_ms = np.sort(np.array(lat) * 1e3)
     return {
-        "stream": (f"{len(reqs)} requests, sizes log-uniform 10k-8M of the mixture (subsamples of "
-                   "one 8M cloud, seed 1000), knn in {8,16,32,64}, normal/eigenvalues/"
-                   "covariancefeatures(all) in equal shares; host buffers in and out"),
-        "points": pts,
-        "plain_mpts_s": pts / plain_s / 1e6,
-        "served_mpts_s": pts / cap_s / 1e6,
-        "served_vs_plain": plain_s / cap_s,
-        "slots": args.served_slots, "hbm_budget_gb": 120,
+        "stream": (f"bounded sample of the 2,000-request stream: requests 0-{len(reqs) - 1} "
+                   f"(own tile seeds 1000-{999 + len(reqs)}), sizes log-uniform 10k-8M, knn in "
+                   "{8,16,32,64}, normal/eigenvalues/covariancefeatures(all); host buffers; "
+                   "120 GB budget"),
+        "points": int(pts),
+        "plain_mpts_s": round(pts / plain_s / 1e6, 1),
+        "served_mpts_s": round(pts / cap_s / 1e6, 1),
+        "served_vs_plain": round(plain_s / cap_s, 2),
         "rate_req_s": args.served_rate,
-        "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
-        "rate_mpts_s": pts / rate_s / 1e6,
+        "p50_ms": round(float(np.percentile(lat_ms, 50)), 2),
+        "p99_ms": round(float(np.percentile(lat_ms, 99)), 2),
+        "rate_mpts_s": round(pts / rate_s / 1e6, 1),
     }
 
 
@@ -564,9 +578,45 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def cpu_only(args):
+    """The CPU baselines, timed in a process that has touched no GPU and runs
+    nothing else: the main workload's window (all host threads, and one
+    thread) and each extra stage's window.  Printed as one JSON object."""
+    x, y, z = workload(args.points, 2)
+    out = {"main": cpu_reference(x, y, z, args.knn, args.cpu_sample, single_thread=True)}
+    del x, y, z
+    if not args.no_extras:
+        out["extras"] = extras_cpu()
+    print(json.dumps(out), flush=True)
+
+
+def run_cpu_child(args):
+    """Runs cpu_only() in a fresh interpreter before this process starts any
+    GPU work (an in-process timing after the GPU legs read 40 % low: CUDA
+    contexts and their host threads share the cores)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-only", "--points", str(args.points),
+           "--knn", str(args.knn), "--cpu-sample", str(args.cpu_sample)]
+    if args.no_extras:
+        cmd.append("--no-extras")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900, env=env)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        return json.loads(lines[-1]) if lines else {"error": r.stderr[-400:]}
+    except Exception as exc:  # recorded, not fatal to the main line
+        return {"error": str(exc)}
+
+
 def main():
     args = parse()
+    if args.cpu_only:
+        cpu_only(args)
+        return
     ws, rank, local = dist_setup()
+    cpu = None
+    if (args.impl == "ours" and rank == 0 and ws == 1 and not args.no_cpu_baseline
+            and not args.served_sweep):
+        cpu = run_cpu_child(args)
     if args.impl == "reference":
         run_reference(args, ws, rank)
         if ws > 1:
@@ -689,6 +739,18 @@ def main():
                                 "throughput (8.9 of 32 lanes active per instruction)"},
         "clocks": clk,
     }
+    if cpu is not None:
+        cb = cpu.get("main")
+        if cb:
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                       "cpu_model", "nproc", "single_thread")}
+            line["cpu_baseline"]["process"] = "fresh process, before any GPU work"
+        else:
+            line["cpu_baseline"] = {"error": cpu.get("error", "no result")}
+    # the large legs first, the compact summaries last (the end of the line
+    # is what a log tail keeps)
+    if ws == 1 and not args.no_extras:
+        line["extras"] = extras_leg(ctx, args, (cpu or {}).get("extras"))
     if fp64 is not None:
         line["eigen_fp64"] = fp64
     if ws == 1 and not args.no_extras:
@@ -700,12 +762,6 @@ def main():
         line["batched"] = batched_leg(ctx, args)
     if ws == 1 and not args.no_served:
         line["served"] = served_leg(ctx, args)
-    if ws == 1 and not args.no_extras:
-        line["extras"] = extras_leg(ctx, args)
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cb = cpu_reference(x, y, z, args.knn, args.cpu_sample, single_thread=True)
-        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
-                                                   "cpu_model", "nproc", "single_thread")}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -4,8 +4,9 @@ A set is `count` tiles with log-normal sizes (median 200k points, sigma 1.0,
 clipped to [20k, 4M]) of the building/vegetation/terrain mixture, knn uniform
 in {8, 16, 32} per tile, and each tile running filters.normal plus
 filters.covariancefeatures (feature_set=all, with OptimalKNN/OptimalRadius
-columns).  Tiles are uniform subsamples of one pre-generated, pre-shuffled
-mixture cloud, so a set of ~10^8 points generates in seconds.
+columns).  Tile i is a compact mixture tile of its own seed (seed + i, the
+seeds 100-355 of the batched configuration by default), generated in
+parallel worker processes.
 
 Coordinates, OptimalKNN/OptimalRadius and outputs stay device-resident; a
 step uploads every tile from its resident coordinates (a fresh tile: grid and
@@ -24,26 +25,25 @@ from .native import record_columns
 RECORD = 128  # bytes per point: NormalX..Curvature (4) + 11 features, padded
 
 
-def make_set(count=256, seed=100, pool_points=8_000_000, median=200_000, sigma=1.0,
-             lo=20_000, hi=4_000_000, device="cuda"):
+def make_set(count=256, seed=100, median=200_000, sigma=1.0, lo=20_000, hi=4_000_000,
+             device="cuda"):
+    """`count` compact tiles: tile i is syn.tile(n_i, seed + i) (the mixture at
+    16 points per square metre, its own seed), n_i log-normal (median, sigma)
+    clipped to [lo, hi], knn uniform in {8, 16, 32}."""
     import torch
     rng = np.random.default_rng(seed)
-    x, y, z = syn.mixture(pool_points, seed)
-    perm = rng.permutation(pool_points)
-    x, y, z = x[perm], y[perm], z[perm]
-    sizes = np.clip(np.exp(rng.normal(np.log(median), sigma, count)), lo, min(hi, pool_points))
+    sizes = syn.batched_sizes(count, seed, median, sigma, lo, hi)
+    clouds = syn.tiles(sizes, [seed + i for i in range(count)])
     tiles = []
-    for i in range(count):
-        n = int(sizes[i])
-        s0 = int(rng.integers(0, pool_points))
-        idx = (s0 + np.arange(n)) % pool_points
+    for i, (x, y, z) in enumerate(clouds):
+        n = len(x)
         knn = int(rng.choice((8, 16, 32)))
         st = [abi.make_opts(abi.STAGE_NORMAL, knn=knn),
               abi.make_opts(abi.STAGE_COVARIANCEFEATURES, knn=knn, feature_mask=abi.FEAT_ALL)]
         kopt, ropt = syn.optimal_columns(n, seed + i, knn=knn)
-        dev = [torch.from_numpy(np.ascontiguousarray(v[idx])).to(device) for v in (x, y, z)]
+        dev = [torch.from_numpy(np.ascontiguousarray(v)).to(device) for v in (x, y, z)]
         rec = torch.empty((n, RECORD // 8), dtype=torch.float64, device=device)
-        tiles.append(dict(xyz=dev, n=n, knn=knn, stages=st, rec=rec,
+        tiles.append(dict(xyz=dev, n=n, knn=knn, stages=st, rec=rec, seed=seed + i,
                           cols=record_columns(rec.data_ptr(), st, RECORD, 1),
                           optimal=(torch.from_numpy(kopt).to(device), torch.from_numpy(ropt).to(device))))
     return tiles

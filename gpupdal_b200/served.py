@@ -4,9 +4,11 @@ A stream is a list of requests shaped like the served configuration: sizes
 log-uniform in [10k, 8M] points of the building/vegetation/terrain mixture,
 knn uniform in {8, 16, 32, 64}, and the stage normal, eigenvalues or
 covariancefeatures (feature_set=all, with OptimalKNN/OptimalRadius columns)
-in equal shares.  Requests are uniform subsamples of one pre-generated,
-pre-shuffled mixture cloud, handed out as views of it (so a stream of any
-length generates in seconds and submitting a request copies nothing).
+in equal shares.  make_requests() gives each request its own compact mixture
+tile and seed (the configuration's seeds 1000-2999); make_stream() hands out
+requests as views of one pre-generated, pre-shuffled mixture cloud instead,
+so that a 2,000-request rate sweep (2.4G points) costs host memory only for
+the pool and submitting a request copies nothing.
 
 run_plain() answers the requests one after another with the plain per-tile
 call (upload, nbg_run, free; host buffers in and out).  run_served() submits
@@ -80,6 +82,25 @@ def make_stream(count, seed=1000, pool_points=8_000_000, min_points=10_000,
         specs.append((s0, n, knn, kind))
     stream = Stream((x, y, z), specs, seed, max_points)
     return stream if lazy else list(stream)
+
+
+def make_requests(count, seed=1000, lo=10_000, hi=8_000_000):
+    """`count` requests of the served configuration, request i a compact
+    mixture tile of its own seed (seed + i: seeds 1000-2999 for the full
+    2,000-request stream), its size, knn and stage from syn.served_specs."""
+    specs = syn.served_specs(count, seed, lo, hi)
+    clouds = syn.tiles([s[0] for s in specs], [s[1] for s in specs])
+    reqs = []
+    for (n, rseed, knn, kind), (x, y, z) in zip(specs, clouds):
+        if kind == abi.STAGE_COVARIANCEFEATURES:
+            st = abi.make_opts(kind, knn=knn, feature_mask=abi.FEAT_ALL)
+            kopt, ropt = syn.optimal_columns(n, rseed, knn=knn)
+        else:
+            st = abi.make_opts(kind, knn=knn)
+            kopt = ropt = None
+        reqs.append(dict(x=x, y=y, z=z, stages=[st], kopt=kopt, ropt=ropt, knn=knn, kind=kind,
+                         seed=rseed))
+    return reqs
 
 
 def run_plain(ctx, reqs):

@@ -14,7 +14,9 @@ Workloads (sizes and mixtures of the benchmark configurations):
 * ``stress``       mixture + 2 % exact duplicates of random points + 3 %
                    collinear wire points on random lines at z = 10-25 m
 * ``tile``         the mixture on a square whose side keeps the mixture's
-                   density (16 points per square metre) for any point count
+                   density (16 points per square metre) for any point count;
+                   ``tiles`` makes many (one seed each) in parallel, the
+                   batched and served workloads' tiles
 """
 from __future__ import annotations
 
@@ -157,6 +159,37 @@ def tile(n, seed, density=16.0):
     rng = np.random.default_rng(seed)
     side = float(np.sqrt(n / density))
     return quantise(*_mixture(rng, n, side))
+
+
+def _tile_job(args):
+    n, seed = args
+    return tile(n, seed)
+
+
+def tiles(sizes, seeds, workers=None):
+    """Mixture tiles of the given sizes, one seed each (tile(n, seed)),
+    generated in parallel by a pool of fresh (spawned) processes."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    import os
+    jobs = [(int(n), int(s)) for n, s in zip(sizes, seeds)]
+    workers = workers or min(16, os.cpu_count() or 1, max(1, len(jobs)))
+    if workers <= 1 or len(jobs) <= 1:
+        return [_tile_job(j) for j in jobs]
+    with cf.ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_tile_job, jobs, chunksize=1))
+
+
+def served_specs(count=2000, seed=1000, lo=10_000, hi=8_000_000):
+    """The served stream's requests: (points, seed, knn, stage kind) each;
+    sizes log-uniform in [lo, hi], knn uniform in {8, 16, 32, 64}, the stage
+    normal / eigenvalues / covariancefeatures (1 / 2 / 3) in equal shares,
+    request i with its own tile seed seed + i."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(np.int64)
+    knn = rng.choice((8, 16, 32, 64), count)
+    kind = rng.integers(1, 4, count)
+    return [(int(sizes[i]), seed + i, int(knn[i]), int(kind[i])) for i in range(count)]
 
 
 def batched_sizes(count=256, seed=100, median=200_000, sigma=1.0, lo=20_000, hi=4_000_000):

@@ -51,3 +51,16 @@ def test_cpu_baseline_single_thread(bench):
     st = r["single_thread"]
     assert st["cores"] == 1 and st["value"] > 0 and st["seconds"] > 0
     assert r["cores"] == (os.cpu_count() or 1) and r["value"] > 0
+
+
+def test_cpu_baseline_runs_in_a_fresh_process(bench):
+    # the main line's CPU baselines come from a child interpreter that has
+    # touched no GPU; it prints one JSON object the main process reads
+    class A:
+        points, knn, cpu_sample, no_extras = 40_000, 8, 8_000, True
+    out = bench.run_cpu_child(A)
+    assert "error" not in out, out
+    main = out["main"]
+    assert main["value"] > 0 and main["cores"] == (os.cpu_count() or 1)
+    assert main["single_thread"]["cores"] == 1
+    assert "extras" not in out

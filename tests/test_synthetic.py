@@ -40,12 +40,27 @@ def test_batched_set_sizes_and_knn():
     assert len(s) == 256 and s.min() >= 20_000 and s.max() <= 4_000_000
     assert 120_000 < np.median(s) < 330_000     # log-normal around 200k
     from gpupdal_b200 import batched
-    tset = batched.make_set(count=12, seed=100, pool_points=1_000_000, device="cpu")
-    for t in tset:
+    tset = batched.make_set(count=12, seed=100, hi=1_000_000, device="cpu")
+    for i, t in enumerate(tset):
         assert t["knn"] in (8, 16, 32)
         kinds = [st.kind for st in t["stages"]]
         assert kinds == [abi.STAGE_NORMAL, abi.STAGE_COVARIANCEFEATURES]
         assert 20_000 <= t["n"] <= 1_000_000
+        # tile i: the mixture tile of its own seed 100 + i
+        assert t["seed"] == 100 + i
+        x, y, z = syn.tile(t["n"], 100 + i)
+        assert np.array_equal(t["xyz"][0].numpy(), x)
+
+
+def test_served_requests_own_seeds():
+    from gpupdal_b200 import served
+    reqs = served.make_requests(9, seed=1000, hi=300_000)
+    for i, r in enumerate(reqs):
+        assert r["seed"] == 1000 + i
+        x, y, z = syn.tile(len(r["x"]), 1000 + i)
+        assert np.array_equal(r["x"], x) and np.array_equal(r["z"], z)
+        assert r["knn"] in (8, 16, 32, 64)
+        assert 10_000 <= len(r["x"]) <= 300_000
 
 
 def test_served_stream_mix():
