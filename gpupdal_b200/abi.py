@@ -135,6 +135,7 @@ class RunStats(ctypes.Structure):
         ("outliers", ctypes.c_uint64),
         ("inliers", ctypes.c_uint64),
         ("output_chunks", ctypes.c_uint64),
+        ("retry_rows", ctypes.c_uint64),
     ]
 
 

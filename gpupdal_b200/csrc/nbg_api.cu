@@ -728,7 +728,7 @@ struct HostOut {
 // for bit.
 struct PipeStats {
     float query_ms = 0, tree_ms = 0, build_ms = 0;
-    uint64_t tie_rows = 0, deferred_rows = 0, replay_rows = 0;
+    uint64_t tie_rows = 0, deferred_rows = 0, replay_rows = 0, retry_rows = 0;
 };
 
 static int run_pipelined(Context* ctx, Tile* t, int K, const StageGroup& g, const ExceptionSink& sink,
@@ -764,13 +764,14 @@ static int run_pipelined(Context* ctx, Tile* t, int K, const StageGroup& g, cons
     auto finish_chunk = [&](int c) -> int {
         const uint32_t rows_c = (uint32_t)(b[c + 1] - b[c]);
         uint32_t* cnt_dev = ctx->counters + 8 * c;
-        uint32_t cnt[5] = {0, 0, 0, 0, 0};
+        uint32_t cnt[7] = {0, 0, 0, 0, 0, 0, 0};
         cudaError_t e = cudaStreamWaitEvent(ctx->side, sel[c], 0);
         if (!e) e = cudaMemcpyAsync(cnt, cnt_dev, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->side);
         if (!e) e = cudaStreamSynchronize(ctx->side);
         if (e) return fail(ctx, NBG_ERR_CUDA, std::string("query kernel: ") + cudaGetErrorString(e));
         ps.tie_rows += cnt[1];
         ps.deferred_rows += cnt[2];
+        ps.retry_rows += cnt[6];
         cudaEventRecord(t0[c], ctx->side);
         const uint32_t nties = std::min(cnt[4], rows_c);
         if (nties) {
@@ -1073,7 +1074,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     bool packed_copied = false;
     cudaEventRecord(ctx->ev[0], stream);
     float grid_ms = 0, query_ms = 0, tree_ms = 0;
-    uint64_t tie_rows = 0, deferred_rows = 0, replay_rows = 0;
+    uint64_t tie_rows = 0, deferred_rows = 0, replay_rows = 0, retry_rows = 0;
     float build_ms = 0;
     ExceptionSink sink{ctx->ex_rows, ctx->counters + 3, (uint32_t)std::max<uint32_t>(exception_capacity, 1)};
     if (cudaMemsetAsync(ctx->counters, 0, 64 * sizeof(uint32_t), stream)) { cleanup(); return NBG_ERR_CUDA; }
@@ -1179,6 +1180,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             tie_rows += ps.tie_rows;
             deferred_rows += ps.deferred_rows;
             replay_rows += ps.replay_rows;
+            retry_rows += ps.retry_rows;
             packed_copied = true;
             continue;
         }
@@ -1216,13 +1218,14 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             cudaEventRecord(ctx->xev[1], ctx->side);
             cudaStreamWaitEvent(stream, ctx->xev[1], 0);
         }
-        uint32_t cnt[5] = {0, 0, 0, 0, 0};
-        cudaError_t e = cudaMemcpyAsync(cnt, ctx->counters, 5 * sizeof(uint32_t),
+        uint32_t cnt[7] = {0, 0, 0, 0, 0, 0, 0};
+        cudaError_t e = cudaMemcpyAsync(cnt, ctx->counters, 7 * sizeof(uint32_t),
                                         cudaMemcpyDeviceToHost, stream);
         if (!e) e = cudaStreamSynchronize(stream);
         if (e) { cleanup(); return cuda_fail(ctx, e, "query kernel"); }
         tie_rows += cnt[1];
         deferred_rows += cnt[2];
+        retry_rows += cnt[6];
         float ms = 0;
         cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
         grid_ms += ms;
@@ -1329,6 +1332,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         stats->tree_ms = tree_ms;
         stats->kd_build_ms = build_ms;
         stats->output_chunks = packed_copied ? (uint64_t)pipe_chunks : 0;
+        stats->retry_rows = retry_rows;
         float ms = 0;
         cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[6]);
         stats->total_ms = ms;

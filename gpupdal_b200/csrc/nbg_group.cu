@@ -51,6 +51,7 @@ namespace nbg {
 template <int G>
 struct GroupShape {
     static constexpr int kThreads = G == 8 ? 128 : 256;
+    static constexpr int kMinBlocks = G == 8 ? 6 : 3;  // resident blocks per SM the registers allow
     static constexpr int kGroups = kThreads / G;
     static constexpr int kIdxBits = G == 32 ? 10 : 9;
     static constexpr uint32_t kCap = 1u << kIdxBits;
@@ -97,7 +98,7 @@ __device__ __forceinline__ int ring_for(const GridParams& g, const QueryCell& qc
 }
 
 template <int KS, int G>
-__global__ void __launch_bounds__(GroupShape<G>::kThreads)
+__global__ void __launch_bounds__(GroupShape<G>::kThreads, GroupShape<G>::kMinBlocks)
     knn_group_kernel(const QueryArgs a, const float margin0) {
     using S = GroupShape<G>;
     using Sort = cub::BlockRadixSort<uint32_t, S::kThreads, 1, uint32_t>;
@@ -441,7 +442,9 @@ static int launch_group_kg(const QueryArgs& q, float margin0, cudaStream_t strea
     if (!blocks) return NBG_OK;
     // the candidate lists and the sort's storage pass the 48 KB default
     if (cudaFuncSetAttribute(knn_group_kernel<KS, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)S::kSmem))
+                             (int)S::kSmem) ||
+        cudaFuncSetAttribute(knn_group_kernel<KS, G>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout, 100))
         return NBG_ERR_CUDA;
     knn_group_kernel<KS, G><<<(unsigned)blocks, S::kThreads, S::kSmem, stream>>>(q, margin0);
     NBG_LAUNCHED(1);

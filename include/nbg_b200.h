@@ -197,6 +197,8 @@ typedef struct nbg_run_stats {
     uint64_t output_chunks;   /* host records copied back in this many chunks of
                                  the point-id range, each while the later chunks
                                  were answered (0: one copy at the end)         */
+    uint64_t retry_rows;      /* rows the group select handed to the per-thread
+                                 ring search (see nbg_tile_set_group)           */
 } nbg_run_stats;
 
 typedef struct nbg_context nbg_context;
