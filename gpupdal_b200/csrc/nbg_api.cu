@@ -544,9 +544,9 @@ int nbg_tile_tune(nbg_context* h, nbg_tile* th, float cell_factor, int32_t fixed
 extern "C" int nbg_tile_set_group(nbg_context* h, nbg_tile* th, int32_t queries_per_group,
                                   float first_margin) {
     if (!h || !th) return NBG_ERR_INVALID;
-    if (queries_per_group != 0 && queries_per_group != 8 && queries_per_group != 16 &&
+    if (queries_per_group != 0 && queries_per_group != 1 && queries_per_group != 8 && queries_per_group != 16 &&
         queries_per_group != 32)
-        return fail(&h->c, NBG_ERR_INVALID, "queries per group must be 0, 8, 16 or 32");
+        return fail(&h->c, NBG_ERR_INVALID, "queries per group must be 0, 1, 8, 16 or 32");
     if (!(first_margin > 0.0f && first_margin <= 16.0f))
         return fail(&h->c, NBG_ERR_INVALID, "first margin must be in (0, 16] cell edges");
     std::lock_guard<std::mutex> lock(h->c.mu);

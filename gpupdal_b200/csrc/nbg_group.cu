@@ -65,16 +65,6 @@ struct GroupShape {
     static constexpr size_t kSmem = (size_t)kGroups * kGroupBytes;
 };
 
-// 10-bit Morton interleave of three coordinates.
-__device__ __forceinline__ uint32_t spread3(uint32_t v) {
-    v &= 0x3FFu;
-    v = (v | (v << 16)) & 0x030000FFu;
-    v = (v | (v << 8)) & 0x0300F00Fu;
-    v = (v | (v << 4)) & 0x030C30C3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
-
 template <int G>
 __device__ __forceinline__ int group_min(int v) {
 #pragma unroll
@@ -115,44 +105,10 @@ __global__ void __launch_bounds__(GroupShape<G>::kThreads, GroupShape<G>::kMinBl
     const GridParams g = *a.gp;
 
     // ---- block-local Morton order of the rows
-    uint32_t pos = 0;
-    int qi0 = 0, qi1 = 0, qi2 = 0;
-    if (tid < (int)nvalid) {
-        pos = a.rows ? __ldg(&a.rows[r0 + tid]) : (uint32_t)(r0 + tid);
-        const float4 q = __ldg(&a.gv.sorted[pos]);
-        qi0 = __float2int_rz(q.x);
-        qi1 = __float2int_rz(q.y);
-        qi2 = __float2int_rz(q.z);
-    }
-    if (tid < 6) s_box[tid] = tid < 3 ? INT_MAX : INT_MIN;
-    __syncthreads();
+    uint32_t pos;
     {
-        const bool v = tid < (int)nvalid;
-        const int lo0 = __reduce_min_sync(0xffffffffu, v ? qi0 : INT_MAX);
-        const int lo1 = __reduce_min_sync(0xffffffffu, v ? qi1 : INT_MAX);
-        const int lo2 = __reduce_min_sync(0xffffffffu, v ? qi2 : INT_MAX);
-        const int hi0 = __reduce_max_sync(0xffffffffu, v ? qi0 : INT_MIN);
-        const int hi1 = __reduce_max_sync(0xffffffffu, v ? qi1 : INT_MIN);
-        const int hi2 = __reduce_max_sync(0xffffffffu, v ? qi2 : INT_MIN);
-        if (lane == 0) {
-            atomicMin(&s_box[0], lo0);
-            atomicMin(&s_box[1], lo1);
-            atomicMin(&s_box[2], lo2);
-            atomicMax(&s_box[3], hi0);
-            atomicMax(&s_box[4], hi1);
-            atomicMax(&s_box[5], hi2);
-        }
-    }
-    __syncthreads();
-    {
-        const int ext = max(s_box[3] - s_box[0], max(s_box[4] - s_box[1], s_box[5] - s_box[2]));
-        const int sh = max(0, 32 - __clz(max(ext, 1)) - 10);  // (ext >> sh) < 1024
-        uint32_t key[1] = {0x7FFFFFFFu};
-        uint32_t val[1] = {pos};
-        if (tid < (int)nvalid)
-            key[0] = spread3((uint32_t)(qi0 - s_box[0]) >> sh) |
-                     (spread3((uint32_t)(qi1 - s_box[1]) >> sh) << 1) |
-                     (spread3((uint32_t)(qi2 - s_box[2]) >> sh) << 2);
+        uint32_t key[1], val[1];
+        block_morton_order<S::kThreads>(a, r0, nvalid, s_box, key, val);
         Sort(sort_tmp).Sort(key, val, 0, 31);  // rows past the end sort last
         pos = val[0];
     }

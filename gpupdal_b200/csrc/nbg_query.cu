@@ -24,6 +24,7 @@
 // row with no boundary tie has exactly the reference's neighbour set.
 #include <algorithm>
 
+#include <cub/block/block_radix_sort.cuh>
 #include <cub/device/device_select.cuh>
 #include <cub/iterator/counting_input_iterator.cuh>
 
@@ -242,6 +243,27 @@ __global__ void __launch_bounds__(128) knn_select_kernel(const QueryArgs a) {
     if (i >= (a.rows ? a.nq : a.n)) return;
     if (a.rows) i = __ldg(&a.rows[i]);
     select_row<KS>(a, i);
+}
+
+// The per-thread select with the queries of each block of 256 rows re-sorted
+// by a Morton key of their coordinates (block-local radix sort): a warp's 32
+// lanes are then spatially compact, so their ring searches visit nearly the
+// same cells (rows in cell order are random points of a cell that spans
+// several warps).
+template <int KS>
+__global__ void __launch_bounds__(256) knn_select_morton_kernel(const QueryArgs a) {
+    using Sort = cub::BlockRadixSort<uint32_t, 256, 1, uint32_t>;
+    __shared__ typename Sort::TempStorage sort_tmp;
+    __shared__ int s_box[6];
+    const uint64_t nrows = a.rows ? a.nq : a.n;
+    const uint64_t r0 = (uint64_t)blockIdx.x * 256u;
+    if (r0 >= nrows) return;
+    const int tid = threadIdx.x;
+    const uint32_t nvalid = (uint32_t)min((uint64_t)256, nrows - r0);
+    uint32_t key[1], val[1];
+    block_morton_order<256>(a, r0, nvalid, s_box, key, val);
+    Sort(sort_tmp).Sort(key, val, 0, 31);  // rows past the end sort last
+    if (tid < (int)nvalid) select_row<KS>(a, val[0]);
 }
 
 // Split form, finish: covariance, eigensolve and stage projections of the
@@ -1032,7 +1054,14 @@ struct KnnLauncher {
         const uint64_t rows = la.q.rows ? la.q.nq : la.q.n;
         const uint64_t blocks = (rows + threads - 1) / threads;
         if (blocks == 0) return NBG_OK;
-        if (la.group && (la.ids || la.q.sums)) {
+        if (la.group == 1 && la.q.sums && !la.ids) {
+            const uint64_t b256 = (rows + 255) / 256;
+            knn_select_morton_kernel<KS><<<(unsigned)b256, 256, 0, la.stream>>>(la.q);
+            knn_finish_kernel<<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
+            NBG_LAUNCHED(2);
+            return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+        }
+        if (la.group > 1 && (la.ids || la.q.sums)) {
             // group select, then the rows it handed back through the per-thread
             // select (count read on the device), then the finish pass
             if (cudaMemsetAsync(la.q.counters + 6, 0, sizeof(uint32_t), la.stream))

@@ -2,6 +2,8 @@
 // search, exact integer distance keys, register top list, row hand-off).
 #pragma once
 
+#include <climits>
+
 #include "nbg_common.cuh"
 
 namespace nbg {
@@ -138,6 +140,62 @@ __device__ __forceinline__ void defer_row(const QueryArgs& a, uint32_t id, bool 
     }
     const uint32_t slot = atomicAdd(&a.counters[0], 1u);
     a.exact_rows[slot] = id;
+}
+
+// 10-bit Morton interleave of three coordinates.
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+    v &= 0x3FFu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// Sort keys of a block's rows r0 .. r0 + nvalid - 1 (threads past nvalid get
+// a key above every row's): a Morton key of the row's coordinates relative to
+// the block's bounding box, at the resolution that fits the box in 10 bits
+// per axis; val = the row's sorted position.  s_box: 6 ints of shared memory.
+template <int THREADS>
+__device__ __forceinline__ void block_morton_order(const QueryArgs& a, uint64_t r0, uint32_t nvalid,
+                                                   int* s_box, uint32_t (&key)[1],
+                                                   uint32_t (&val)[1]) {
+    const int tid = threadIdx.x;
+    const bool v = tid < (int)nvalid;
+    uint32_t pos = 0;
+    int q0 = 0, q1 = 0, q2 = 0;
+    if (v) {
+        pos = a.rows ? __ldg(&a.rows[r0 + tid]) : (uint32_t)(r0 + tid);
+        const float4 q = __ldg(&a.gv.sorted[pos]);
+        q0 = __float2int_rz(q.x);
+        q1 = __float2int_rz(q.y);
+        q2 = __float2int_rz(q.z);
+    }
+    if (tid < 6) s_box[tid] = tid < 3 ? INT_MAX : INT_MIN;
+    __syncthreads();
+    const int lo0 = __reduce_min_sync(0xffffffffu, v ? q0 : INT_MAX);
+    const int lo1 = __reduce_min_sync(0xffffffffu, v ? q1 : INT_MAX);
+    const int lo2 = __reduce_min_sync(0xffffffffu, v ? q2 : INT_MAX);
+    const int hi0 = __reduce_max_sync(0xffffffffu, v ? q0 : INT_MIN);
+    const int hi1 = __reduce_max_sync(0xffffffffu, v ? q1 : INT_MIN);
+    const int hi2 = __reduce_max_sync(0xffffffffu, v ? q2 : INT_MIN);
+    if ((tid & 31) == 0) {
+        atomicMin(&s_box[0], lo0);
+        atomicMin(&s_box[1], lo1);
+        atomicMin(&s_box[2], lo2);
+        atomicMax(&s_box[3], hi0);
+        atomicMax(&s_box[4], hi1);
+        atomicMax(&s_box[5], hi2);
+    }
+    __syncthreads();
+    const int ext = max(s_box[3] - s_box[0], max(s_box[4] - s_box[1], s_box[5] - s_box[2]));
+    const int sh = max(0, 32 - __clz(max(ext, 1)) - 10);  // (ext >> sh) < 1024
+    key[0] = 0x7FFFFFFFu;
+    val[0] = pos;
+    if (v)
+        key[0] = spread3((uint32_t)(q0 - s_box[0]) >> sh) |
+                 (spread3((uint32_t)(q1 - s_box[1]) >> sh) << 1) |
+                 (spread3((uint32_t)(q2 - s_box[2]) >> sh) << 2);
 }
 
 }  // namespace nbg
