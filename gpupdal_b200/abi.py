@@ -196,7 +196,7 @@ class TuneEntry(ctypes.Structure):
         ("size_class", ctypes.c_int32),
         ("slots", ctypes.c_int32),
         ("cell_factor", ctypes.c_float),
-        ("reserved", ctypes.c_int32),
+        ("queries_per_group", ctypes.c_int32),
     ]
 
 

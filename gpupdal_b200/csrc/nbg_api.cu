@@ -1347,7 +1347,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
 namespace nbg {
 
 int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, int32_t n_candidates,
-                  bool use_cache, float* chosen, cudaStream_t stream) {
+                  bool use_cache, float* chosen, cudaStream_t stream, bool per_thread_only) {
     if (knn < 0 || knn > 64) return fail(ctx, NBG_ERR_INVALID, "knn must be in [0, 64]");
     static const float defaults[] = {1.0f, 1.5f, 2.0f, 3.0f, 4.0f, 6.0f};
     if (!candidates || n_candidates <= 0) {
@@ -1362,71 +1362,115 @@ int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, i
     const std::pair<int, int> key(lg, slots_for_k(K));
     auto hit = ctx->tuned.find(key);
     if (use_cache && hit != ctx->tuned.end()) {
-        if (t->cell_factor != hit->second) {
-            t->cell_factor = hit->second;
+        if (t->cell_factor != hit->second.first) {
+            t->cell_factor = hit->second.first;
             t->fixed_cell = 0;
             t->grid_valid = false;
         }
-        if (chosen) *chosen = hit->second;
+        t->group = hit->second.second;
+        if (chosen) *chosen = hit->second.first;
         return NBG_OK;
     }
     int rc = ensure_scratch(ctx, n, 1);
     if (rc) return rc;
-    // sample: runs of 32 consecutive blocks (4096 rows), four waves of 8 blocks
-    // per SM (one wave would time its slowest SM, not the throughput)
+    // sample: runs of 32 consecutive 128-row blocks (4096 rows) spread over the
+    // tile, four waves of 8 blocks per SM (one wave would time its slowest SM,
+    // not the throughput); neighbouring blocks share cells as in a full launch
     const uint64_t rows_total = (n + 127) / 128;
     const unsigned run = 32;
     const unsigned blocks = (unsigned)std::min<uint64_t>(rows_total, (uint64_t)ctx->sm_count * 32 / run * run);
-    const unsigned groups = std::max(1u, blocks / run);
-    const uint64_t stride = std::max<uint64_t>((uint64_t)run * 128, (n / groups) / 128 * 128);
-    const double scale = (double)n / ((double)blocks * 128.0);
+    const unsigned nruns = std::max(1u, blocks / run);
+    const uint64_t stride = std::max<uint64_t>((uint64_t)run * 128, (n / nruns) / 128 * 128);
+    std::vector<uint32_t> sample;
+    sample.reserve((size_t)blocks * 128);
+    for (unsigned b = 0; b < blocks; ++b) {
+        const uint64_t first = (b / run) * stride + (uint64_t)(b % run) * 128;
+        for (uint64_t r = first; r < first + 128 && r < n; ++r) sample.push_back((uint32_t)r);
+    }
+    const double scale = (double)n / (double)std::max<size_t>(sample.size(), 1);
+    uint32_t* rows_dev = nullptr;
+    rc = ctx_alloc(ctx, (void**)&rows_dev, sample.size() * 4 + 4);
+    if (rc) return rc;
+    rc = host_to_device(ctx, rows_dev, sample.data(), sample.size() * 4, stream);
+    if (rc) {
+        ctx_free(ctx, rows_dev, sample.size() * 4 + 4);
+        return rc;
+    }
+    // select kernels tried: the per-thread ring search, the same in Morton
+    // order, 32 queries per candidate list (the batched form's queue kernels
+    // are per-thread only)
+    static const int kGroups[] = {0, 1, 32};
+    const int ngroups = per_thread_only ? 1 : 3;
     uint32_t* cnt_dev = ctx->counters + 32;  // scratch block, not the call counters
     float best = candidates[0];
+    int best_group = 0;
     double best_ms = 1e300;
-    for (int c = 0; c < n_candidates; ++c) {
+    for (int c = 0; c < n_candidates && !rc; ++c) {
         const float cf = candidates[c];
-        if (!(cf > 0.0f) || cf > 64.0f) return fail(ctx, NBG_ERR_INVALID, "bad cell factor");
+        if (!(cf > 0.0f) || cf > 64.0f) {
+            rc = fail(ctx, NBG_ERR_INVALID, "bad cell factor");
+            break;
+        }
         t->cell_factor = cf;
         t->fixed_cell = 0;
         t->grid_valid = false;
         cudaEventRecord(ctx->ev[0], stream);
         rc = ensure_grid(ctx, t, K, stream);
-        if (rc) return rc;
+        if (rc) break;
         cudaEventRecord(ctx->ev[1], stream);
-        QueryLaunch ql;
-        ql.tile = t;
-        ql.K = K;
-        ql.rmax = 8;
-        ql.grp = StageGroup{};
-        ql.ex = ExceptionSink{ctx->ex_rows, cnt_dev + 3, 1};
-        ql.exact_rows = ctx->exact_rows;
-        ql.counters = cnt_dev;
-        ql.ties = ctx->ties;
-        ql.tie_cap = (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX);
-        ql.sums = ctx->sums;
-        cudaMemsetAsync(cnt_dev, 0, 8 * sizeof(uint32_t), stream);
-        cudaEventRecord(ctx->ev[2], stream);
-        rc = launch_select_sample(ctx, ql, stride, blocks, std::min(run, blocks), stream);
-        if (rc) return fail(ctx, rc, "autotune sample launch");
-        cudaEventRecord(ctx->ev[3], stream);
-        uint32_t cnt[3] = {0, 0, 0};
-        NBG_TRY(cudaMemcpyAsync(cnt, cnt_dev, sizeof(cnt), cudaMemcpyDeviceToHost, stream), "autotune");
-        NBG_TRY(cudaStreamSynchronize(stream), "autotune");
-        float build_ms = 0, sample_ms = 0;
-        cudaEventElapsedTime(&build_ms, ctx->ev[0], ctx->ev[1]);
-        cudaEventElapsedTime(&sample_ms, ctx->ev[2], ctx->ev[3]);
-        // rows the ring search cannot finish go to the search replay: charge
-        // each an estimated 5 us of replay
-        const double deferred = (double)cnt[0] * scale;
-        const double est = build_ms + sample_ms * scale + deferred * 0.005;
-        if (est < best_ms) {
-            best_ms = est;
-            best = cf;
+        for (int gi = 0; gi < ngroups; ++gi) {
+            const int G = kGroups[gi];
+            QueryLaunch ql;
+            ql.tile = t;
+            ql.K = K;
+            ql.rmax = 8;
+            ql.grp = StageGroup{};
+            ql.ex = ExceptionSink{ctx->ex_rows, cnt_dev + 3, 1};
+            ql.exact_rows = ctx->exact_rows;
+            ql.counters = cnt_dev;
+            ql.ties = ctx->ties;
+            ql.tie_cap = (uint32_t)std::min<uint64_t>(ctx->tie_cap, UINT32_MAX);
+            ql.sums = ctx->sums;
+            ql.rows = rows_dev;
+            ql.nrows = sample.size();
+            ql.retry_rows = ctx->retry_rows;
+            ql.group = G;
+            ql.margin0 = t->margin0;
+            cudaMemsetAsync(cnt_dev, 0, 8 * sizeof(uint32_t), stream);
+            cudaEventRecord(ctx->ev[2], stream);
+            rc = launch_query(ctx, ql, stream);
+            if (rc) {
+                rc = fail(ctx, rc, "autotune sample launch");
+                break;
+            }
+            cudaEventRecord(ctx->ev[3], stream);
+            uint32_t cnt[3] = {0, 0, 0};
+            cudaError_t e = cudaMemcpyAsync(cnt, cnt_dev, sizeof(cnt), cudaMemcpyDeviceToHost, stream);
+            if (!e) e = cudaStreamSynchronize(stream);
+            if (e) {
+                rc = fail(ctx, NBG_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+                break;
+            }
+            float build_ms = 0, sample_ms = 0;
+            cudaEventElapsedTime(&build_ms, ctx->ev[0], ctx->ev[1]);
+            cudaEventElapsedTime(&sample_ms, ctx->ev[2], ctx->ev[3]);
+            // rows the ring search cannot finish go to the search replay: charge
+            // each an estimated 5 us of replay
+            const double deferred = (double)cnt[0] * scale;
+            const double est = build_ms + sample_ms * scale + deferred * 0.005;
+            if (est < best_ms) {
+                best_ms = est;
+                best = cf;
+                best_group = G;
+            }
         }
     }
+    ctx_free(ctx, rows_dev, sample.size() * 4 + 4);
+    if (rc) return rc;
     t->cell_factor = best;
+    t->group = best_group;
     t->grid_valid = false;
-    ctx->tuned[key] = best;
+    ctx->tuned[key] = std::make_pair(best, best_group);
     if (chosen) *chosen = best;
     return NBG_OK;
 }
@@ -1454,8 +1498,8 @@ extern "C" int nbg_autotune_cache_get(nbg_context* h, nbg_tune_entry* entries, i
         if (i < capacity) {
             entries[i].size_class = kv.first.first;
             entries[i].slots = kv.first.second;
-            entries[i].cell_factor = kv.second;
-            entries[i].reserved = 0;
+            entries[i].cell_factor = kv.second.first;
+            entries[i].queries_per_group = kv.second.second;
         }
         ++i;
     }
@@ -1470,12 +1514,14 @@ extern "C" int nbg_autotune_cache_set(nbg_context* h, const nbg_tune_entry* entr
     for (int32_t i = 0; i < count; ++i) {
         const nbg_tune_entry& e = entries[i];
         if (e.size_class < 0 || e.size_class > 63 || e.slots < 1 || e.slots > 128 ||
-            !std::isfinite(e.cell_factor) || !(e.cell_factor > 0.0f))
+            !std::isfinite(e.cell_factor) || !(e.cell_factor > 0.0f) ||
+            (e.queries_per_group != 0 && e.queries_per_group != 1 && e.queries_per_group != 8 &&
+             e.queries_per_group != 16 && e.queries_per_group != 32))
             return fail(ctx, NBG_ERR_INVALID, "bad tuning-cache entry");
     }
     for (int32_t i = 0; i < count; ++i)
         ctx->tuned[std::make_pair((int)entries[i].size_class, (int)entries[i].slots)] =
-            entries[i].cell_factor;
+            std::make_pair(entries[i].cell_factor, (int)entries[i].queries_per_group);
     return NBG_OK;
 }
 

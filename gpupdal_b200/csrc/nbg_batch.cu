@@ -200,7 +200,7 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
     if (flags & NBG_BATCH_AUTOTUNE) {
         for (int i : live) {
             rc = tile_autotune(ctx, &items[i].tile->t, items[i].stages[0].knn, nullptr, 0, true,
-                               nullptr, st);
+                               nullptr, st, true);
             if (rc) return rc;
         }
     }

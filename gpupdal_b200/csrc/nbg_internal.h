@@ -70,8 +70,9 @@ struct Context {
     std::multimap<size_t, void*> cache;
     uint64_t cached = 0;
     std::unordered_map<void*, size_t> live;  // block sizes of handed-out blocks
-    // autotuner: chosen cell factor per (log2 points, neighbour slots) class
-    std::map<std::pair<int, int>, float> tuned;
+    // autotuner: chosen cell factor and select kernel (queries per group)
+    // per (log2 points, neighbour slots) class
+    std::map<std::pair<int, int>, std::pair<float, int>> tuned;
     // pinned bounce buffers for copies to and from pageable host memory
     char* bounce[2] = {nullptr, nullptr};
     cudaEvent_t bev[2];
@@ -243,7 +244,8 @@ int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t*
 
 // Autotuner (nbg_tile_autotune without the context lock).
 int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, int32_t n_candidates,
-                  bool use_cache, float* chosen, cudaStream_t stream);
+                  bool use_cache, float* chosen, cudaStream_t stream,
+                  bool per_thread_only = false);
 
 // A tile of n points with its device storage allocated (coordinates unset),
 // and its release (nbg_api.cu).

@@ -78,14 +78,15 @@ class Context:
         return buf
 
     def tuning_cache(self):
-        """The autotuner's cached choices: a list of
-        {"size_class", "slots", "cell_factor"} (nbg_autotune_cache_get)."""
+        """The autotuner's cached choices: a list of {"size_class", "slots",
+        "cell_factor", "queries_per_group"} (nbg_autotune_cache_get)."""
         count = ctypes.c_int32(0)
         self._check(self.lib.nbg_autotune_cache_get(self.h, None, 0, ctypes.byref(count)))
         buf = (abi.TuneEntry * max(count.value, 1))()
         self._check(self.lib.nbg_autotune_cache_get(self.h, buf, count.value, ctypes.byref(count)))
         return [{"size_class": int(e.size_class), "slots": int(e.slots),
-                 "cell_factor": float(e.cell_factor)} for e in buf[:count.value]]
+                 "cell_factor": float(e.cell_factor),
+                 "queries_per_group": int(e.queries_per_group)} for e in buf[:count.value]]
 
     def set_tuning_cache(self, entries):
         """Adds or replaces autotuner choices (nbg_autotune_cache_set)."""
@@ -94,6 +95,7 @@ class Context:
             e.size_class = int(d["size_class"])
             e.slots = int(d["slots"])
             e.cell_factor = float(d["cell_factor"])
+            e.queries_per_group = int(d.get("queries_per_group", 0))
         self._check(self.lib.nbg_autotune_cache_set(self.h, buf, len(entries)))
 
     def save_tuning(self, path):

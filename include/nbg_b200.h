@@ -248,9 +248,12 @@ int nbg_tile_set_group(nbg_context* ctx, nbg_tile* tile, int32_t queries_per_gro
  * 1, 1.5, 2, 3, 4, 6), times the select pass on a sample of four waves of
  * blocks taken as runs of 32 consecutive 128-row blocks spread over the tile,
  * and keeps the factor with the least estimated grid + query time (rows the
- * ring search would defer charged at 5 us each).  The choice is cached per
- * (log2 points, neighbour slots) class of the context; with use_cache a
- * cached class is applied without measuring. */
+ * ring search would defer charged at 5 us each).  For each factor it also
+ * times the select kernels of nbg_tile_set_group (per-thread ring search,
+ * the same in block-local Morton order, and 32 queries per candidate list)
+ * on the same sample rows, select + finish, and keeps the fastest pair.  The
+ * choice is cached per (log2 points, neighbour slots) class of the context;
+ * with use_cache a cached class is applied without measuring. */
 int nbg_tile_autotune(nbg_context* ctx, nbg_tile* tile, int32_t knn, const float* candidates,
                       int32_t n_candidates, int32_t use_cache, float* chosen, void* stream);
 
@@ -258,13 +261,14 @@ int nbg_tile_autotune(nbg_context* ctx, nbg_tile* tile, int32_t knn, const float
  * processes: one entry per (log2 points, neighbour slots) class.
  * nbg_autotune_cache_get writes up to `capacity` entries (sorted by class)
  * and the number the cache holds to *count; nbg_autotune_cache_set adds or
- * replaces entries (NBG_ERR_INVALID for a class outside [0, 63] x [1, 128]
- * or a factor that is not finite and positive; nothing is set then). */
+ * replaces entries (NBG_ERR_INVALID for a class outside [0, 63] x [1, 128],
+ * a factor that is not finite and positive, or a queries_per_group other
+ * than 0, 1, 8, 16, 32; nothing is set then). */
 typedef struct nbg_tune_entry {
     int32_t size_class;    /* floor(log2(points))                            */
     int32_t slots;         /* neighbour slots of the select kernel           */
     float cell_factor;
-    int32_t reserved;
+    int32_t queries_per_group; /* select kernel (nbg_tile_set_group)         */
 } nbg_tune_entry;
 int nbg_autotune_cache_get(nbg_context* ctx, nbg_tune_entry* entries, int32_t capacity,
                            int32_t* count);

@@ -1,6 +1,6 @@
-"""The autotuner's tuning file: choices made in one context, saved and loaded
-into a fresh context, are applied there without measuring (use_cache), and
-the cache refuses malformed entries."""
+"""The autotuner's tuning file: choices (cell factor and select kernel) made in
+one context, saved and loaded into a fresh context, are applied there without
+measuring (use_cache), and the cache refuses malformed entries."""
 import pytest
 
 from gpupdal_b200 import synthetic as syn
@@ -18,6 +18,8 @@ def test_tuning_file_round_trip(nbg, tmp_path):
     assert len(cache) >= 1
     # 1M points: class floor(log2 n) = 19
     assert any(e["size_class"] == 19 and e["cell_factor"] == chosen for e in cache)
+    # the select kernel is chosen with the cell factor
+    assert all(e["queries_per_group"] in (0, 1, 32) for e in cache)
     path = tmp_path / "tuning.json"
     nbg.save_tuning(path)
     fresh = Context(0)
@@ -33,6 +35,9 @@ def test_tuning_file_round_trip(nbg, tmp_path):
             fresh.set_tuning_cache([{"size_class": 19, "slots": 18, "cell_factor": -1.0}])
         with pytest.raises(NbgError):
             fresh.set_tuning_cache([{"size_class": 99, "slots": 18, "cell_factor": 2.0}])
+        with pytest.raises(NbgError):
+            fresh.set_tuning_cache([{"size_class": 19, "slots": 18, "cell_factor": 2.0,
+                                     "queries_per_group": 7}])
         assert fresh.tuning_cache() == cache
     finally:
         fresh.close()
