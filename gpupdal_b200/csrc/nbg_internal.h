@@ -120,10 +120,11 @@ struct Tile {
     bool fixed_storage = false;  // storage provided by the caller: never grow
     float cell_factor = 4.0f;
     int32_t fixed_cell = 0;
-    // select kernel: queries sharing one candidate list (8, 16, 32), or 0 for
-    // the per-thread ring search; first box margin in cell edges
-    int group = 32;
-    float margin0 = 0.25f;
+    // select kernel: 0 the per-thread ring search (default, fastest measured),
+    // 1 the same in block-local Morton order, 8 / 16 / 32 queries sharing one
+    // candidate list; the group select's first box margin in cell edges
+    int group = 0;
+    float margin0 = 0.5f;
     int grid_k1 = 0;
     int32_t grid_fixed = 0;      // fixed cell edge the current grid was built with (0: density)
     bool grid_valid = false;

@@ -330,9 +330,10 @@ class Tile:
         self.ctx._check(self.ctx.lib.nbg_tile_tune(self.ctx.h, self.h, float(cell_factor),
                                                    int(fixed_cell)))
 
-    def set_group(self, queries_per_group=32, first_margin=0.25):
-        """Select kernel: 8, 16 or 32 queries sharing one candidate list, or 0
-        for the per-thread ring search (results are identical)."""
+    def set_group(self, queries_per_group=0, first_margin=0.5):
+        """Select kernel: 8, 16 or 32 queries sharing one candidate list, 1 the
+        per-thread ring search in block-local Morton order, 0 (default) the
+        per-thread ring search; results are identical."""
         self.ctx._check(self.ctx.lib.nbg_tile_set_group(self.ctx.h, self.h, int(queries_per_group),
                                                         float(first_margin)))
 

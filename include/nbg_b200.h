@@ -239,9 +239,10 @@ int nbg_tile_tune(nbg_context* ctx, nbg_tile* tile, float cell_factor, int32_t f
 /* Select kernel of a tile: queries_per_group 8, 16 or 32 lets that many
  * neighbouring queries (a block-local Morton order makes them compact) share
  * one candidate list, gathered box ring by box ring with a first margin of
- * first_margin cell edges (default 32 and 0.25); 0 selects the per-thread
- * ring search.  Results are identical for every setting.  Used by the
- * autotuner; no counterpart in the reference. */
+ * first_margin cell edges; 1 selects the per-thread ring search with the
+ * queries of each 256-row block in Morton order, 0 (the default) the
+ * per-thread ring search.  Results are identical for every setting.  Used by
+ * the autotuner; no counterpart in the reference. */
 int nbg_tile_set_group(nbg_context* ctx, nbg_tile* tile, int32_t queries_per_group,
                        float first_margin);
 /* Autotuner: builds the tile's grid with each candidate cell factor (null:
