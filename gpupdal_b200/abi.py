@@ -196,7 +196,7 @@ class TuneEntry(ctypes.Structure):
         ("size_class", ctypes.c_int32),
         ("slots", ctypes.c_int32),
         ("cell_factor", ctypes.c_float),
-        ("queries_per_group", ctypes.c_int32),
+        ("select_kernel", ctypes.c_int32),
     ]
 
 
@@ -320,8 +320,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.nbg_tile_free.restype = ctypes.c_int
     lib.nbg_tile_tune.argtypes = [vp, vp, ctypes.c_float, i32]
     lib.nbg_tile_tune.restype = ctypes.c_int
-    lib.nbg_tile_set_group.argtypes = [vp, vp, i32, ctypes.c_float]
-    lib.nbg_tile_set_group.restype = ctypes.c_int
+    lib.nbg_tile_set_select.argtypes = [vp, vp, i32, ctypes.c_float]
+    lib.nbg_tile_set_select.restype = ctypes.c_int
     lib.nbg_tile_autotune.argtypes = [vp, vp, i32, ctypes.POINTER(ctypes.c_float), i32, i32,
                                       ctypes.POINTER(ctypes.c_float), vp]
     lib.nbg_tile_autotune.restype = ctypes.c_int

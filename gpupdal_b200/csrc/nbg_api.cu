@@ -541,16 +541,19 @@ int nbg_tile_tune(nbg_context* h, nbg_tile* th, float cell_factor, int32_t fixed
     return NBG_OK;
 }
 
-extern "C" int nbg_tile_set_group(nbg_context* h, nbg_tile* th, int32_t queries_per_group,
-                                  float first_margin) {
+static bool valid_select(int32_t k) {
+    return k == 0 || k == 1 || k == 2 || k == 8 || k == 16 || k == 32;
+}
+
+extern "C" int nbg_tile_set_select(nbg_context* h, nbg_tile* th, int32_t select_kernel,
+                                   float first_margin) {
     if (!h || !th) return NBG_ERR_INVALID;
-    if (queries_per_group != 0 && queries_per_group != 1 && queries_per_group != 8 && queries_per_group != 16 &&
-        queries_per_group != 32)
-        return fail(&h->c, NBG_ERR_INVALID, "queries per group must be 0, 1, 8, 16 or 32");
+    if (!valid_select(select_kernel))
+        return fail(&h->c, NBG_ERR_INVALID, "select kernel must be 0, 1, 2, 8, 16 or 32");
     if (!(first_margin > 0.0f && first_margin <= 16.0f))
         return fail(&h->c, NBG_ERR_INVALID, "first margin must be in (0, 16] cell edges");
     std::lock_guard<std::mutex> lock(h->c.mu);
-    th->t.group = queries_per_group;
+    th->t.group = select_kernel;
     th->t.margin0 = first_margin;
     return NBG_OK;
 }
@@ -1396,11 +1399,11 @@ int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, i
         ctx_free(ctx, rows_dev, sample.size() * 4 + 4);
         return rc;
     }
-    // select kernels tried: the per-thread ring search, the same in Morton
-    // order, 32 queries per candidate list (the batched form's queue kernels
-    // are per-thread only)
-    static const int kGroups[] = {0, 1, 32};
-    const int ngroups = per_thread_only ? 1 : 3;
+    // select kernels tried: the two-pass ring search, the same in Morton
+    // order, the single-pass ring search, 32 queries per candidate list (the
+    // batched form's queue kernels are the two-pass ring search only)
+    static const int kGroups[] = {0, 1, 2, 32};
+    const int ngroups = per_thread_only ? 1 : 4;
     uint32_t* cnt_dev = ctx->counters + 32;  // scratch block, not the call counters
     float best = candidates[0];
     int best_group = 0;
@@ -1499,7 +1502,7 @@ extern "C" int nbg_autotune_cache_get(nbg_context* h, nbg_tune_entry* entries, i
             entries[i].size_class = kv.first.first;
             entries[i].slots = kv.first.second;
             entries[i].cell_factor = kv.second.first;
-            entries[i].queries_per_group = kv.second.second;
+            entries[i].select_kernel = kv.second.second;
         }
         ++i;
     }
@@ -1515,13 +1518,12 @@ extern "C" int nbg_autotune_cache_set(nbg_context* h, const nbg_tune_entry* entr
         const nbg_tune_entry& e = entries[i];
         if (e.size_class < 0 || e.size_class > 63 || e.slots < 1 || e.slots > 128 ||
             !std::isfinite(e.cell_factor) || !(e.cell_factor > 0.0f) ||
-            (e.queries_per_group != 0 && e.queries_per_group != 1 && e.queries_per_group != 8 &&
-             e.queries_per_group != 16 && e.queries_per_group != 32))
+            !valid_select(e.select_kernel))
             return fail(ctx, NBG_ERR_INVALID, "bad tuning-cache entry");
     }
     for (int32_t i = 0; i < count; ++i)
         ctx->tuned[std::make_pair((int)entries[i].size_class, (int)entries[i].slots)] =
-            std::make_pair(entries[i].cell_factor, (int)entries[i].queries_per_group);
+            std::make_pair(entries[i].cell_factor, (int)entries[i].select_kernel);
     return NBG_OK;
 }
 

@@ -245,6 +245,205 @@ __global__ void __launch_bounds__(128) knn_select_kernel(const QueryArgs a) {
     select_row<KS>(a, i);
 }
 
+// ---------------------------------------------------------------------------
+// Single-pass select: the ring search of select_kth with keys that say where
+// the candidate lies, so the row's K nearest are read back directly instead
+// of re-scanning the rings for their sums (the second pass is about 40 % of
+// the two-pass kernel).  A key is
+//     d2 << (ob + 5) | slot << ob | offset
+// with d2 the exact integer squared distance (saturated at the field's top),
+// slot = (dx + 2) * 5 + (dy + 2) the candidate's column among the 5 x 5
+// around the query's, and offset its position in that column's run of cells
+// (from the column's first point).  Keys order as squared distances (the low
+// fields only separate equal distances, which the tie test compares without
+// them).  ob is chosen per tile so that d2 holds (2.2 c)^2 for cell edge c.
+// Rows this form cannot answer exactly -- a search past ring 2, an offset or
+// a K-th distance beyond its field, no neighbours at all -- go to the retry
+// list, which the two-pass kernel answers.
+struct LocFn {
+    float qx, qy, qz;
+    uint32_t ob;        // offset bits
+    uint32_t ib;        // index bits: ob + 5
+    uint32_t d2max;     // saturated squared distance
+    uint32_t colkey;    // the current column's slot << ob
+    uint32_t colbase;   // the current column's first point
+    bool bad;           // an inserted candidate's offset did not fit
+};
+
+template <int KS>
+__device__ __forceinline__ unsigned long long loc_limit(const TopK<KS>& top, const LocFn& f) {
+    const uint32_t d2 = top.k[KS - 1] >> f.ib;
+    return d2 >= f.d2max ? ~0ull : (unsigned long long)d2;
+}
+
+template <int KS>
+__device__ __forceinline__ void loc_candidate(TopK<KS>& top, LocFn& f, const float4 p, uint32_t j) {
+    const uint32_t key = dist_key(p.x - f.qx, p.y - f.qy, p.z - f.qz);
+    const uint32_t d2 = key < KEY_EXACT_END ? min(key - KEY_BASE, f.d2max) : f.d2max;
+    const uint32_t cand = d2 << f.ib;
+    if (cand < (top.k[KS - 1] & ~((1u << f.ib) - 1u))) {
+        const uint32_t off = j - f.colbase;
+        if (off >> f.ob) f.bad = true;
+        top.insert(cand | f.colkey | (off & ((1u << f.ob) - 1u)));
+    }
+}
+
+// Ring R of the located search (R <= 2): scan_shell's columns and z-reach,
+// with each column's slot and first point set before its points are keyed.
+template <int KS>
+__device__ __forceinline__ void loc_shell(const GridView& gv, const GridParams& g, const QueryCell& qc,
+                                          int R, TopK<KS>& top, LocFn& f) {
+    const int zlo = qc.cz - R, zhi = qc.cz + R;
+    const int c = g.cell;
+    for (int dy = -R; dy <= R; ++dy) {
+        const int y = qc.cy + dy;
+        if (y < 0 || y >= g.gy) continue;
+        const int ady = dy < 0 ? -dy : dy;
+        const int gy_ = slab_gap(qc.qy, y, c);
+        for (int dx = -R; dx <= R; ++dx) {
+            const int x = qc.cx + dx;
+            if (x < 0 || x >= g.gx) continue;
+            const int gx_ = slab_gap(qc.qx, x, c);
+            const long long h2 = (long long)gx_ * gx_ + (long long)gy_ * gy_;
+            const unsigned long long lim = loc_limit(top, f);
+            if ((unsigned long long)h2 > lim) continue;
+            const int4 ci = __ldg(&gv.colinfo[(uint32_t)y * (uint32_t)g.gx + (uint32_t)x]);
+            if (ci.z < ci.y) continue;
+            int zr0 = zlo, zr1 = zhi;
+            if (lim < (1ull << 46)) {
+                const float s = sqrtf((float)(lim - (unsigned long long)h2)) + 1.0f;
+                zr0 = max(zr0, (int)floorf(((float)qc.qz - s) / (float)c));
+                zr1 = min(zr1, (int)floorf(((float)qc.qz + s) / (float)c));
+            }
+            f.colkey = (uint32_t)((dx + 2) * 5 + (dy + 2)) << f.ob;
+            f.colbase = __ldg(&gv.cstart[(uint32_t)ci.x]);
+            const int adx = dx < 0 ? -dx : dx;
+            auto run = [&](int zl, int zh) {
+                zl = max(zl, ci.y);
+                zh = min(zh, ci.z);
+                if (zl > zh) return;
+                const uint32_t e0 = (uint32_t)ci.x + (uint32_t)(zl - ci.y);
+                const uint32_t e1 = (uint32_t)ci.x + (uint32_t)(zh - ci.y) + 1;
+                const uint32_t pe = __ldg(&gv.cstart[e1]);
+                for (uint32_t j = __ldg(&gv.cstart[e0]); j < pe; ++j)
+                    loc_candidate(top, f, __ldg(&gv.sorted[j]), j);
+            };
+            if (max(ady, adx) == R) {
+                run(zr0, zr1);
+            } else {
+                if (zlo >= zr0 && zlo <= zr1) run(zlo, zlo);
+                if (zhi >= zr0 && zhi <= zr1) run(zhi, zhi);
+            }
+        }
+    }
+}
+
+template <int KS>
+__device__ __forceinline__ void select_row_loc(const QueryArgs& a, const uint64_t i, uint32_t ob) {
+    const GridParams g = *a.gp;
+    const float4 q = __ldg(&a.gv.sorted[i]);
+    const uint32_t id = __float_as_uint(q.w);
+    const int K = row_neighbours(a.row_k, a.K, a.n, id);
+    auto retry = [&]() {
+        const uint32_t slot = atomicAdd(&a.counters[6], 1u);
+        a.retry_rows[slot] = (uint32_t)i;
+    };
+    if (K <= 0) {
+        retry();
+        return;
+    }
+    QueryCell qc;
+    qc.qx = __float2int_rz(q.x);
+    qc.qy = __float2int_rz(q.y);
+    qc.qz = __float2int_rz(q.z);
+    qc.cx = qc.qx / g.cell;
+    qc.cy = qc.qy / g.cell;
+    qc.cz = qc.qz / g.cell;
+    const int off = KS - (K + 1);
+    TopK<KS> top;
+    top.init(off);
+    LocFn f;
+    f.qx = q.x;
+    f.qy = q.y;
+    f.qz = q.z;
+    f.ob = ob;
+    f.ib = ob + 5;
+    f.d2max = (1u << (27 - ob)) - 1u;
+    f.bad = false;
+    bool complete = false;
+    int R;
+    for (R = 0; R <= 2; ++R) {
+        loc_shell(a.gv, g, qc, R, top, f);
+        const uint32_t kd = top.at(off + K - 1) >> f.ib;
+        const unsigned long long gap2 = outside_gap2(g, qc, R);
+        if (gap2 == ~0ull) {
+            complete = kd < f.d2max;
+            break;
+        }
+        if (kd < f.d2max && (unsigned long long)kd < gap2) {
+            complete = true;
+            break;
+        }
+    }
+    const uint32_t kk = top.at(off + K - 1) >> f.ib;
+    const uint32_t kk1 = top.at(off + K) >> f.ib;
+    if (!complete || f.bad || kk >= f.d2max || kk >= (1u << 23)) {
+        retry();
+        return;
+    }
+    if (kk1 == kk) {
+        atomicAdd(&a.counters[1], 1u);
+        defer_row(a, id, true, KEY_BASE + kk, R);
+        RowSums z;
+        z.cnt = 0;
+        a.sums[i] = z;
+        return;
+    }
+    int s1x = 0, s1y = 0, s1z = 0, sxx = 0, syx = 0, syy = 0, szx = 0, szy = 0, szz = 0;
+    const uint32_t omask = (1u << f.ob) - 1u;
+#pragma unroll
+    for (int s = 0; s < KS; ++s) {
+        if (s >= off && s < off + K) {
+            const uint32_t idx = top.k[s];
+            const uint32_t slot = (idx >> f.ob) & 31u;
+            const int dx = (int)(slot / 5) - 2, dy = (int)(slot % 5) - 2;
+            const int4 ci = __ldg(&a.gv.colinfo[(uint32_t)(qc.cy + dy) * (uint32_t)g.gx +
+                                                (uint32_t)(qc.cx + dx)]);
+            const float4 p = __ldg(&a.gv.sorted[__ldg(&a.gv.cstart[(uint32_t)ci.x]) + (idx & omask)]);
+            const int ix = small_int(p.x - q.x), iy = small_int(p.y - q.y), iz = small_int(p.z - q.z);
+            s1x += ix;
+            s1y += iy;
+            s1z += iz;
+            sxx += ix * ix;
+            syx += iy * ix;
+            syy += iy * iy;
+            szx += iz * ix;
+            szy += iz * iy;
+            szz += iz * iz;
+        }
+    }
+    RowSums out;
+    out.s[0] = s1x;
+    out.s[1] = s1y;
+    out.s[2] = s1z;
+    out.s[3] = sxx;
+    out.s[4] = syx;
+    out.s[5] = syy;
+    out.s[6] = szx;
+    out.s[7] = szy;
+    out.s[8] = szz;
+    out.cnt = K;
+    a.sums[i] = out;
+}
+
+template <int KS>
+__global__ void __launch_bounds__(128) knn_select_loc_kernel(const QueryArgs a, const uint32_t ob) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= (a.rows ? a.nq : a.n)) return;
+    if (a.rows) i = __ldg(&a.rows[i]);
+    select_row_loc<KS>(a, i, ob);
+}
+
 // The per-thread select with the queries of each block of 256 rows re-sorted
 // by a Morton key of their coordinates (block-local radix sort): a warp's 32
 // lanes are then spatially compact, so their ring searches visit nearly the
@@ -1034,13 +1233,23 @@ static int dispatch_slots(int K, typename Launcher<10>::Args args) {
     return NBG_ERR_INVALID;
 }
 
+// Offset bits of the single-pass select's keys for cell edge c: the squared
+// distance field (27 - ob bits) holds (2.2 c)^2, the search's reach at ring 2.
+static uint32_t loc_offset_bits(int32_t c) {
+    const double need = 4.84 * (double)std::max(c, 1) * (double)std::max(c, 1);
+    int bits = 1;
+    while (bits < 27 && (double)(1u << bits) < need) ++bits;
+    return (uint32_t)std::min(16, std::max(6, 27 - bits));
+}
+
 struct LaunchArgs {
     QueryArgs q;
     cudaStream_t stream;
     bool ids;
-    int group = 0;        // queries per group of the group select (0: per-thread select)
+    int group = 0;        // select kernel (nbg_tile_set_select; 0: two-pass per-thread)
     float margin0 = 0.25f;
     int sms = 148;
+    uint32_t ob = 11;     // single-pass select: offset bits of a key
 };
 
 int launch_group_select(const QueryArgs& q, int slots, int group, float margin0,
@@ -1054,6 +1263,21 @@ struct KnnLauncher {
         const uint64_t rows = la.q.rows ? la.q.nq : la.q.n;
         const uint64_t blocks = (rows + threads - 1) / threads;
         if (blocks == 0) return NBG_OK;
+        if (la.group == 2 && la.q.sums && !la.ids) {
+            // single pass with located keys; rows it hands back through the
+            // two-pass kernel (count read on the device); then the finish pass
+            if (cudaMemsetAsync(la.q.counters + 6, 0, sizeof(uint32_t), la.stream))
+                return NBG_ERR_CUDA;
+            knn_select_loc_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q, la.ob);
+            QueryArgs r = la.q;
+            r.rows = la.q.retry_rows;
+            r.nq_dev = la.q.counters + 6;
+            knn_retry_kernel<KS><<<(unsigned)std::min<uint64_t>(blocks, (uint64_t)la.sms * 4), threads,
+                                   0, la.stream>>>(r);
+            knn_finish_kernel<<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
+            NBG_LAUNCHED(3);
+            return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+        }
         if (la.group == 1 && la.q.sums && !la.ids) {
             const uint64_t b256 = (rows + 255) / 256;
             knn_select_morton_kernel<KS><<<(unsigned)b256, 256, 0, la.stream>>>(la.q);
@@ -1129,6 +1353,7 @@ int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
     la.group = ql.retry_rows ? ql.group : 0;
     la.margin0 = ql.margin0;
     la.sms = ctx ? ctx->sm_count : 148;
+    la.ob = loc_offset_bits(ql.tile->host_gp.cell);
     return dispatch_slots<KnnLauncher>(ql.K, la);
 }
 

@@ -79,14 +79,14 @@ class Context:
 
     def tuning_cache(self):
         """The autotuner's cached choices: a list of {"size_class", "slots",
-        "cell_factor", "queries_per_group"} (nbg_autotune_cache_get)."""
+        "cell_factor", "select_kernel"} (nbg_autotune_cache_get)."""
         count = ctypes.c_int32(0)
         self._check(self.lib.nbg_autotune_cache_get(self.h, None, 0, ctypes.byref(count)))
         buf = (abi.TuneEntry * max(count.value, 1))()
         self._check(self.lib.nbg_autotune_cache_get(self.h, buf, count.value, ctypes.byref(count)))
         return [{"size_class": int(e.size_class), "slots": int(e.slots),
                  "cell_factor": float(e.cell_factor),
-                 "queries_per_group": int(e.queries_per_group)} for e in buf[:count.value]]
+                 "select_kernel": int(e.select_kernel)} for e in buf[:count.value]]
 
     def set_tuning_cache(self, entries):
         """Adds or replaces autotuner choices (nbg_autotune_cache_set)."""
@@ -95,7 +95,7 @@ class Context:
             e.size_class = int(d["size_class"])
             e.slots = int(d["slots"])
             e.cell_factor = float(d["cell_factor"])
-            e.queries_per_group = int(d.get("queries_per_group", 0))
+            e.select_kernel = int(d.get("select_kernel", 0))
         self._check(self.lib.nbg_autotune_cache_set(self.h, buf, len(entries)))
 
     def save_tuning(self, path):
@@ -330,12 +330,13 @@ class Tile:
         self.ctx._check(self.ctx.lib.nbg_tile_tune(self.ctx.h, self.h, float(cell_factor),
                                                    int(fixed_cell)))
 
-    def set_group(self, queries_per_group=0, first_margin=0.5):
-        """Select kernel: 8, 16 or 32 queries sharing one candidate list, 1 the
-        per-thread ring search in block-local Morton order, 0 (default) the
-        per-thread ring search; results are identical."""
-        self.ctx._check(self.ctx.lib.nbg_tile_set_group(self.ctx.h, self.h, int(queries_per_group),
-                                                        float(first_margin)))
+    def set_select(self, kernel=0, first_margin=0.5):
+        """Select kernel (nbg_tile_set_select): 0 two-pass ring search
+        (default), 1 the same in block-local Morton order, 2 single-pass ring
+        search, 8 / 16 / 32 queries sharing one candidate list; results are
+        identical."""
+        self.ctx._check(self.ctx.lib.nbg_tile_set_select(self.ctx.h, self.h, int(kernel),
+                                                         float(first_margin)))
 
     def autotune(self, knn, candidates=None, use_cache=False):
         """Cell factor chosen by the library's autotuner (applied to the tile)."""

@@ -197,8 +197,8 @@ typedef struct nbg_run_stats {
     uint64_t output_chunks;   /* host records copied back in this many chunks of
                                  the point-id range, each while the later chunks
                                  were answered (0: one copy at the end)         */
-    uint64_t retry_rows;      /* rows the group select handed to the per-thread
-                                 ring search (see nbg_tile_set_group)           */
+    uint64_t retry_rows;      /* rows a faster select kernel handed to the
+                                 two-pass ring search (nbg_tile_set_select)     */
 } nbg_run_stats;
 
 typedef struct nbg_context nbg_context;
@@ -236,22 +236,25 @@ int nbg_tile_free(nbg_context* ctx, nbg_tile* tile);
  * (the grid is rebuilt).  Used by the autotuner; no counterpart in the
  * reference (whose KD tree has no tunable). */
 int nbg_tile_tune(nbg_context* ctx, nbg_tile* tile, float cell_factor, int32_t fixed_cell);
-/* Select kernel of a tile: queries_per_group 8, 16 or 32 lets that many
- * neighbouring queries (a block-local Morton order makes them compact) share
- * one candidate list, gathered box ring by box ring with a first margin of
- * first_margin cell edges; 1 selects the per-thread ring search with the
- * queries of each 256-row block in Morton order, 0 (the default) the
- * per-thread ring search.  Results are identical for every setting.  Used by
- * the autotuner; no counterpart in the reference. */
-int nbg_tile_set_group(nbg_context* ctx, nbg_tile* tile, int32_t queries_per_group,
-                       float first_margin);
+/* Select kernel of a tile (the k-nearest search of nbg_run; results are
+ * identical for every setting):
+ *   0  two-pass ring search, one query per thread (default)
+ *   1  the same with the queries of each 256-row block in Morton order
+ *   2  single-pass ring search: top-list keys carry the candidate's column and
+ *      position, so the K nearest are read back without a second scan
+ *   8, 16, 32  that many neighbouring queries (Morton-compact) share one
+ *      candidate list, gathered box ring by box ring from a first margin of
+ *      first_margin cell edges
+ * Rows the faster forms cannot answer exactly go to the two-pass search.
+ * Used by the autotuner; no counterpart in the reference. */
+int nbg_tile_set_select(nbg_context* ctx, nbg_tile* tile, int32_t select_kernel,
+                        float first_margin);
 /* Autotuner: builds the tile's grid with each candidate cell factor (null:
  * 1, 1.5, 2, 3, 4, 6), times the select pass on a sample of four waves of
  * blocks taken as runs of 32 consecutive 128-row blocks spread over the tile,
  * and keeps the factor with the least estimated grid + query time (rows the
  * ring search would defer charged at 5 us each).  For each factor it also
- * times the select kernels of nbg_tile_set_group (per-thread ring search,
- * the same in block-local Morton order, and 32 queries per candidate list)
+ * times the select kernels of nbg_tile_set_select (0, 1, 2 and 32)
  * on the same sample rows, select + finish, and keeps the fastest pair.  The
  * choice is cached per (log2 points, neighbour slots) class of the context;
  * with use_cache a cached class is applied without measuring. */
@@ -263,13 +266,13 @@ int nbg_tile_autotune(nbg_context* ctx, nbg_tile* tile, int32_t knn, const float
  * nbg_autotune_cache_get writes up to `capacity` entries (sorted by class)
  * and the number the cache holds to *count; nbg_autotune_cache_set adds or
  * replaces entries (NBG_ERR_INVALID for a class outside [0, 63] x [1, 128],
- * a factor that is not finite and positive, or a queries_per_group other
- * than 0, 1, 8, 16, 32; nothing is set then). */
+ * a factor that is not finite and positive, or a select kernel other than
+ * 0, 1, 2, 8, 16, 32; nothing is set then). */
 typedef struct nbg_tune_entry {
     int32_t size_class;    /* floor(log2(points))                            */
     int32_t slots;         /* neighbour slots of the select kernel           */
     float cell_factor;
-    int32_t queries_per_group; /* select kernel (nbg_tile_set_group)         */
+    int32_t select_kernel;     /* nbg_tile_set_select                        */
 } nbg_tune_entry;
 int nbg_autotune_cache_get(nbg_context* ctx, nbg_tune_entry* entries, int32_t capacity,
                            int32_t* count);

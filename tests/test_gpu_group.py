@@ -17,7 +17,7 @@ from tests import _util as U
 
 pytestmark = pytest.mark.gpu
 
-GROUPS = (0, 1, 8, 16, 32)
+GROUPS = (0, 1, 2, 8, 16, 32)
 
 
 def _clouds():
@@ -43,7 +43,7 @@ def test_group_sizes_agree_with_oracle(nbg, port, name, xyz):
     base = None
     for G in GROUPS:
         tile = nbg.tile(x, y, z)
-        tile.set_group(G)
+        tile.set_select(G)
         for k in (8, 16):
             ids, _ = nbg.neighbor_sets(tile, k)
             bad = np.flatnonzero((U.sorted_rows(ids) != want_ids[k]).any(axis=1))
@@ -70,7 +70,7 @@ def test_group_optimized_per_row_k(nbg):
     res = []
     for G in GROUPS:
         tile = nbg.tile(x, y, z)
-        tile.set_group(G)
+        tile.set_select(G)
         outs, ex, _ = nbg.run(tile, [st], optimal_knn=kopt, optimal_radius=ropt)
         tile.free()
         res.append((outs[0], np.sort(ex, order=["point_id", "stage"])))
@@ -84,6 +84,6 @@ def test_group_setting_refused(nbg):
     tile = nbg.tile(x, y, z)
     from gpupdal_b200.native import NbgError
     with pytest.raises(NbgError):
-        tile.set_group(12)
+        tile.set_select(12)
     with pytest.raises(NbgError):
-        tile.set_group(32, first_margin=0.0)
+        tile.set_select(32, first_margin=0.0)
