@@ -5,7 +5,8 @@
 // allocator, side stream, batch scratch) and a stream.  A free worker takes a
 // wave: every queued request, head first, while the bytes charged to running
 // requests plus the next estimate fit the budget (an idle server always
-// admits its head) and the wave stays within kWavePoints / kWaveItems.  The
+// admits its head), the wave stays within kWavePoints / kWaveItems and within
+// this worker's share of the queued points (split over the free workers).  The
 // wave's requests are uploaded, their grids, KD replicas and outputs held on
 // the device, and all of them answered by ONE nbg_run_batch call: a
 // persistent kernel per neighbour-count class drains a device queue of
@@ -73,7 +74,9 @@ struct nbg_server {
     std::unordered_map<uint64_t, nbg_request_result> done;
     uint64_t next_ticket = 1;
     uint64_t charged = 0;   // estimates of running requests
+    uint64_t queued_points = 0;
     int running = 0;
+    int idle = 0;           // workers waiting for a wave
     bool stop = false;
     std::vector<std::thread> workers;
     std::vector<nbg_context*> contexts;
@@ -298,22 +301,29 @@ void nbg_server::worker(int slot) {
         std::vector<Job> wave;
         {
             std::unique_lock<std::mutex> lk(mu);
+            ++idle;
             work_cv.wait(lk, [&] {
                 if (queue.empty()) return stop;
                 // FIFO: the head waits for memory; an idle server always admits
                 return running == 0 || !budget || charged + queue.front().est <= budget;
             });
+            // this worker's share of the queue: the waiting requests are split
+            // over the workers now free, so their waves run side by side
+            const uint64_t share = std::max<uint64_t>(1, queued_points / (uint64_t)std::max(idle, 1));
+            --idle;
             if (queue.empty()) break;
             uint64_t pts = 0;
             while (!queue.empty()) {
                 const Job& h = queue.front();
                 const bool fits = running == 0 || !budget || charged + h.est <= budget;
                 if (!fits) break;
-                if (!wave.empty() && (wave.size() >= kWaveItems || pts + h.req.n > kWavePoints))
+                if (!wave.empty() && (wave.size() >= kWaveItems || pts + h.req.n > kWavePoints ||
+                                      pts >= share))
                     break;
                 charged += h.est;
                 ++running;
                 pts += h.req.n;
+                queued_points -= h.req.n;
                 wave.push_back(std::move(queue.front()));
                 queue.pop_front();
             }
@@ -373,6 +383,7 @@ extern "C" int nbg_server_submit(nbg_server* s, const nbg_request* r, uint64_t* 
     job.ticket = s->next_ticket++;
     job.submit_us = s->now_us();
     *ticket = job.ticket;
+    s->queued_points += job.req.n;
     s->queue.push_back(std::move(job));
     s->work_cv.notify_all();
     return NBG_OK;
