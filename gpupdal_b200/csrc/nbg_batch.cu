@@ -8,10 +8,8 @@
 //              finish kernel then takes every item of every class.  The head
 //              resets and the launches are captured in a CUDA graph, replayed
 //              while the batch's job arrays and counts are unchanged.
-// 3. replicas  a host thread builds the tiles' KD replicas, all as one forest
-//              (one level-synchronous build for every tile), on the context's
-//              side stream while the queue drains (they depend only on the
-//              coordinates)
+// 3. replicas  the tiles' KD replicas, all as one forest (one level-synchronous
+//              build for every tile), once the queue has drained
 // 4. exact     per tile: the tie-order resolver, then the search replay for
 //              the rows it hands on, as in nbg_run
 // Each tile owns disjoint slices of the row-sum, tie and replay lists and
@@ -22,7 +20,6 @@
 #include <cstring>
 #include <map>
 #include <set>
-#include <thread>
 #include <vector>
 
 #include "nbg_internal.h"
@@ -316,12 +313,11 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
     cudaMemsetAsync(B->counters, 0, (size_t)nl * kCounters * sizeof(uint32_t), st);
     rc = host_to_device(ctx, B->jobs, jobs.data(), jobs.size() * sizeof(BatchJob), st);
     if (rc) return rc;
-    // tiles whose KD replica is built beside the queue
+    // tiles whose KD replica is built after the queue
     std::vector<Tile*> kd_tiles;
     for (int i : live)
         if (items[i].tile->t.n > 100 && !kd_built(&items[i].tile->t)) kd_tiles.push_back(&items[i].tile->t);
-    // the KD build beside the queue gains nothing from resident blocks left
-    // free (measured: the queue slows by more than the build gains)
+    // the persistent launches take every resident block slot
     const int reserve = 0;
     // ---- the queue launches, captured once per batch shape
     std::vector<uint64_t> key;
@@ -370,28 +366,26 @@ extern "C" int nbg_run_batch(nbg_context* h, const nbg_batch_item* items, int32_
         }
         B->key = key;
     }
-    // ---- KD replicas on the side stream (host thread), queue on st
+    // ---- the queue on st, then the KD replicas of its tiles as one forest.
+    // The forest's level passes are many short launches with host
+    // synchronisations between levels: beside the persistent queue kernels,
+    // which hold every resident block slot, each waited for free slots (the
+    // forest of 256 tiles took longer than the queue itself); after the queue
+    // they have the whole GPU.
     cudaEventRecord(B->ev[2], st);
-    int kd_rc = NBG_OK;
-    float kd_ms = 0;
-    std::thread kd_thread;
-    if (!kd_tiles.empty()) {
-        cudaStreamWaitEvent(ctx->side, B->ev[1], 0);
-        kd_thread = std::thread([&] {
-            cudaSetDevice(ctx->device);
-            cudaEventRecord(ctx->ev[8], ctx->side);
-            kd_rc = kd_ensure_many(ctx, kd_tiles.data(), (int)kd_tiles.size(), ctx->side);
-            cudaEventRecord(ctx->ev[9], ctx->side);
-            cudaStreamSynchronize(ctx->side);
-            cudaEventElapsedTime(&kd_ms, ctx->ev[8], ctx->ev[9]);
-        });
-    }
     int qrc = graph ? (cudaGraphLaunch(B->exec, st) == cudaSuccess ? NBG_OK : NBG_ERR_CUDA) : record(st);
     cudaEventRecord(B->ev[3], st);
     cudaError_t qe = cudaStreamSynchronize(st);
-    if (kd_thread.joinable()) kd_thread.join();
     if (qrc || qe != cudaSuccess) return fail(ctx, NBG_ERR_CUDA, "batch queue launch failed");
-    if (kd_rc) return kd_rc;
+    float kd_ms = 0;
+    if (!kd_tiles.empty()) {
+        cudaEventRecord(ctx->ev[8], st);
+        rc = kd_ensure_many(ctx, kd_tiles.data(), (int)kd_tiles.size(), st);
+        if (rc) return rc;
+        cudaEventRecord(ctx->ev[9], st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return fail(ctx, NBG_ERR_CUDA, "batch KD replicas");
+        cudaEventElapsedTime(&kd_ms, ctx->ev[8], ctx->ev[9]);
+    }
     // ---- exact rows per tile
     std::vector<uint32_t> cnt((size_t)nl * kCounters);
     cudaMemcpyAsync(cnt.data(), B->counters, cnt.size() * 4, cudaMemcpyDeviceToHost, st);
