@@ -542,14 +542,14 @@ int nbg_tile_tune(nbg_context* h, nbg_tile* th, float cell_factor, int32_t fixed
 }
 
 static bool valid_select(int32_t k) {
-    return k == 0 || k == 1 || k == 2 || k == 3 || k == 8 || k == 16 || k == 32;
+    return k == 0 || k == 1 || k == 2 || k == 8 || k == 16 || k == 32;
 }
 
 extern "C" int nbg_tile_set_select(nbg_context* h, nbg_tile* th, int32_t select_kernel,
                                    float first_margin) {
     if (!h || !th) return NBG_ERR_INVALID;
     if (!valid_select(select_kernel))
-        return fail(&h->c, NBG_ERR_INVALID, "select kernel must be 0, 1, 2, 3, 8, 16 or 32");
+        return fail(&h->c, NBG_ERR_INVALID, "select kernel must be 0, 1, 2, 8, 16 or 32");
     if (!(first_margin > 0.0f && first_margin <= 16.0f))
         return fail(&h->c, NBG_ERR_INVALID, "first margin must be in (0, 16] cell edges");
     std::lock_guard<std::mutex> lock(h->c.mu);
@@ -1400,11 +1400,10 @@ int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, i
         return rc;
     }
     // select kernels tried: the two-pass ring search, the same in Morton
-    // order, the single-pass ring search, the counting select, 32 queries per
-    // candidate list (the batched form's queue kernels are the two-pass ring
-    // search only)
-    static const int kGroups[] = {0, 1, 2, 3, 32};
-    const int ngroups = per_thread_only ? 1 : 5;
+    // order, the single-pass ring search, 32 queries per candidate list (the
+    // batched form's queue kernels are the two-pass ring search only)
+    static const int kGroups[] = {0, 1, 2, 32};
+    const int ngroups = per_thread_only ? 1 : 4;
     uint32_t* cnt_dev = ctx->counters + 32;  // scratch block, not the call counters
     float best = candidates[0];
     int best_group = 0;

@@ -465,339 +465,6 @@ __global__ void __launch_bounds__(256) knn_select_morton_kernel(const QueryArgs 
     if (tid < (int)nvalid) select_row<KS>(a, val[0]);
 }
 
-// ---------------------------------------------------------------------------
-// Counting select: the ring search of select_kth with neither a register top
-// list nor per-column inner loops.  Two things keep a warp of per-thread ring
-// searches from issuing with its lanes together: the nested column / cell
-// loops (a lane that pruned a column, or whose z-run there is shorter, waits
-// for the others at every column), and the top list's insertion network,
-// which the whole warp runs whenever any lane inserts.  Here:
-//   * rings 0 and 1 are walked flat: each lane first lists the point ranges
-//     of the ring's cells that can hold a point within its bound (at most 10
-//     ranges), then one loop walks its own ranges back to back, so lanes
-//     leave the loop only when their own candidates run out;
-//   * each lane counts its candidates into a histogram of log-spaced squared
-//     distance bins in shared memory (four bins per octave of d2 + 1, read
-//     from the float bits of d2 + 1, which the FMA chain forms exactly below
-//     2^24): one shared-memory add per candidate.
-//   pass 1  rings 0, 1, ...: count; the K-th nearest lies in the first bin bK
-//           where the running count reaches K.  The row is complete once every
-//           squared distance of bins <= bK is below the squared gap to the
-//           unscanned cells; later rings skip what lies beyond bin bK.
-//   pass 2  the same rings: candidates of bins < bK are among the K nearest
-//           and go straight into the exact int32 sums; the few of bin bK are
-//           kept (squared distance and offsets in one 64-bit entry) and
-//           sorted, which gives the exact K-th and (K+1)-th distances: a tie
-//           goes to the tie list, otherwise the first K - (count below bK)
-//           entries complete the sums.
-// Rings from 2 up (sparse regions) use scan_shell.  Bin 92 holds every
-// squared distance from 2^23 - 1 up (beyond the exact keys): a K-th nearest
-// there defers the row, as select_kth does.  Counts are 8 bits: a bin that
-// wraps (or carries into the next) makes pass 2 disagree with pass 1's counts
-// below and in bin bK, and such rows, and rows whose bin bK holds more entries
-// than a lane keeps, go to the retry list, answered by the two-pass kernel.
-static constexpr int CNT_THREADS = 128;
-static constexpr int CNT_BINS = 93;
-static constexpr int CNT_WORDS = (CNT_BINS + 3) / 4;  // four 8-bit counts per word
-static constexpr int CNT_BUF = 12;                    // bin-bK entries a lane keeps
-static constexpr int CNT_RANGES = 10;                 // point ranges of ring 0 or 1
-
-// d2 + 1 for an offset of exact small integers (exact while below 2^24)
-__device__ __forceinline__ float cnt_d2p1(float dx, float dy, float dz) {
-    return fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 1.0f)));
-}
-
-__device__ __forceinline__ int cnt_bin(float d2p1) {
-    return min((int)(__float_as_uint(d2p1) >> 21) - 508, CNT_BINS - 1);
-}
-
-// Largest integer squared distance whose bin is <= b (b < CNT_BINS - 1):
-// bin(d2) <= b  <=>  d2 + 1 < 2^e * (1 + m/4) of bin b + 1.
-__device__ __forceinline__ unsigned long long cnt_upper(int b) {
-    const float edge = __uint_as_float((uint32_t)(b + 1 + 508) << 21);
-    return (unsigned long long)ceilf(edge) - 2ull;
-}
-
-struct CountFn {
-    float qx, qy, qz;
-    uint32_t* h;               // this lane's bins, CNT_THREADS words apart
-    unsigned long long lim;    // candidates beyond this squared distance cannot matter
-    __device__ __forceinline__ unsigned long long limit() const { return lim; }
-    __device__ __forceinline__ void operator()(const float4 p) {
-        const int b = cnt_bin(cnt_d2p1(p.x - qx, p.y - qy, p.z - qz));
-        atomicAdd(&h[(b >> 2) * CNT_THREADS], 1u << ((b & 3) << 3));
-    }
-};
-
-// First bin where the running count reaches K (-1: fewer than K counted), the
-// count below it and the count in it.
-__device__ __forceinline__ int cnt_find(const uint32_t* h, int K, int& below, int& inbin) {
-    int cum = 0;
-    for (int w = 0; w < CNT_WORDS; ++w) {
-        const uint32_t v = h[w * CNT_THREADS];
-        const int s = (int)__dp4a(v, 0x01010101u, 0u);
-        if (cum + s < K) {
-            cum += s;
-            continue;
-        }
-        for (int t = 0; t < 4; ++t) {
-            const int c = (int)((v >> (8 * t)) & 0xFFu);
-            if (cum + c >= K) {
-                below = cum;
-                inbin = c;
-                return 4 * w + t;
-            }
-            cum += c;
-        }
-    }
-    below = cum;
-    inbin = 0;
-    return -1;
-}
-
-// The point ranges of ring R (<= 1) that can hold a point within squared
-// distance lim: scan_shell's columns and z-reach, listed instead of walked.
-__device__ __forceinline__ int cnt_ring_ranges(const GridView& gv, const GridParams& g,
-                                               const QueryCell& qc, int R, unsigned long long lim,
-                                               uint2* rg) {
-    int nr = 0;
-    const int zlo = qc.cz - R, zhi = qc.cz + R;
-    const int c = g.cell;
-    for (int dy = -R; dy <= R; ++dy) {
-        const int y = qc.cy + dy;
-        if (y < 0 || y >= g.gy) continue;
-        const int ady = dy < 0 ? -dy : dy;
-        const int gy_ = slab_gap(qc.qy, y, c);
-        for (int dx = -R; dx <= R; ++dx) {
-            const int x = qc.cx + dx;
-            if (x < 0 || x >= g.gx) continue;
-            const int gx_ = slab_gap(qc.qx, x, c);
-            const long long h2 = (long long)gx_ * gx_ + (long long)gy_ * gy_;
-            if ((unsigned long long)h2 > lim) continue;
-            const int4 ci = __ldg(&gv.colinfo[(uint32_t)y * (uint32_t)g.gx + (uint32_t)x]);
-            if (ci.z < ci.y) continue;
-            int zr0 = zlo, zr1 = zhi;
-            if (lim < (1ull << 46)) {
-                const float s = sqrtf((float)(lim - (unsigned long long)h2)) + 1.0f;
-                zr0 = max(zr0, (int)floorf(((float)qc.qz - s) / (float)c));
-                zr1 = min(zr1, (int)floorf(((float)qc.qz + s) / (float)c));
-            }
-            auto add = [&](int zl, int zh) {
-                zl = max(zl, ci.y);
-                zh = min(zh, ci.z);
-                if (zl > zh) return;
-                const uint32_t e0 = (uint32_t)ci.x + (uint32_t)(zl - ci.y);
-                const uint32_t e1 = (uint32_t)ci.x + (uint32_t)(zh - ci.y) + 1;
-                const uint32_t ps = __ldg(&gv.cstart[e0]), pe = __ldg(&gv.cstart[e1]);
-                if (ps < pe) {
-                    rg[nr * CNT_THREADS] = make_uint2(ps, pe);
-                    ++nr;
-                }
-            };
-            const int adx = dx < 0 ? -dx : dx;
-            if (max(ady, adx) == R) {
-                add(zr0, zr1);
-            } else {
-                if (zlo >= zr0 && zlo <= zr1) add(zlo, zlo);
-                if (zhi >= zr0 && zhi <= zr1) add(zhi, zhi);
-            }
-        }
-    }
-    return nr;
-}
-
-// One loop over the lane's listed ranges, back to back.
-template <class F>
-__device__ __forceinline__ void cnt_walk(const GridView& gv, const uint2* rg, int nr, F& f) {
-    int k = 0;
-    uint32_t j = 0, e = 0;
-    for (;;) {
-        if (j >= e) {
-            if (k >= nr) break;
-            const uint2 r = rg[k * CNT_THREADS];
-            ++k;
-            j = r.x;
-            e = r.y;
-        }
-        f(__ldg(&gv.sorted[j]));
-        ++j;
-    }
-}
-
-template <class F>
-__device__ __forceinline__ void cnt_ring(const GridView& gv, const GridParams& g, const QueryCell& qc,
-                                         int R, uint2* rg, F& f) {
-    if (R <= 1) {
-        const int nr = cnt_ring_ranges(gv, g, qc, R, f.limit(), rg);
-        cnt_walk(gv, rg, nr, f);
-    } else {
-        scan_shell(gv, g, qc, R, f);
-    }
-}
-
-struct CountSumFn {
-    float qx, qy, qz;
-    int bk;
-    unsigned long long lim;
-    unsigned long long* e;     // this lane's bin-bK entries, CNT_THREADS apart
-    int nb;
-    int s1x, s1y, s1z, sxx, syx, syy, szx, szy, szz, cnt;
-    __device__ __forceinline__ unsigned long long limit() const { return lim; }
-    __device__ __forceinline__ void operator()(const float4 p) {
-        const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
-        const float v = cnt_d2p1(dx, dy, dz);
-        const int b = cnt_bin(v);
-        if (b > bk) return;
-        const int ix = small_int(dx), iy = small_int(dy), iz = small_int(dz);
-        if (b < bk) {
-            s1x += ix;
-            s1y += iy;
-            s1z += iz;
-            sxx += ix * ix;
-            syx += iy * ix;
-            syy += iy * iy;
-            szx += iz * ix;
-            szy += iz * iy;
-            szz += iz * iz;
-            ++cnt;
-            return;
-        }
-        // bin bK (< 92: d2 <= 2^23 - 2, so |offsets| < 2^12 fit 13 bits)
-        if (nb < CNT_BUF) {
-            const uint32_t d2 = __float2uint_rn(v) - 1u;
-            e[nb * CNT_THREADS] = ((unsigned long long)d2 << 39) |
-                                  ((unsigned long long)((uint32_t)ix & 0x1FFFu) << 26) |
-                                  ((unsigned long long)((uint32_t)iy & 0x1FFFu) << 13) |
-                                  (unsigned long long)((uint32_t)iz & 0x1FFFu);
-        }
-        ++nb;
-    }
-};
-
-template <int KS>
-__device__ __forceinline__ void select_row_count(const QueryArgs& a, const uint64_t i,
-                                                 uint32_t* hist, uint2* rg, unsigned long long* ent) {
-    const GridParams g = *a.gp;
-    const float4 q = __ldg(&a.gv.sorted[i]);
-    const uint32_t id = __float_as_uint(q.w);
-    const int K = row_neighbours(a.row_k, a.K, a.n, id);
-    auto retry = [&]() {
-        const uint32_t slot = atomicAdd(&a.counters[6], 1u);
-        a.retry_rows[slot] = (uint32_t)i;
-    };
-    if (K <= 0) {
-        retry();
-        return;
-    }
-    QueryCell qc;
-    qc.qx = __float2int_rz(q.x);
-    qc.qy = __float2int_rz(q.y);
-    qc.qz = __float2int_rz(q.z);
-    qc.cx = qc.qx / g.cell;
-    qc.cy = qc.qy / g.cell;
-    qc.cz = qc.qz / g.cell;
-    for (int w = 0; w < CNT_WORDS; ++w) hist[w * CNT_THREADS] = 0u;
-    CountFn f{q.x, q.y, q.z, hist, ~0ull};
-    int R, bk = -1, below = 0, inbin = 0;
-    bool complete = false;
-    const int rmax = a.rmax;
-    for (R = 0; R <= rmax; ++R) {
-        cnt_ring(a.gv, g, qc, R, rg, f);
-        bk = cnt_find(hist, K, below, inbin);
-        const unsigned long long gap2 = outside_gap2(g, qc, R);
-        if (gap2 == ~0ull) {
-            complete = bk >= 0;
-            break;
-        }
-        if (bk >= 0 && bk < CNT_BINS - 1) {
-            const unsigned long long u = cnt_upper(bk);
-            if (u < gap2) {
-                complete = true;
-                break;
-            }
-            f.lim = u;
-        }
-    }
-    RowSums out;
-    out.cnt = 0;
-    if (R > rmax) R = rmax;
-    if (!complete || bk >= CNT_BINS - 1) {
-        atomicAdd(&a.counters[2], 1u);
-        defer_row(a, id, false, 0u, R);
-        a.sums[i] = out;
-        return;
-    }
-    CountSumFn f2;
-    f2.qx = q.x;
-    f2.qy = q.y;
-    f2.qz = q.z;
-    f2.bk = bk;
-    f2.lim = cnt_upper(bk);
-    f2.e = ent;
-    f2.nb = 0;
-    f2.s1x = f2.s1y = f2.s1z = f2.sxx = f2.syx = f2.syy = f2.szx = f2.szy = f2.szz = f2.cnt = 0;
-    for (int r = 0; r <= R; ++r) cnt_ring(a.gv, g, qc, r, rg, f2);
-    const int nb = f2.nb;
-    if (nb > CNT_BUF || nb != inbin || f2.cnt != below) {
-        retry();
-        return;
-    }
-    for (int s = 1; s < nb; ++s) {  // ascending (squared distance, offsets)
-        const unsigned long long v = ent[s * CNT_THREADS];
-        int t = s - 1;
-        while (t >= 0 && ent[t * CNT_THREADS] > v) {
-            ent[(t + 1) * CNT_THREADS] = ent[t * CNT_THREADS];
-            --t;
-        }
-        ent[(t + 1) * CNT_THREADS] = v;
-    }
-    const int need = K - below;  // 1 <= need <= nb
-    const uint32_t kk = (uint32_t)(ent[(need - 1) * CNT_THREADS] >> 39);
-    if (nb > need && (uint32_t)(ent[need * CNT_THREADS] >> 39) == kk) {
-        atomicAdd(&a.counters[1], 1u);
-        defer_row(a, id, true, KEY_BASE + kk, R);
-        a.sums[i] = out;
-        return;
-    }
-    for (int s = 0; s < need; ++s) {
-        const unsigned long long v = ent[s * CNT_THREADS];
-        const int ix = (int)((uint32_t)(v >> 26) << 19) >> 19;
-        const int iy = (int)((uint32_t)(v >> 13) << 19) >> 19;
-        const int iz = (int)((uint32_t)v << 19) >> 19;
-        f2.s1x += ix;
-        f2.s1y += iy;
-        f2.s1z += iz;
-        f2.sxx += ix * ix;
-        f2.syx += iy * ix;
-        f2.syy += iy * iy;
-        f2.szx += iz * ix;
-        f2.szy += iz * iy;
-        f2.szz += iz * iz;
-    }
-    out.s[0] = f2.s1x;
-    out.s[1] = f2.s1y;
-    out.s[2] = f2.s1z;
-    out.s[3] = f2.sxx;
-    out.s[4] = f2.syx;
-    out.s[5] = f2.syy;
-    out.s[6] = f2.szx;
-    out.s[7] = f2.szy;
-    out.s[8] = f2.szz;
-    out.cnt = K;
-    a.sums[i] = out;
-}
-
-template <int KS>
-__global__ void __launch_bounds__(CNT_THREADS) knn_select_count_kernel(const QueryArgs a) {
-    __shared__ uint32_t hist[CNT_WORDS * CNT_THREADS];
-    __shared__ uint2 rg[CNT_RANGES * CNT_THREADS];
-    __shared__ unsigned long long ent[CNT_BUF * CNT_THREADS];
-    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= (a.rows ? a.nq : a.n)) return;
-    if (a.rows) i = __ldg(&a.rows[i]);
-    select_row_count<KS>(a, i, hist + threadIdx.x, rg + threadIdx.x, ent + threadIdx.x);
-}
-
 // Split form, finish: covariance, eigensolve and stage projections of the
 // rows the select kernel completed.  Uniform work per thread.
 __device__ __forceinline__ void finish_row(const QueryArgs& a, const uint64_t i) {
@@ -1602,21 +1269,6 @@ struct KnnLauncher {
             if (cudaMemsetAsync(la.q.counters + 6, 0, sizeof(uint32_t), la.stream))
                 return NBG_ERR_CUDA;
             knn_select_loc_kernel<KS><<<(unsigned)blocks, threads, 0, la.stream>>>(la.q, la.ob);
-            QueryArgs r = la.q;
-            r.rows = la.q.retry_rows;
-            r.nq_dev = la.q.counters + 6;
-            knn_retry_kernel<KS><<<(unsigned)std::min<uint64_t>(blocks, (uint64_t)la.sms * 4), threads,
-                                   0, la.stream>>>(r);
-            knn_finish_kernel<<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
-            NBG_LAUNCHED(3);
-            return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
-        }
-        if (la.group == 3 && la.q.sums && !la.ids) {
-            // counting select; rows it hands back through the two-pass kernel
-            // (count read on the device); then the finish pass
-            if (cudaMemsetAsync(la.q.counters + 6, 0, sizeof(uint32_t), la.stream))
-                return NBG_ERR_CUDA;
-            knn_select_count_kernel<KS><<<(unsigned)blocks, CNT_THREADS, 0, la.stream>>>(la.q);
             QueryArgs r = la.q;
             r.rows = la.q.retry_rows;
             r.nq_dev = la.q.counters + 6;

@@ -333,8 +333,8 @@ class Tile:
     def set_select(self, kernel=0, first_margin=0.5):
         """Select kernel (nbg_tile_set_select): 0 two-pass ring search
         (default), 1 the same in block-local Morton order, 2 single-pass ring
-        search, 3 counting select (shared-memory distance histograms), 8 / 16
-        / 32 queries sharing one candidate list; results are identical."""
+        search, 8 / 16 / 32 queries sharing one candidate list; results are
+        identical."""
         self.ctx._check(self.ctx.lib.nbg_tile_set_select(self.ctx.h, self.h, int(kernel),
                                                          float(first_margin)))
 

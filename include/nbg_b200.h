@@ -242,9 +242,6 @@ int nbg_tile_tune(nbg_context* ctx, nbg_tile* tile, float cell_factor, int32_t f
  *   1  the same with the queries of each 256-row block in Morton order
  *   2  single-pass ring search: top-list keys carry the candidate's column and
  *      position, so the K nearest are read back without a second scan
- *   3  counting select: per-lane histograms of log-spaced squared-distance
- *      bins in shared memory instead of a register top list; a second scan
- *      sums the bins below the K-th and sorts the K-th's bin
  *   8, 16, 32  that many neighbouring queries (Morton-compact) share one
  *      candidate list, gathered box ring by box ring from a first margin of
  *      first_margin cell edges
@@ -257,7 +254,7 @@ int nbg_tile_set_select(nbg_context* ctx, nbg_tile* tile, int32_t select_kernel,
  * blocks taken as runs of 32 consecutive 128-row blocks spread over the tile,
  * and keeps the factor with the least estimated grid + query time (rows the
  * ring search would defer charged at 5 us each).  For each factor it also
- * times the select kernels of nbg_tile_set_select (0, 1, 2, 3 and 32)
+ * times the select kernels of nbg_tile_set_select (0, 1, 2 and 32)
  * on the same sample rows, select + finish, and keeps the fastest pair.  The
  * choice is cached per (log2 points, neighbour slots) class of the context;
  * with use_cache a cached class is applied without measuring. */
@@ -270,7 +267,7 @@ int nbg_tile_autotune(nbg_context* ctx, nbg_tile* tile, int32_t knn, const float
  * and the number the cache holds to *count; nbg_autotune_cache_set adds or
  * replaces entries (NBG_ERR_INVALID for a class outside [0, 63] x [1, 128],
  * a factor that is not finite and positive, or a select kernel other than
- * 0, 1, 2, 3, 8, 16, 32; nothing is set then). */
+ * 0, 1, 2, 8, 16, 32; nothing is set then). */
 typedef struct nbg_tune_entry {
     int32_t size_class;    /* floor(log2(points))                            */
     int32_t slots;         /* neighbour slots of the select kernel           */

@@ -17,7 +17,7 @@ from tests import _util as U
 
 pytestmark = pytest.mark.gpu
 
-GROUPS = (0, 1, 2, 3, 8, 16, 32)
+GROUPS = (0, 1, 2, 8, 16, 32)
 
 
 def _clouds():

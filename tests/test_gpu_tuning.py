@@ -19,7 +19,7 @@ def test_tuning_file_round_trip(nbg, tmp_path):
     # 1M points: class floor(log2 n) = 19
     assert any(e["size_class"] == 19 and e["cell_factor"] == chosen for e in cache)
     # the select kernel is chosen with the cell factor
-    assert all(e["select_kernel"] in (0, 1, 2, 3, 32) for e in cache)
+    assert all(e["select_kernel"] in (0, 1, 2, 32) for e in cache)
     path = tmp_path / "tuning.json"
     nbg.save_tuning(path)
     fresh = Context(0)
