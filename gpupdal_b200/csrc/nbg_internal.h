@@ -120,11 +120,16 @@ struct Tile {
     bool fixed_storage = false;  // storage provided by the caller: never grow
     float cell_factor = 4.0f;
     int32_t fixed_cell = 0;
-    // select kernel: 0 the per-thread ring search (default, fastest measured),
-    // 1 the same in block-local Morton order, 8 / 16 / 32 queries sharing one
-    // candidate list; the group select's first box margin in cell edges
+    // select kernel: 0 the two-pass per-thread ring search (default), 1 the
+    // same in block-local Morton order, 2 the single-pass ring search, 8 / 16
+    // / 32 queries sharing one candidate list; the group select's first box
+    // margin in cell edges
     int group = 0;
     float margin0 = 0.5f;
+    // the caller chose the cell factor or select kernel (nbg_tile_tune,
+    // nbg_tile_set_select, nbg_tile_autotune): the context's cached tuning of
+    // the tile's class is then not applied by nbg_run
+    bool tuning_set = false;
     int grid_k1 = 0;
     int32_t grid_fixed = 0;      // fixed cell edge the current grid was built with (0: density)
     bool grid_valid = false;
@@ -242,6 +247,10 @@ int kd_export(Context* ctx, Tile* t, uint32_t* vind, uint32_t* nnodes, int32_t* 
 int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
                          uint32_t* exact_rows, uint32_t* counters, uint2* ties, uint32_t tie_cap,
                          cudaStream_t stream, uint32_t* retry_rows = nullptr);
+
+// A tile the caller did not tune (cell factor, select kernel) takes the
+// context's cached autotuner choice for its (size, neighbour slots) class.
+void apply_cached_tuning(Context* ctx, Tile* t, int K);
 
 // Autotuner (nbg_tile_autotune without the context lock).
 int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, int32_t n_candidates,

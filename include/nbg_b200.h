@@ -250,14 +250,17 @@ int nbg_tile_tune(nbg_context* ctx, nbg_tile* tile, float cell_factor, int32_t f
 int nbg_tile_set_select(nbg_context* ctx, nbg_tile* tile, int32_t select_kernel,
                         float first_margin);
 /* Autotuner: builds the tile's grid with each candidate cell factor (null:
- * 1, 1.5, 2, 3, 4, 6), times the select pass on a sample of four waves of
- * blocks taken as runs of 32 consecutive 128-row blocks spread over the tile,
- * and keeps the factor with the least estimated grid + query time (rows the
- * ring search would defer charged at 5 us each).  For each factor it also
+ * 1, 1.5, 2, 3, 4, 6), times the select pass (best of two launches) on one
+ * contiguous window of the tile's rows in grid order (the whole tile up to 4M
+ * rows), and keeps the factor with the least estimated grid + query time
+ * (rows the ring search would defer charged at 5 us each).  For each factor it also
  * times the select kernels of nbg_tile_set_select (0, 1, 2 and 32)
  * on the same sample rows, select + finish, and keeps the fastest pair.  The
  * choice is cached per (log2 points, neighbour slots) class of the context;
- * with use_cache a cached class is applied without measuring. */
+ * with use_cache a cached class is applied without measuring.  nbg_run applies
+ * the cached choice of a tile's class to every tile whose cell factor and
+ * select kernel the caller left alone (no nbg_tile_tune, nbg_tile_set_select
+ * or nbg_tile_autotune on it), so a loaded tuning file reaches fresh tiles. */
 int nbg_tile_autotune(nbg_context* ctx, nbg_tile* tile, int32_t knn, const float* candidates,
                       int32_t n_candidates, int32_t use_cache, float* chosen, void* stream);
 

@@ -41,3 +41,35 @@ def test_tuning_file_round_trip(nbg, tmp_path):
         assert fresh.tuning_cache() == cache
     finally:
         fresh.close()
+
+
+def test_cached_tuning_reaches_untuned_tiles():
+    """nbg_run applies the context's cached choice of a tile's class (here
+    loaded, as from a tuning file) to tiles the caller did not tune, and leaves
+    a tile whose select kernel the caller set alone; results are the same."""
+    from gpupdal_b200 import abi
+    import numpy as np
+
+    x, y, z = syn.mixture(1_000_000, 7)
+    st = [abi.make_opts(abi.STAGE_NORMAL, knn=16)]
+    ctx = Context(0)
+    try:
+        # 1M points: class 19; knn 16 -> 17 neighbours -> 18 select slots.
+        # Kernel 2 (single pass) hands some rows to the two-pass search,
+        # kernel 0 never does: the retry count shows which one ran.
+        ctx.set_tuning_cache([{"size_class": 19, "slots": 18, "cell_factor": 3.0,
+                               "select_kernel": 2}])
+        untuned = ctx.tile(x, y, z)
+        out_a, ex_a, st_a = ctx.run(untuned, st)
+        untuned.free()
+        assert st_a.retry_rows > 0
+        chosen = ctx.tile(x, y, z)
+        chosen.set_select(0)
+        out_b, ex_b, st_b = ctx.run(chosen, st)
+        chosen.free()
+        assert st_b.retry_rows == 0
+        assert np.array_equal(out_a[0], out_b[0], equal_nan=True)
+        assert np.array_equal(np.sort(ex_a, order=["point_id", "stage"]),
+                              np.sort(ex_b, order=["point_id", "stage"]))
+    finally:
+        ctx.close()
