@@ -422,31 +422,64 @@ __global__ void __launch_bounds__(KD_THREADS) kd_classify_kernel(const KdSeg* se
     }
 }
 
+// The misplaced pairs of a tile: every load of the thread's pairs is issued
+// before any store (each position belongs to exactly one pair of the level, so
+// the loads never read what a store of this launch writes), which keeps the
+// dependent position -> coordinate loads of all the thread's items in flight
+// together instead of one item at a time.
 template <int PASS>
-__global__ void __launch_bounds__(KD_THREADS) kd_swap_kernel(const KdSeg* segs, const uint32_t* tile_first,
-                                                             const uint32_t* tile_seg, const KdSplit* sp,
-                                                             const uint32_t* mlpos,
-                                                             const uint32_t* mrpos, int32_t* rx,
-                                                             int32_t* ry, int32_t* rz, uint32_t* rid) {
+__global__ void __launch_bounds__(KD_THREADS) kd_swap_kernel(const KdSeg* __restrict__ segs,
+                                                             const uint32_t* __restrict__ tile_first,
+                                                             const uint32_t* __restrict__ tile_seg,
+                                                             const KdSplit* __restrict__ sp,
+                                                             const uint32_t* __restrict__ mlpos,
+                                                             const uint32_t* __restrict__ mrpos,
+                                                             int32_t* __restrict__ rx,
+                                                             int32_t* __restrict__ ry,
+                                                             int32_t* __restrict__ rz,
+                                                             uint32_t* __restrict__ rid) {
     const uint32_t t = blockIdx.x;
     const uint32_t s = tile_seg[t];
     const KdSeg sg = segs[s];
     const uint32_t m = PASS == 1 ? sp[s].m : sp[s].m2;
+    const uint32_t l0 = (t - tile_first[s]) * KD_TILE + threadIdx.x;
+    if (l0 >= m) return;
+    uint32_t a[KD_ITEMS], b[KD_ITEMS];
+    int32_t ax[KD_ITEMS], ay[KD_ITEMS], az[KD_ITEMS], bx[KD_ITEMS], by[KD_ITEMS], bz[KD_ITEMS];
+    uint32_t ai[KD_ITEMS], bi[KD_ITEMS];
 #pragma unroll
     for (int k = 0; k < KD_ITEMS; ++k) {
-        const uint32_t li = (t - tile_first[s]) * KD_TILE + threadIdx.x + k * KD_THREADS;
-        if (li >= m) return;
-        const uint32_t a = mlpos[sg.begin + li], b = mrpos[sg.begin + li];
-        const int32_t tx = rx[a], ty = ry[a], tz = rz[a];
-        const uint32_t ti = rid[a];
-        rx[a] = rx[b];
-        ry[a] = ry[b];
-        rz[a] = rz[b];
-        rid[a] = rid[b];
-        rx[b] = tx;
-        ry[b] = ty;
-        rz[b] = tz;
-        rid[b] = ti;
+        const uint32_t li = l0 + k * KD_THREADS;
+        if (li < m) {
+            a[k] = mlpos[sg.begin + li];
+            b[k] = mrpos[sg.begin + li];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < KD_ITEMS; ++k) {
+        if (l0 + k * KD_THREADS < m) {
+            ax[k] = rx[a[k]];
+            ay[k] = ry[a[k]];
+            az[k] = rz[a[k]];
+            ai[k] = rid[a[k]];
+            bx[k] = rx[b[k]];
+            by[k] = ry[b[k]];
+            bz[k] = rz[b[k]];
+            bi[k] = rid[b[k]];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < KD_ITEMS; ++k) {
+        if (l0 + k * KD_THREADS < m) {
+            rx[a[k]] = bx[k];
+            ry[a[k]] = by[k];
+            rz[a[k]] = bz[k];
+            rid[a[k]] = bi[k];
+            rx[b[k]] = ax[k];
+            ry[b[k]] = ay[k];
+            rz[b[k]] = az[k];
+            rid[b[k]] = ai[k];
+        }
     }
 }
 

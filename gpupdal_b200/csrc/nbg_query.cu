@@ -1255,6 +1255,12 @@ struct LaunchArgs {
 int launch_group_select(const QueryArgs& q, int slots, int group, float margin0,
                         cudaStream_t stream);
 
+// Handed-back rows are the sparse-region and hard rows: long ring searches
+// that need many resident warps to hide their latency.  The row count is read
+// on the device, so the grid is sized for the largest expected share (a few
+// per cent of the tile) at one row per thread; blocks past it exit at once.
+static constexpr uint64_t kRetryBlocksPerSm = 16;
+
 template <int KS>
 struct KnnLauncher {
     using Args = LaunchArgs;
@@ -1272,7 +1278,7 @@ struct KnnLauncher {
             QueryArgs r = la.q;
             r.rows = la.q.retry_rows;
             r.nq_dev = la.q.counters + 6;
-            knn_retry_kernel<KS><<<(unsigned)std::min<uint64_t>(blocks, (uint64_t)la.sms * 4), threads,
+            knn_retry_kernel<KS><<<(unsigned)std::min<uint64_t>(blocks, (uint64_t)la.sms * kRetryBlocksPerSm), threads,
                                    0, la.stream>>>(r);
             knn_finish_kernel<<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
             NBG_LAUNCHED(3);
@@ -1295,7 +1301,7 @@ struct KnnLauncher {
             QueryArgs r = la.q;
             r.rows = la.q.retry_rows;
             r.nq_dev = la.q.counters + 6;
-            knn_retry_kernel<KS><<<(unsigned)std::min<uint64_t>(blocks, (uint64_t)la.sms * 4), threads,
+            knn_retry_kernel<KS><<<(unsigned)std::min<uint64_t>(blocks, (uint64_t)la.sms * kRetryBlocksPerSm), threads,
                                    0, la.stream>>>(r);
             NBG_LAUNCHED(1);
             if (!la.ids) {
