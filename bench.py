@@ -38,9 +38,19 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mpts/s k=16 normals+eigen, served vs plain @<=1e-5 rel err; p50/p99 latency"
 BYTES_PER_POINT = 20 + 8 * 7 + 1  # sorted xyz+id, id permutation, 7 f64 outputs, status
-# DRAM bytes per point of knn_select_kernel + knn_finish_kernel (read + write) from one
-# ncu capture of the same workload at 4M points: (182.3 + 628.9) MB / 4e6
-TRAFFIC_PER_POINT = 202.8
+# Per select kernel (the one the autotuner chose for the timed tile): the query
+# kernels, their DRAM bytes per point (read + write) and the select kernel's
+# active lanes per warp instruction and issue-slot fraction, from one ncu
+# capture per kernel of the same workload at 4M points (64-byte device
+# records), summarised under profiles/.
+QUERY_PROFILES = {
+    0: {"kernel": "knn_select_kernel+knn_finish_kernel",
+        # (182.3 + 628.9) MB / 4e6
+        "traffic": 202.8, "lanes": 8.91, "issue": 0.793, "dram_pct": 0.54},
+    2: {"kernel": "knn_select_loc_kernel+knn_retry_kernel+knn_finish_kernel",
+        # select (70.3 + 101.1) + retry (10.3 + 0.0) + finish (364.6 + 261.4) MB / 4e6
+        "traffic": 201.9, "lanes": 10.13, "issue": 0.662, "dram_pct": 0.58},
+}
 
 
 def parse():
@@ -51,6 +61,12 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--points", type=int, default=32_000_000)
     ap.add_argument("--knn", type=int, default=16)
+    ap.add_argument("--select", type=int, default=None,
+                    help="select kernel for the main line's tiles instead of the autotuner's "
+                         "choice (nbg_tile_set_select: 0, 1, 2, 8, 16, 32)")
+    ap.add_argument("--cell-factor", type=float, default=None,
+                    help="cell factor for the main line's tiles instead of the autotuner's "
+                         "choice (nbg_tile_tune)")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true",
@@ -649,14 +665,23 @@ def main():
     hcols = record_columns(hrec.data_ptr(), sts, 56, 2)
     hxn, hyn, hzn = hx.numpy(), hy.numpy(), hz.numpy()
 
+    fixed = args.select is not None or args.cell_factor is not None
+
+    def configure(tile):
+        if args.cell_factor is not None:
+            tile.tune(args.cell_factor)
+        if args.select is not None:
+            tile.set_select(args.select)
+        return tile
+
     def step_device():
-        tile = ctx.tile(dx, dy, dz)
+        tile = configure(ctx.tile(dx, dy, dz))
         ex, st = ctx.run_columns(tile, sts, dcols)
         tile.free()
         return st
 
     def step_e2e():
-        tile = ctx.tile(hxn, hyn, hzn)
+        tile = configure(ctx.tile(hxn, hyn, hzn))
         ex, st = ctx.run_columns(tile, sts, hcols)
         tile.free()
         return st
@@ -685,10 +710,14 @@ def main():
     # the context's autotuner measures this tile's size / knn class once (cell
     # factor and select kernel); every fresh tile of the steps below then takes
     # the cached choice in nbg_run, as tiles of a loaded tuning file do
-    tune_tile = ctx.tile(dx, dy, dz)
-    tune_tile.autotune(args.knn)
-    tune_tile.free()
-    tuning = ctx.tuning_cache()
+    if fixed:
+        tuning = [{"cell_factor": args.cell_factor if args.cell_factor is not None else 4.0,
+                   "select_kernel": args.select if args.select is not None else 0}]
+    else:
+        tune_tile = ctx.tile(dx, dy, dz)
+        tune_tile.autotune(args.knn)
+        tune_tile.free()
+        tuning = ctx.tuning_cache()
     for _ in range(max(args.warmup, 3)):
         step_device()
     clocks = ClockSampler(local)
@@ -702,6 +731,8 @@ def main():
     launches = int(sum(s.kernel_launches for s in stats))
     hbm, peak_kind = peaks()
     achieved = n * BYTES_PER_POINT / (query_ms / 1e3) / 1e9
+    sel_kernel = tuning[0]["select_kernel"] if len(tuning) == 1 else 0
+    qp = QUERY_PROFILES.get(sel_kernel, QUERY_PROFILES[0])
     # end to end through the C ABI with host buffers
     for _ in range(2):
         step_e2e()
@@ -722,9 +753,10 @@ def main():
         "config": {"workload": f"stress tile {n} points per GPU (seed 2+rank), filters.eigenvalues "
                                f"knn={args.knn} then filters.normal knn={args.knn}, one grid",
                    "points_per_gpu": n, "knn": args.knn, "form": "plain per-tile launch",
-                   "tuning": {"source": "context autotuner, one measurement of this size/knn "
-                                        "class before the warm-up, applied by nbg_run to each "
-                                        "fresh tile", "entries": tuning},
+                   "tuning": {"source": ("fixed by --select / --cell-factor" if fixed else
+                                         "context autotuner, one measurement of this size/knn "
+                                         "class before the warm-up, applied by nbg_run to each "
+                                         "fresh tile"), "entries": tuning},
                    "l2": "inputs larger than L2 (tile 384 MB + sorted copy 512 MB per step)",
                    "tie_rows": int(last.tie_rows), "deferred_rows": int(last.deferred_rows),
                    "resolved_rows": int(last.resolved_rows), "replay_rows": int(last.replay_rows),
@@ -739,14 +771,17 @@ def main():
                         "later chunks run when output_chunks > 0)"},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": TRAFFIC_PER_POINT * n,
-                     "traffic_source": "ncu dram bytes of select+finish on the 4M-point tile, "
-                                       "scaled per point",
-                     "kernel": "knn_select_kernel+knn_finish_kernel", "peak_source": peak_kind,
+                     "frac": achieved / hbm, "traffic": qp["traffic"] * n,
+                     "traffic_source": "ncu dram bytes of the query kernels on the 4M-point "
+                                       "tile, scaled per point",
+                     "kernel": qp["kernel"], "peak_source": peak_kind,
                      "bytes_per_point": BYTES_PER_POINT,
-                     "limiter": "instruction issue, not HBM: ncu on the 4M-point stress tile shows "
-                                "knn_select_kernel with 79.3 % of issue slots busy and 0.54 % DRAM "
-                                "throughput (8.9 of 32 lanes active per instruction)"},
+                     "issue_efficiency": round(qp["lanes"] / 32 * qp["issue"], 3),
+                     "limiter": (f"instruction issue, not HBM: ncu on the 4M-point stress tile shows "
+                                 f"the select kernel with {100 * qp['issue']:.1f} % of issue slots "
+                                 f"busy, {qp['lanes']:.2f} of 32 lanes active per instruction "
+                                 f"(issue efficiency = lanes/32 x issue fraction) and "
+                                 f"{qp['dram_pct']:.2f} % DRAM throughput")},
         "clocks": clk,
     }
     if cpu is not None:

@@ -1401,11 +1401,12 @@ int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, i
     int rc = ensure_scratch(ctx, n, 1);
     if (rc) return rc;
     // sample: one contiguous window of rows in the grid's order (the whole
-    // tile up to 4M rows), so that neighbouring blocks share cells and the
+    // tile up to 8M rows), so that neighbouring blocks share cells and the
     // caches behave as in a full launch (runs of blocks scattered over the
     // tile misjudged the 32M-point stress tile: they chose a cell factor and
-    // kernel 10 % slower than the default)
-    const uint64_t window = std::min<uint64_t>(n, 4ull << 20);
+    // kernel 10 % slower than the default; a 4M-row window, best of two, did
+    // not always separate kernels 8 % apart)
+    const uint64_t window = std::min<uint64_t>(n, 8ull << 20);
     const uint64_t first_row = (n - window) / 2;
     std::vector<uint32_t> sample(window);
     for (uint64_t r = 0; r < window; ++r) sample[r] = (uint32_t)(first_row + r);
@@ -1458,10 +1459,10 @@ int tile_autotune(Context* ctx, Tile* t, int32_t knn, const float* candidates, i
             ql.retry_rows = ctx->retry_rows;
             ql.group = G;
             ql.margin0 = t->margin0;
-            // best of two launches of the window
+            // best of three launches of the window
             float build_ms = 0, sample_ms = 1e30f;
             uint32_t cnt[3] = {0, 0, 0};
-            for (int rep = 0; rep < 2 && !rc; ++rep) {
+            for (int rep = 0; rep < 3 && !rc; ++rep) {
                 cudaMemsetAsync(cnt_dev, 0, 8 * sizeof(uint32_t), stream);
                 cudaEventRecord(ctx->ev[2], stream);
                 rc = launch_query(ctx, ql, stream);

@@ -250,8 +250,8 @@ int nbg_tile_tune(nbg_context* ctx, nbg_tile* tile, float cell_factor, int32_t f
 int nbg_tile_set_select(nbg_context* ctx, nbg_tile* tile, int32_t select_kernel,
                         float first_margin);
 /* Autotuner: builds the tile's grid with each candidate cell factor (null:
- * 1, 1.5, 2, 3, 4, 6), times the select pass (best of two launches) on one
- * contiguous window of the tile's rows in grid order (the whole tile up to 4M
+ * 1, 1.5, 2, 3, 4, 6), times the select pass (best of three launches) on one
+ * contiguous window of the tile's rows in grid order (the whole tile up to 8M
  * rows), and keeps the factor with the least estimated grid + query time
  * (rows the ring search would defer charged at 5 us each).  For each factor it also
  * times the select kernels of nbg_tile_set_select (0, 1, 2 and 32)
