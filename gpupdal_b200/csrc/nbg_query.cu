@@ -785,13 +785,40 @@ __device__ __forceinline__ void tie_row(const TieArgs& a, uint32_t r) {
         }
         d64[t] = acc;
     }
+    // Members at equal FP64 distance are taken in the search's visiting order.
+    // Without a neighbour-id export only their offsets reach the sums: when every
+    // member at the m-th smallest FP64 distance has the same offsets (duplicate
+    // points, most of a lidar tile's tie groups), any of them gives the same
+    // sums, and the row needs no walk down the tree.  (The test is per row: a
+    // member skipped as "equivalent" in a pairwise walk would stand in for its
+    // twin in later comparisons with the other members and break the order.)
+    bool any_order = f.row == nullptr;
+    if (any_order) {
+        double v = 0.0;  // the m-th smallest FP64 distance
+        for (int t = 0; t < f.gcnt; ++t) {
+            int less = 0, le = 0;
+            for (int u = 0; u < f.gcnt; ++u) {
+                less += d64[u] < d64[t];
+                le += d64[u] <= d64[t];
+            }
+            if (less < m && m <= le) v = d64[t];
+        }
+        int ref = -1;
+        for (int t = 0; t < f.gcnt && any_order; ++t) {
+            if (d64[t] != v) continue;
+            if (ref < 0) ref = t;
+            else if (f.gd[t][0] != f.gd[ref][0] || f.gd[t][1] != f.gd[ref][1] ||
+                     f.gd[t][2] != f.gd[ref][2])
+                any_order = false;
+        }
+    }
     uint32_t taken = 0;
     for (int j = 0; j < m; ++j) {
         int best = -1;
         for (int t = 0; t < f.gcnt; ++t) {
             if ((taken >> t) & 1u) continue;
             if (best < 0 || d64[t] < d64[best] ||
-                (d64[t] == d64[best] &&
+                (d64[t] == d64[best] && !any_order &&
                  kd_meets_first(a.kd, q64, __ldg(&a.kd.kpos[a.kd.base + f.gid[t]]),
                                 __ldg(&a.kd.kpos[a.kd.base + f.gid[best]]))))
                 best = t;
