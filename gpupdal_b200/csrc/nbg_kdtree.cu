@@ -606,20 +606,25 @@ __global__ void kd_leaf_bbox_kernel(const uint32_t* leaves, uint32_t nleaves, co
 // One Hoare pass of nanoflann's planeSplit over [b, e) by one warp: with L
 // the count satisfying the predicate, the t-th element from the left failing
 // it inside [b, b+L) swaps with the t-th element from the right satisfying it
-// inside [b+L, e).  Returns L.  mlpos/mrpos[b ...] are the warp's scratch.
+// inside [b+L, e).  Returns L; *eq (pass 1) counts the elements equal to the
+// cut value, the only ones pass 2 can move.  mlpos/mrpos[b ...] are the
+// warp's scratch.
 template <int PASS>
 __device__ uint32_t kd_warp_pass(int32_t* rx, int32_t* ry, int32_t* rz, uint32_t* rid,
                                  uint32_t* mlpos, uint32_t* mrpos, uint32_t b, uint32_t e, int f,
-                                 double cut, const Transform& tf, int lane) {
+                                 double cut, const Transform& tf, int lane, uint32_t* eq = nullptr) {
     const int32_t* rc = f == 0 ? rx : (f == 1 ? ry : rz);
     const double sc = tf.scale[f], of = tf.offset[f];
     const unsigned lt = (1u << lane) - 1u;
-    uint32_t L = 0;
+    uint32_t L = 0, neq = 0;
     for (uint32_t base = b; base < e; base += 32) {
         const uint32_t i = base + lane;
-        const bool p = i < e && kd_pred<PASS>(ref_coord(rc[i], sc, of), cut);
+        const double v = i < e ? ref_coord(rc[i], sc, of) : 0.0;
+        const bool p = i < e && kd_pred<PASS>(v, cut);
         L += __popc(__ballot_sync(0xffffffffu, p));
+        if (PASS == 1) neq += __popc(__ballot_sync(0xffffffffu, i < e && v == cut));
     }
+    if (eq) *eq = neq;
     uint32_t m = 0;
     for (uint32_t base = b; base < b + L; base += 32) {
         const uint32_t i = base + lane;
@@ -691,8 +696,13 @@ __global__ void __launch_bounds__(32 * KD_WARPS) kd_warp_build_kernel(
         int f;
         double cut;
         kd_choose_cut(sg.lo, sg.hi, mn, mx, tf, f, cut);
-        const uint32_t L = kd_warp_pass<1>(rx, ry, rz, rid, mlpos, mrpos, b, e, f, cut, tf, lane);
-        const uint32_t L2 = kd_warp_pass<2>(rx, ry, rz, rid, mlpos, mrpos, b + L, e, f, cut, tf, lane);
+        uint32_t eq = 0;
+        const uint32_t L = kd_warp_pass<1>(rx, ry, rz, rid, mlpos, mrpos, b, e, f, cut, tf, lane, &eq);
+        // pass 2 (<= cut on [b+L, e), which pass 1 left holding the elements
+        // >= cut) moves only elements equal to the cut value: with none, its
+        // count is 0 and it swaps nothing
+        const uint32_t L2 =
+            eq ? kd_warp_pass<2>(rx, ry, rz, rid, mlpos, mrpos, b + L, e, f, cut, tf, lane) : 0u;
         const uint32_t lim1 = L, lim2 = L + L2;
         uint32_t index;
         if (lim1 > count / 2) index = lim1;
