@@ -174,13 +174,14 @@ def cpu_model():
     return None
 
 
-def cpu_reference(x, y, z, knn, sample, kind=None, single_thread=False):
+def cpu_reference(x, y, z, knn, sample, kind=None, single_thread=False, reps=1):
     """Times the reference's CPU path (KD build + eigenvalues + normal) on a
     spatially contiguous window of `sample` points: all host threads for the
     rows in fixed contiguous chunks, and the KD build on min(8, cores)
-    threads.  With `single_thread`, also one thread for both (the stage's
-    own semantics: one thread per view) on a window of a quarter of the
-    points."""
+    threads; with reps > 1, after one untimed run, the median of `reps` runs.
+    With `single_thread`, also one thread for both (the stage's own
+    semantics: one thread per view) on a window of a quarter of the points,
+    after one untimed run."""
     from gpupdal_b200 import synthetic as syn
     from oracle import oracle as orc
     if kind is None:
@@ -204,7 +205,11 @@ def cpu_reference(x, y, z, knn, sample, kind=None, single_thread=False):
 
     threads = os.cpu_count() or 1
     side, xyz = window(sample)
-    dt = timed_run(xyz, threads)
+    if reps > 1:
+        timed_run(xyz, threads)
+        dt = statistics.median(timed_run(xyz, threads) for _ in range(reps))
+    else:
+        dt = timed_run(xyz, threads)
     n = len(xyz[0])
     out = {"value": n / dt / 1e6, "unit": "Mpts/s", "cores": threads,
            "kind": kind, "sample": f"{n}-point window ({side / 100:.0f} x "
@@ -214,6 +219,8 @@ def cpu_reference(x, y, z, knn, sample, kind=None, single_thread=False):
            "seconds": dt, "cpu_model": cpu_model(), "nproc": threads}
     if single_thread:
         side1, xyz1 = window(sample // 4)
+        if reps > 1:
+            timed_run(xyz1, 1)
         dt1 = timed_run(xyz1, 1)
         n1 = len(xyz1[0])
         out["single_thread"] = {"value": n1 / dt1 / 1e6, "unit": "Mpts/s", "cores": 1,
@@ -615,7 +622,9 @@ def cpu_only(args):
     nothing else: the main workload's window (all host threads, and one
     thread) and each extra stage's window.  Printed as one JSON object."""
     x, y, z = workload(args.points, 2)
-    out = {"main": cpu_reference(x, y, z, args.knn, args.cpu_sample, single_thread=True)}
+    # warm and repeated as the reference arm's steps are (a single cold run
+    # read 16 % below the arm on the same box)
+    out = {"main": cpu_reference(x, y, z, args.knn, args.cpu_sample, single_thread=True, reps=3)}
     del x, y, z
     if not args.no_extras:
         out["extras"] = extras_cpu()
@@ -805,7 +814,8 @@ def main():
         if cb:
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
                                                        "cpu_model", "nproc", "single_thread")}
-            line["cpu_baseline"]["process"] = "fresh process, before any GPU work"
+            line["cpu_baseline"]["process"] = ("fresh process, before any GPU work; one untimed "
+                                               "run, then the median of three")
         else:
             line["cpu_baseline"] = {"error": cpu.get("error", "no result")}
     # the large legs first, the compact summaries last (the end of the line

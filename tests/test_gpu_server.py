@@ -110,3 +110,37 @@ def test_admission_holds_the_budget():
         assert e.value.code == abi.NBG_ERR_BUDGET
     finally:
         srv.close()
+
+
+def test_pinned_buffers_give_the_same_results(nbg):
+    """The served stream with its host buffers pinned (served.pin_requests:
+    coordinates, OptimalKNN/OptimalRadius and reused output columns in
+    page-locked memory, copied by DMA instead of through the bounce buffers)
+    answers every request exactly as with pageable buffers, served and plain."""
+    from gpupdal_b200 import served
+    reqs = [dict(x=x, y=y, z=z, stages=st, kopt=kopt, ropt=ropt)
+            for (x, y, z, st, kopt, ropt) in _requests()[:6]]
+    preqs, keep = served.pin_requests(reqs)
+    srv = Server(0, slots=4)
+    try:
+        for rs in (reqs, preqs):
+            tickets = [srv.submit(r["x"], r["y"], r["z"], r["stages"], optimal_knn=r["kopt"],
+                                  optimal_radius=r["ropt"], out=r.get("out"))
+                       for r in rs]
+            got = [srv.wait(t) for t in tickets]
+            if rs is reqs:
+                want = [([o.copy() for o in outs], _sorted_ex(ex)) for outs, ex, _ in got]
+                continue
+            for i, (outs, ex, _) in enumerate(got):
+                assert _same(outs, want[i][0]), f"request {i}: pinned outputs differ"
+                assert np.array_equal(_sorted_ex(ex), want[i][1]), f"request {i}: exceptions differ"
+    finally:
+        srv.close()
+    # the plain per-tile call writes the same into the pinned output columns
+    for r, (outs_want, _) in zip(preqs, want):
+        tile = nbg.tile(r["x"], r["y"], r["z"])
+        outs, ex, _ = nbg.run(tile, r["stages"], optimal_knn=r["kopt"], optimal_radius=r["ropt"],
+                              out=r["out"])
+        tile.free()
+        assert _same(outs, outs_want)
+    del preqs, keep
