@@ -196,9 +196,9 @@ __global__ void cell_scatter_kernel(const int32_t* __restrict__ x, const int32_t
     }
 }
 
-static int grid_blocks(uint64_t n, int threads, int sms) {
+static int grid_blocks(uint64_t n, int threads, int sms, int per_sm = 8) {
     uint64_t b = (n + threads - 1) / threads;
-    uint64_t cap = (uint64_t)sms * 8;
+    uint64_t cap = (uint64_t)sms * per_sm;
     if (b > cap) b = cap;
     if (b < 1) b = 1;
     return (int)b;
@@ -218,6 +218,9 @@ int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
     const uint64_t n = t->n;
     const int sms = ctx->sm_count;
     const int nb = grid_blocks(n, 256, sms);
+    // the scatter waits on a returned atomic per point: more resident threads
+    // keep more of those round trips in flight
+    const int sb = grid_blocks(n, 256, sms, 32);
     bbox_init_kernel<<<1, 32, 0, stream>>>(t->bbox);
     bbox_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->bbox);
     grid_config_kernel<<<1, 1, 0, stream>>>(t->bbox, n, k1, t->cell_factor, t->cols_cap,
@@ -251,7 +254,7 @@ int build_grid(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
     if (cudaMemcpyAsync(t->cursor, t->cstart, ((size_t)T + 1) * sizeof(uint32_t),
                         cudaMemcpyDeviceToDevice, stream))
         return NBG_ERR_CUDA;
-    cell_scatter_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->keys, t->cursor,
+    cell_scatter_kernel<<<sb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->keys, t->cursor,
                                                 t->sorted);
     // bbox (2), config, col init, zrange, extent, scan (2), bases, count, scan (2), scatter
     NBG_LAUNCHED(13);
@@ -266,6 +269,9 @@ int build_grid_async(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
     const uint64_t n = t->n;
     const int sms = ctx->sm_count;
     const int nb = grid_blocks(n, 256, sms);
+    // the scatter waits on a returned atomic per point: more resident threads
+    // keep more of those round trips in flight
+    const int sb = grid_blocks(n, 256, sms, 32);
     const uint64_t entries = t->table_cap - 1;  // cstart needs entries + 1 slots
     bbox_init_kernel<<<1, 32, 0, stream>>>(t->bbox);
     bbox_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->bbox);
@@ -291,7 +297,7 @@ int build_grid_async(Context* ctx, Tile* t, int k1, cudaStream_t stream) {
     if (cudaMemcpyAsync(t->cursor, t->cstart, (size_t)(entries + 1) * sizeof(uint32_t),
                         cudaMemcpyDeviceToDevice, stream))
         return NBG_ERR_CUDA;
-    cell_scatter_kernel<<<nb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->keys, t->cursor,
+    cell_scatter_kernel<<<sb, 256, 0, stream>>>(t->x, t->y, t->z, n, t->gp, t->keys, t->cursor,
                                                 t->sorted);
     NBG_LAUNCHED(13);
     t->table_size = entries;
