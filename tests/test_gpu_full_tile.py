@@ -90,3 +90,30 @@ def test_refine_is_output_neutral(nbg, stress):
     b, ex_b, _ = nbg.run(tile, [refined])
     assert np.array_equal(a[0], b[0], equal_nan=True)
     assert np.array_equal(ex_a, ex_b)
+
+
+def test_stress_tile_tuned_configuration_matches_default(nbg, stress):
+    """The bench's timed step runs the autotuner's choice for this tile (cell
+    factor 4, single-pass select kernel 2) rather than the plain call's
+    default (two-pass select).  Both answer each row from the same exact
+    integer neighbourhood sums, so the tuned configuration's outputs and row
+    statuses on the full 32M-point tile equal, bit for bit, the default's,
+    which the test above checks against the FP64 oracle."""
+    x, y, z = stress
+    stages = [abi.make_opts(abi.STAGE_EIGENVALUES, knn=KNN),
+              abi.make_opts(abi.STAGE_NORMAL, knn=KNN, always_up=True)]
+    tile = nbg.tile(x, y, z)
+    tile.set_select(0)  # the default, whatever the shared context has cached
+    want, ex_want, st_want = nbg.run(tile, stages)
+    tile.free()
+    tile = nbg.tile(x, y, z)
+    tile.tune(4.0)
+    tile.set_select(2)
+    got, ex_got, st_got = nbg.run(tile, stages)
+    tile.free()
+    assert st_got.retry_rows > 0  # the single-pass kernel ran (it hands some rows back)
+    assert st_want.retry_rows == 0
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b, equal_nan=True)
+    order = ["point_id", "stage"]
+    assert np.array_equal(np.sort(ex_got, order=order), np.sort(ex_want, order=order))
