@@ -384,10 +384,13 @@ int nbg_create(nbg_context** out, int device, uint64_t hbm_budget_bytes) {
     ctx->events = true;
     int lo_prio = 0, hi_prio = 0;
     cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
-    if (cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, hi_prio) != cudaSuccess) {
+    if (cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, hi_prio) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->fork, cudaStreamNonBlocking, lo_prio) != cudaSuccess) {
+        if (ctx->side) cudaStreamDestroy(ctx->side);
         delete h;
         return NBG_ERR_CUDA;
     }
+    for (int i = 0; i < 3; ++i) cudaEventCreateWithFlags(&ctx->fev[i], cudaEventDisableTiming);
     if (dev_alloc(ctx, (void**)&ctx->counters, 64 * sizeof(uint32_t), nullptr)) {
         delete h;
         return NBG_ERR_OOM;
@@ -413,6 +416,10 @@ int nbg_destroy(nbg_context* h) {
     }
     batch_release(ctx);
     if (ctx->side) cudaStreamDestroy(ctx->side);
+    if (ctx->fork) {
+        cudaStreamDestroy(ctx->fork);
+        for (int i = 0; i < 3; ++i) cudaEventDestroy(ctx->fev[i]);
+    }
     if (ctx->bounce_ready) {
         for (int i = 0; i < 2; ++i) {
             cudaFreeHost(ctx->bounce[i]);
@@ -831,12 +838,14 @@ static int run_pipelined(Context* ctx, Tile* t, int K, const StageGroup& g, cons
         ql.retry_rows = ctx->retry_rows + b[c];
         ql.group = t->group;
         ql.margin0 = t->margin0;
+        // sel[c] marks the chunk's rows answered; the next chunk's select may
+        // start while this chunk's handed-back rows still run
+        ql.done = sel[c];
         rc = launch_query(ctx, ql, stream);
         if (rc) {
             rc = fail(ctx, rc, std::string("query launch failed: ") + cudaGetErrorString(cudaGetLastError()));
             break;
         }
-        cudaEventRecord(sel[c], stream);
         ++launched;
     }
     if (!rc && speculative) {
@@ -853,6 +862,7 @@ static int run_pipelined(Context* ctx, Tile* t, int K, const StageGroup& g, cons
     }
     e = cudaStreamSynchronize(stream);
     if (cs && !e) e = cudaStreamSynchronize(cs);
+    if (ctx->fork && !e) e = cudaStreamSynchronize(ctx->fork);
     cudaError_t e2 = cudaStreamSynchronize(ctx->side);
     if (!rc && (e || e2))
         rc = fail(ctx, NBG_ERR_CUDA, std::string("pipelined query: ") + cudaGetErrorString(e ? e : e2));

@@ -66,6 +66,10 @@ struct Context {
     // query kernels run on the caller's stream
     cudaStream_t side = nullptr;
     cudaEvent_t xev[2];
+    // normal-priority stream for the single-pass select's handed-back rows,
+    // answered beside the finish pass of the other rows (fev: fork and join)
+    cudaStream_t fork = nullptr;
+    cudaEvent_t fev[3];
     // device blocks released by earlier calls, kept for reuse by size
     std::multimap<size_t, void*> cache;
     uint64_t cached = 0;
@@ -174,6 +178,11 @@ struct QueryLaunch {
     uint32_t* retry_rows = nullptr;
     int group = 0;
     float margin0 = 0.25f;
+    // when set, the launch records `done` once every row is answered and
+    // leaves `stream` free for the next launch (the single-pass select's
+    // handed-back rows may still run on the context's fork stream); when
+    // null, every row is answered in `stream` order
+    cudaEvent_t done = nullptr;
 };
 int launch_query(Context* ctx, const QueryLaunch& q, cudaStream_t stream);
 // rows + bounds[c] receives, in ascending order, the sorted positions whose

@@ -182,8 +182,10 @@ __global__ void __launch_bounds__(128) knn_fused_kernel(const QueryArgs a) {
 }
 
 // Split form, pass 1 + pass 2: the row's exact neighbourhood sums, in sorted
-// order (cnt = 0 marks a row handed to the exact path).
-template <int KS>
+// order (cnt = 0 marks a row handed to the exact path).  With FINISH the row
+// is finished in place instead and its sums are not written (the handed-back
+// rows of the single-pass select, whose sums slot already holds cnt = 0).
+template <int KS, bool FINISH = false>
 __device__ __forceinline__ void select_row(const QueryArgs& a, const uint64_t i) {
     const GridParams g = *a.gp;
     const float4 q = __ldg(&a.gv.sorted[i]);
@@ -195,9 +197,11 @@ __device__ __forceinline__ void select_row(const QueryArgs& a, const uint64_t i)
         const int32_t qraw[3] = {__float2int_rz(q.x) + g.minx, __float2int_rz(q.y) + g.miny,
                                  __float2int_rz(q.z) + g.minz};
         nbg_finish_row(a.grp, a.tf, a.ex, id, 0, M, qraw);
-        RowSums z;
-        z.cnt = 0;
-        a.sums[i] = z;
+        if (!FINISH) {
+            RowSums z;
+            z.cnt = 0;
+            a.sums[i] = z;
+        }
         return;
     }
     QueryCell qc;
@@ -214,14 +218,27 @@ __device__ __forceinline__ void select_row(const QueryArgs& a, const uint64_t i)
     out.cnt = 0;
     if (!select_kth<KS>(a, g, qc, q, K, R, kk, tie)) {
         defer_row(a, id, tie, kk, R);
-        a.sums[i] = out;
+        if (!FINISH) a.sums[i] = out;
         return;
     }
     Pass2Fn f2{q.x, q.y, q.z, kk, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int r = 0; r <= R; ++r) scan_shell(a.gv, g, qc, r, f2);
     if (f2.cnt != K) {
         defer_row(a, id, false, kk, R);
-        a.sums[i] = out;
+        if (!FINISH) a.sums[i] = out;
+        return;
+    }
+    if (FINISH) {
+        const long long n = f2.cnt;
+        long long M[6];
+        M[0] = n * f2.sxx - (long long)f2.s1x * f2.s1x;
+        M[1] = n * f2.syx - (long long)f2.s1y * f2.s1x;
+        M[2] = n * f2.syy - (long long)f2.s1y * f2.s1y;
+        M[3] = n * f2.szx - (long long)f2.s1z * f2.s1x;
+        M[4] = n * f2.szy - (long long)f2.s1z * f2.s1y;
+        M[5] = n * f2.szz - (long long)f2.s1z * f2.s1z;
+        const int32_t qraw[3] = {qc.qx + g.minx, qc.qy + g.miny, qc.qz + g.minz};
+        nbg_finish_row(a.grp, a.tf, a.ex, id, (int)n, M, qraw);
         return;
     }
     out.s[0] = f2.s1x;
@@ -347,6 +364,7 @@ __device__ __forceinline__ void select_row_loc(const QueryArgs& a, const uint64_
     auto retry = [&]() {
         const uint32_t slot = atomicAdd(&a.counters[6], 1u);
         a.retry_rows[slot] = (uint32_t)i;
+        a.sums[i].cnt = 0;  // the finish pass leaves the row to the retry launch
     };
     if (K <= 0) {
         retry();
@@ -636,6 +654,18 @@ __global__ void __launch_bounds__(128) knn_retry_kernel(const QueryArgs a) {
         if (a.ids_out) ids_row<KS>(a, i);
         else select_row<KS>(a, i);
     }
+}
+
+// Rows the single-pass select handed back, answered by the per-thread ring
+// search and finished in place (their sums slots hold cnt = 0, so the finish
+// pass over the other rows, which may run at the same time, skips them).  A
+// few of these rows search far and set the launch's length, so it runs beside
+// that finish pass rather than before it.
+template <int KS>
+__global__ void __launch_bounds__(128) knn_retry_finish_kernel(const QueryArgs a) {
+    const uint32_t nr = *a.nq_dev;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += gridDim.x * blockDim.x)
+        select_row<KS, true>(a, __ldg(&a.rows[r]));
 }
 
 // ---------------------------------------------------------------------------
@@ -1272,6 +1302,9 @@ static uint32_t loc_offset_bits(int32_t c) {
 struct LaunchArgs {
     QueryArgs q;
     cudaStream_t stream;
+    cudaStream_t fork = nullptr;   // second stream for the handed-back rows (null: `stream`)
+    cudaEvent_t fev[3] = {};       // fork, handed-back rows done, finish done
+    cudaEvent_t done = nullptr;    // QueryLaunch::done
     bool ids;
     int group = 0;        // select kernel (nbg_tile_set_select; 0: two-pass per-thread)
     float margin0 = 0.25f;
@@ -1305,10 +1338,32 @@ struct KnnLauncher {
             QueryArgs r = la.q;
             r.rows = la.q.retry_rows;
             r.nq_dev = la.q.counters + 6;
-            knn_retry_kernel<KS><<<(unsigned)std::min<uint64_t>(blocks, (uint64_t)la.sms * kRetryBlocksPerSm), threads,
-                                   0, la.stream>>>(r);
+            const unsigned rb = (unsigned)std::min<uint64_t>(blocks, (uint64_t)la.sms * kRetryBlocksPerSm);
+            if (!la.fork) {
+                knn_retry_kernel<KS><<<rb, threads, 0, la.stream>>>(r);
+                knn_finish_kernel<<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
+                NBG_LAUNCHED(3);
+                return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+            }
+            // the handed-back rows on the fork stream, queued first so their
+            // long searches start first; the finish pass of the other rows on
+            // `stream` fills the SMs around them
+            cudaError_t e = cudaEventRecord(la.fev[0], la.stream);
+            if (!e) e = cudaStreamWaitEvent(la.fork, la.fev[0], 0);
+            if (e) return NBG_ERR_CUDA;
+            knn_retry_finish_kernel<KS><<<rb, threads, 0, la.fork>>>(r);
             knn_finish_kernel<<<(unsigned)blocks, threads, 0, la.stream>>>(la.q);
             NBG_LAUNCHED(3);
+            if (la.done) {
+                // join on the fork stream: `stream` may go on to the next launch
+                e = cudaEventRecord(la.fev[2], la.stream);
+                if (!e) e = cudaStreamWaitEvent(la.fork, la.fev[2], 0);
+                if (!e) e = cudaEventRecord(la.done, la.fork);
+            } else {
+                e = cudaEventRecord(la.fev[1], la.fork);
+                if (!e) e = cudaStreamWaitEvent(la.stream, la.fev[1], 0);
+            }
+            if (e) return NBG_ERR_CUDA;
             return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
         }
         if (la.group == 1 && la.q.sums && !la.ids) {
@@ -1382,12 +1437,21 @@ int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
     la.q.nq = ql.sums ? ql.nrows : 0;
     la.q.retry_rows = ql.retry_rows;
     la.stream = stream;
+    if (ctx && ctx->fork) {
+        la.fork = ctx->fork;
+        for (int i = 0; i < 3; ++i) la.fev[i] = ctx->fev[i];
+    }
+    la.done = ql.done;
     la.ids = false;
     la.group = ql.retry_rows ? ql.group : 0;
     la.margin0 = ql.margin0;
     la.sms = ctx ? ctx->sm_count : 148;
     la.ob = loc_offset_bits(ql.tile->host_gp.cell);
-    return dispatch_slots<KnnLauncher>(ql.K, la);
+    const int rc = dispatch_slots<KnnLauncher>(ql.K, la);
+    // the forked single-pass launch records `done` itself, on the fork stream
+    const bool forked = la.fork && la.group == 2 && la.q.sums && (la.q.rows ? la.q.nq : la.q.n) > 0;
+    if (!rc && ql.done && !forked && cudaEventRecord(ql.done, stream) != cudaSuccess) return NBG_ERR_CUDA;
+    return rc;
 }
 
 int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
