@@ -390,7 +390,7 @@ int nbg_create(nbg_context** out, int device, uint64_t hbm_budget_bytes) {
         delete h;
         return NBG_ERR_CUDA;
     }
-    for (int i = 0; i < 3; ++i) cudaEventCreateWithFlags(&ctx->fev[i], cudaEventDisableTiming);
+    for (int i = 0; i < 4; ++i) cudaEventCreateWithFlags(&ctx->fev[i], cudaEventDisableTiming);
     if (dev_alloc(ctx, (void**)&ctx->counters, 64 * sizeof(uint32_t), nullptr)) {
         delete h;
         return NBG_ERR_OOM;
@@ -418,7 +418,7 @@ int nbg_destroy(nbg_context* h) {
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->fork) {
         cudaStreamDestroy(ctx->fork);
-        for (int i = 0; i < 3; ++i) cudaEventDestroy(ctx->fev[i]);
+        for (int i = 0; i < 4; ++i) cudaEventDestroy(ctx->fev[i]);
     }
     if (ctx->bounce_ready) {
         for (int i = 0; i < 2; ++i) {
@@ -1234,6 +1234,36 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
             cudaEventRecord(ctx->xev[1], ctx->side);
             cudaStreamWaitEvent(stream, ctx->xev[1], 0);
         }
+        // With the single-pass select the tie list is complete once its
+        // handed-back rows are answered on the fork stream: the tie rows are
+        // ordered there (count read on the device) beside the finish pass
+        // instead of after it.
+        const bool ties_queued = query_forks(ctx, ql) && kd_built(t);
+        if (ties_queued) {
+            cudaError_t qe = speculative ? cudaStreamWaitEvent(ctx->fork, ctx->xev[1], 0) : cudaSuccess;
+            if (!qe) qe = cudaEventRecord(ctx->ev[4], ctx->fork);
+            TieLaunch tl;
+            tl.tile = t;
+            tl.K = K;
+            tl.grp = g;
+            tl.ex = sink;
+            tl.ties = ctx->ties;
+            tl.nties = ql.tie_cap;
+            tl.kd = kd_order(t);
+            tl.exact_rows = ctx->exact_rows;
+            tl.counters = ctx->counters;
+            tl.ids_out = nullptr;
+            tl.row_k = row_k;
+            rc = qe ? NBG_ERR_CUDA : launch_ties_counted(ctx, tl, ctx->counters + 4, ctx->fork);
+            if (!rc && (cudaEventRecord(ctx->fev[3], ctx->fork) || cudaStreamWaitEvent(stream, ctx->fev[3], 0)))
+                rc = NBG_ERR_CUDA;
+            if (rc) {
+                cudaStreamSynchronize(ctx->fork);
+                cudaStreamSynchronize(stream);
+                cleanup();
+                return fail(ctx, rc, "tie-order resolver launch failed");
+            }
+        }
         uint32_t cnt[7] = {0, 0, 0, 0, 0, 0, 0};
         cudaError_t e = cudaMemcpyAsync(cnt, ctx->counters, 7 * sizeof(uint32_t),
                                         cudaMemcpyDeviceToHost, stream);
@@ -1253,9 +1283,9 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         }
         const uint32_t nties = (uint32_t)std::min<uint64_t>(cnt[4], ctx->tie_cap);
         if (cnt[0] || nties) {
-            cudaEventRecord(ctx->ev[4], stream);
+            if (!ties_queued) cudaEventRecord(ctx->ev[4], stream);
             rc = kd_ensure(ctx, t, stream);
-            if (!rc && nties) {
+            if (!rc && nties && !ties_queued) {
                 TieLaunch tl;
                 tl.tile = t;
                 tl.K = K;

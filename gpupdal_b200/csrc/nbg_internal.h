@@ -69,7 +69,7 @@ struct Context {
     // normal-priority stream for the single-pass select's handed-back rows,
     // answered beside the finish pass of the other rows (fev: fork and join)
     cudaStream_t fork = nullptr;
-    cudaEvent_t fev[3];
+    cudaEvent_t fev[4];
     // device blocks released by earlier calls, kept for reuse by size
     std::multimap<size_t, void*> cache;
     uint64_t cached = 0;
@@ -211,6 +211,14 @@ struct TieLaunch {
     const double* row_k = nullptr;
 };
 int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream);
+// The same with the row count read on the device: min(*count, tl.nties) rows
+// (tl.nties: the list's capacity), so the launch can be queued before the
+// query that fills the list has finished.
+int launch_ties_counted(Context* ctx, const TieLaunch& tl, const uint32_t* count, cudaStream_t stream);
+// True when launch_query answers `q`'s handed-back rows on the context's fork
+// stream (the single-pass select): work queued there after the launch runs
+// once the tie list is complete, beside the finish pass.
+bool query_forks(const Context* ctx, const QueryLaunch& q);
 // The tie rows of several tiles in one launch (returns after it completed).
 int launch_ties_many(Context* ctx, const TieLaunch* tls, int count, cudaStream_t stream);
 

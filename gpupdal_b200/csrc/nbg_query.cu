@@ -886,6 +886,13 @@ __global__ void __launch_bounds__(128) knn_tie_kernel(const TieArgs a) {
     if (r < a.nties) tie_row(a, r);
 }
 
+// Tie rows counted on the device (a.nties: the list's capacity).
+__global__ void __launch_bounds__(128) knn_tie_counted_kernel(const TieArgs a, const uint32_t* count) {
+    const uint32_t nt = min(*count, a.nties);
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nt; r += gridDim.x * blockDim.x)
+        tie_row(a, r);
+}
+
 // The tie rows of many tiles in one launch: jobs[j] is tile j's arguments,
 // its rows are entries first[j] .. first[j+1]-1 of the launch.
 __global__ void __launch_bounds__(128) knn_tie_batch_kernel(const TieArgs* __restrict__ jobs,
@@ -928,6 +935,19 @@ int launch_ties(Context* ctx, const TieLaunch& tl, cudaStream_t stream) {
     (void)ctx;
     if (!tl.nties) return NBG_OK;
     knn_tie_kernel<<<(tl.nties + 127) / 128, 128, 0, stream>>>(tie_args(tl));
+    NBG_LAUNCHED(1);
+    return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
+}
+
+// The grid covers a few per cent of a tile at one row per thread (tie rows
+// are 3 % of the 32M-point stress tile); a longer list is walked in strides.
+static constexpr uint64_t kTieBlocksPerSm = 16;
+
+int launch_ties_counted(Context* ctx, const TieLaunch& tl, const uint32_t* count, cudaStream_t stream) {
+    if (!tl.nties) return NBG_OK;
+    const uint64_t sms = ctx ? (uint64_t)ctx->sm_count : 148;
+    const unsigned blocks = (unsigned)std::min<uint64_t>(((uint64_t)tl.nties + 127) / 128, sms * kTieBlocksPerSm);
+    knn_tie_counted_kernel<<<blocks, 128, 0, stream>>>(tie_args(tl), count);
     NBG_LAUNCHED(1);
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
 }
@@ -1449,9 +1469,14 @@ int launch_query(Context* ctx, const QueryLaunch& ql, cudaStream_t stream) {
     la.ob = loc_offset_bits(ql.tile->host_gp.cell);
     const int rc = dispatch_slots<KnnLauncher>(ql.K, la);
     // the forked single-pass launch records `done` itself, on the fork stream
-    const bool forked = la.fork && la.group == 2 && la.q.sums && (la.q.rows ? la.q.nq : la.q.n) > 0;
-    if (!rc && ql.done && !forked && cudaEventRecord(ql.done, stream) != cudaSuccess) return NBG_ERR_CUDA;
+    if (!rc && ql.done && !query_forks(ctx, ql) && cudaEventRecord(ql.done, stream) != cudaSuccess)
+        return NBG_ERR_CUDA;
     return rc;
+}
+
+bool query_forks(const Context* ctx, const QueryLaunch& ql) {
+    const uint64_t rows = ql.rows ? ql.nrows : ql.tile->n;
+    return ctx && ctx->fork && ql.retry_rows && ql.group == 2 && ql.sums && rows > 0;
 }
 
 int launch_neighbor_sets(Context* ctx, const Tile* t, int K, int rmax, uint32_t* ids_out,
