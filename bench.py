@@ -47,9 +47,9 @@ QUERY_PROFILES = {
     0: {"kernel": "knn_select_kernel+knn_finish_kernel",
         # (182.3 + 628.9) MB / 4e6
         "traffic": 202.8, "lanes": 8.91, "issue": 0.793, "dram_pct": 0.54},
-    2: {"kernel": "knn_select_loc_kernel+knn_retry_kernel+knn_finish_kernel",
-        # select (70.3 + 101.1) + retry (10.3 + 0.0) + finish (364.6 + 261.4) MB / 4e6
-        "traffic": 201.9, "lanes": 10.13, "issue": 0.662, "dram_pct": 0.58},
+    2: {"kernel": "knn_select_loc_kernel+knn_retry_finish_kernel+knn_finish_kernel",
+        # select (70.4 + 99.3) + handed-back rows (10.1 + 0.1) + finish (363.1 + 255.5) MB / 4e6
+        "traffic": 199.6, "lanes": 10.13, "issue": 0.662, "dram_pct": 0.58},
 }
 
 
