@@ -851,7 +851,7 @@ static int run_pipelined(Context* ctx, Tile* t, int K, const StageGroup& g, cons
     if (!rc && speculative) {
         // the KD replica (needed by the tie rows) builds beside the queries
         cudaEventRecord(ctx->ev[8], ctx->side);
-        rc = kd_ensure(ctx, t, ctx->side);
+        rc = kd_ensure(ctx, t, ctx->side);  // uncapped: the first chunk's tie rows wait for it
         cudaEventRecord(ctx->ev[9], ctx->side);
     }
     for (int c = 0; c < launched && !rc; ++c) rc = finish_chunk(c);
@@ -1228,7 +1228,7 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
         cudaEventRecord(ctx->ev[3], stream);
         if (speculative) {
             cudaEventRecord(ctx->ev[8], ctx->side);
-            rc = kd_ensure(ctx, t, ctx->side);
+            rc = kd_ensure(ctx, t, ctx->side, true);
             if (rc) { cudaStreamSynchronize(stream); cleanup(); return rc; }
             cudaEventRecord(ctx->ev[9], ctx->side);
             cudaEventRecord(ctx->xev[1], ctx->side);

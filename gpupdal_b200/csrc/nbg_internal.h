@@ -234,9 +234,13 @@ struct RadiusLaunch {
 int launch_radius(Context* ctx, const RadiusLaunch& rl, cudaStream_t stream);
 
 // Exact path: nanoflann replica build (lazy) + DFS for the listed rows.
-int kd_ensure(Context* ctx, Tile* t, cudaStream_t stream);
+// beside_query: the build shares the SMs with a running query whose results
+// do not wait for it early; from 16M points its launches then keep to a few
+// blocks per SM (tiles and subtrees walked in strides)
+int kd_ensure(Context* ctx, Tile* t, cudaStream_t stream, bool beside_query = false);
 // One forest holding the replicas of every listed tile that has none.
-int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t stream);
+int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t stream,
+                   bool beside_query = false);
 int kd_run_rows(Context* ctx, Tile* t, int K, const StageGroup& grp, const ExceptionSink& ex,
                 const uint32_t* rows, uint32_t nrows, cudaStream_t stream,
                 const double* row_k = nullptr, int stride = 1, int kpick = 0);

@@ -48,6 +48,16 @@ static constexpr int KD_ITEMS = KD_TILE / KD_THREADS;
 static constexpr uint32_t KD_WARP_MAX = 4096;
 static constexpr int KD_WSTACK = 64;
 static constexpr int KD_WARPS = 4;
+// A build beside a running query (the plain call's speculative replica) keeps
+// its level passes to 2 blocks of 256 threads per SM and the warp subtree
+// builder to 2 blocks of 128, walking tiles and subtrees in strides, so the
+// query keeps most of every SM while the build still streams its passes.
+// Uncapped, its one-block-per-tile launches take every slot a query block
+// frees.  Below 16M points the capped build outlasts the query, which then
+// waits for it; the cap applies from there up.
+static constexpr int kKdBesideBlocksPerSm = 2;
+static constexpr int kKdBesideWarpBlocksPerSm = 2;
+static constexpr uint64_t kKdBesideMinPoints = 16000000;
 static constexpr int KD_RETRY = -100;  // kd_build: redo without warp subtrees
 static constexpr int KD_STACK = 96;
 static constexpr int KD_CAP = 66;
@@ -90,6 +100,8 @@ struct KdDev {
 // carry their tree in KdSeg::pad, nodes in ntree[].
 struct KdForest {
     uint64_t n = 0;
+    uint32_t grid_cap = 0;   // blocks of a level-pass launch (0: one per tile)
+    uint32_t wgrid_cap = 0;  // blocks of the warp subtree builder (0: one warp per subtree)
     int ntrees = 0;
     std::vector<uint64_t> base, npts;
     std::vector<Transform> tfh;
@@ -194,44 +206,48 @@ __global__ void kd_minmax_init_kernel(KdSplit* sp, uint32_t S) {
 __global__ void __launch_bounds__(KD_THREADS) kd_minmax_kernel(const KdSeg* segs, const uint32_t* tile_first,
                                                                const uint32_t* tile_seg,
                                                                const int32_t* rx, const int32_t* ry,
-                                                               const int32_t* rz, KdSplit* sp) {
+                                                               const int32_t* rz, KdSplit* sp,
+                                                               uint32_t ntiles) {
     __shared__ int32_t red[KD_THREADS / 32][6];
-    const uint32_t t = blockIdx.x;
-    const uint32_t s = tile_seg[t];
-    const KdSeg sg = segs[s];
-    const uint32_t i0 = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
-    int32_t v[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, w[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    // tiles in strides of the grid (capped beside a query: see kd_grid)
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t s = tile_seg[t];
+        const KdSeg sg = segs[s];
+        const uint32_t i0 = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
+        int32_t v[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, w[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
 #pragma unroll
-    for (int k = 0; k < KD_ITEMS; ++k) {
-        const uint32_t i = i0 + k * KD_THREADS;
-        if (i < sg.end) {
-            const int32_t c[3] = {rx[i], ry[i], rz[i]};
+        for (int k = 0; k < KD_ITEMS; ++k) {
+            const uint32_t i = i0 + k * KD_THREADS;
+            if (i < sg.end) {
+                const int32_t c[3] = {rx[i], ry[i], rz[i]};
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                v[d] = min(v[d], c[d]);
-                w[d] = max(w[d], c[d]);
+                for (int d = 0; d < 3; ++d) {
+                    v[d] = min(v[d], c[d]);
+                    w[d] = max(w[d], c[d]);
+                }
             }
         }
-    }
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        v[d] = __reduce_min_sync(0xffffffffu, v[d]);
-        w[d] = __reduce_max_sync(0xffffffffu, w[d]);
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
         for (int d = 0; d < 3; ++d) {
-            red[warp][d] = v[d];
-            red[warp][3 + d] = w[d];
+            v[d] = __reduce_min_sync(0xffffffffu, v[d]);
+            w[d] = __reduce_max_sync(0xffffffffu, w[d]);
         }
-    }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        int32_t r = red[0][threadIdx.x];
-        for (int k = 1; k < KD_THREADS / 32; ++k)
-            r = threadIdx.x < 3 ? min(r, red[k][threadIdx.x]) : max(r, red[k][threadIdx.x]);
-        if (threadIdx.x < 3) atomicMin(&sp[s].mn[threadIdx.x], r);
-        else atomicMax(&sp[s].mx[threadIdx.x - 3], r);
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            for (int d = 0; d < 3; ++d) {
+                red[warp][d] = v[d];
+                red[warp][3 + d] = w[d];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 6) {
+            int32_t r = red[0][threadIdx.x];
+            for (int k = 1; k < KD_THREADS / 32; ++k)
+                r = threadIdx.x < 3 ? min(r, red[k][threadIdx.x]) : max(r, red[k][threadIdx.x]);
+            if (threadIdx.x < 3) atomicMin(&sp[s].mn[threadIdx.x], r);
+            else atomicMax(&sp[s].mx[threadIdx.x - 3], r);
+        }
+        __syncthreads();
     }
 }
 
@@ -306,34 +322,38 @@ __global__ void __launch_bounds__(KD_THREADS) kd_count_kernel(const KdSeg* segs,
                                                               const KdSplit* sp, const int32_t* rx,
                                                               const int32_t* ry, const int32_t* rz,
                                                               const Transform* tfs,
-                                                              unsigned long long* tile_cnt) {
+                                                              unsigned long long* tile_cnt,
+                                                              uint32_t ntiles) {
     __shared__ unsigned long long red[KD_THREADS / 32];
-    const uint32_t t = blockIdx.x;
-    const uint32_t s = tile_seg[t];
-    const KdSeg sg = segs[s];
-    const Transform& tf = tfs[sg.pad];
-    const int f = sp[s].f;
-    const double cut = sp[s].cutval;
-    const int32_t* rc = f == 0 ? rx : (f == 1 ? ry : rz);
-    const uint32_t i0 = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
-    unsigned long long c = 0;
+    // tiles in strides of the grid (capped beside a query: see kd_grid)
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t s = tile_seg[t];
+        const KdSeg sg = segs[s];
+        const Transform& tf = tfs[sg.pad];
+        const int f = sp[s].f;
+        const double cut = sp[s].cutval;
+        const int32_t* rc = f == 0 ? rx : (f == 1 ? ry : rz);
+        const uint32_t i0 = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x;
+        unsigned long long c = 0;
 #pragma unroll
-    for (int k = 0; k < KD_ITEMS; ++k) {
-        const uint32_t i = i0 + k * KD_THREADS;
-        if (i < sg.end) {
-            const double v = ref_coord(rc[i], tf.scale[f], tf.offset[f]);
-            c += kd_pred<PASS>(v, cut) ? 1ull : 0ull;
-            if (PASS == 1 && v == cut) c += 1ull << 32;
+        for (int k = 0; k < KD_ITEMS; ++k) {
+            const uint32_t i = i0 + k * KD_THREADS;
+            if (i < sg.end) {
+                const double v = ref_coord(rc[i], tf.scale[f], tf.offset[f]);
+                c += kd_pred<PASS>(v, cut) ? 1ull : 0ull;
+                if (PASS == 1 && v == cut) c += 1ull << 32;
+            }
         }
-    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long r = 0;
-        for (int k = 0; k < KD_THREADS / 32; ++k) r += red[k];
-        tile_cnt[t] = r;
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long r = 0;
+            for (int k = 0; k < KD_THREADS / 32; ++k) r += red[k];
+            tile_cnt[t] = r;
+        }
+        __syncthreads();
     }
 }
 
@@ -385,40 +405,44 @@ __global__ void __launch_bounds__(KD_THREADS) kd_classify_kernel(const KdSeg* se
                                                                  const KdSplit* sp, const int32_t* rx,
                                                                  const int32_t* ry, const int32_t* rz,
                                                                  const Transform* tfs, uint32_t* mlpos,
-                                                                 uint32_t* mrpos) {
+                                                                 uint32_t* mrpos,
+                                                                 uint32_t ntiles) {
     typedef cub::BlockScan<uint32_t, KD_THREADS> Scan;
     __shared__ typename Scan::TempStorage tmp;
-    const uint32_t t = blockIdx.x;
-    const uint32_t s = tile_seg[t];
-    const KdSeg sg = segs[s];
-    const Transform& tf = tfs[sg.pad];
-    const int f = sp[s].f;
-    const double cut = sp[s].cutval;
-    const int32_t* rc = f == 0 ? rx : (f == 1 ? ry : rz);
-    const uint32_t L = PASS == 1 ? sp[s].L : sp[s].L2;
-    const uint32_t m = PASS == 1 ? sp[s].m : sp[s].m2;
-    // blocked arrangement: thread j owns elements j*KD_ITEMS .. j*KD_ITEMS+KD_ITEMS-1
-    const uint32_t i0 = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x * KD_ITEMS;
-    uint32_t p[KD_ITEMS], rank[KD_ITEMS];
+    // tiles in strides of the grid (capped beside a query: see kd_grid)
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t s = tile_seg[t];
+        const KdSeg sg = segs[s];
+        const Transform& tf = tfs[sg.pad];
+        const int f = sp[s].f;
+        const double cut = sp[s].cutval;
+        const int32_t* rc = f == 0 ? rx : (f == 1 ? ry : rz);
+        const uint32_t L = PASS == 1 ? sp[s].L : sp[s].L2;
+        const uint32_t m = PASS == 1 ? sp[s].m : sp[s].m2;
+        // blocked arrangement: thread j owns elements j*KD_ITEMS .. j*KD_ITEMS+KD_ITEMS-1
+        const uint32_t i0 = sg.begin + (t - tile_first[s]) * KD_TILE + threadIdx.x * KD_ITEMS;
+        uint32_t p[KD_ITEMS], rank[KD_ITEMS];
 #pragma unroll
-    for (int k = 0; k < KD_ITEMS; ++k) {
-        const uint32_t i = i0 + k;
-        p[k] = i < sg.end && kd_pred<PASS>(ref_coord(rc[i], tf.scale[f], tf.offset[f]), cut);
-    }
-    Scan(tmp).ExclusiveSum(p, rank);
-    const uint32_t before = (uint32_t)(tile_pref[t] - tile_pref[tile_first[s]]);
-#pragma unroll
-    for (int k = 0; k < KD_ITEMS; ++k) {
-        const uint32_t i = i0 + k;
-        if (i >= sg.end) break;
-        const uint32_t prank = before + rank[k];  // predicate holders before i in the segment
-        const uint32_t li = i - sg.begin;
-        if (li < L) {
-            if (!p[k]) mlpos[sg.begin + (li - prank)] = i;
-        } else if (p[k]) {
-            const uint32_t rml = prank - (L - m);
-            mrpos[sg.begin + (m - 1 - rml)] = i;
+        for (int k = 0; k < KD_ITEMS; ++k) {
+            const uint32_t i = i0 + k;
+            p[k] = i < sg.end && kd_pred<PASS>(ref_coord(rc[i], tf.scale[f], tf.offset[f]), cut);
         }
+        Scan(tmp).ExclusiveSum(p, rank);
+        const uint32_t before = (uint32_t)(tile_pref[t] - tile_pref[tile_first[s]]);
+#pragma unroll
+        for (int k = 0; k < KD_ITEMS; ++k) {
+            const uint32_t i = i0 + k;
+            if (i >= sg.end) break;
+            const uint32_t prank = before + rank[k];  // predicate holders before i in the segment
+            const uint32_t li = i - sg.begin;
+            if (li < L) {
+                if (!p[k]) mlpos[sg.begin + (li - prank)] = i;
+            } else if (p[k]) {
+                const uint32_t rml = prank - (L - m);
+                mrpos[sg.begin + (m - 1 - rml)] = i;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -437,48 +461,51 @@ __global__ void __launch_bounds__(KD_THREADS) kd_swap_kernel(const KdSeg* __rest
                                                              int32_t* __restrict__ rx,
                                                              int32_t* __restrict__ ry,
                                                              int32_t* __restrict__ rz,
-                                                             uint32_t* __restrict__ rid) {
-    const uint32_t t = blockIdx.x;
-    const uint32_t s = tile_seg[t];
-    const KdSeg sg = segs[s];
-    const uint32_t m = PASS == 1 ? sp[s].m : sp[s].m2;
-    const uint32_t l0 = (t - tile_first[s]) * KD_TILE + threadIdx.x;
-    if (l0 >= m) return;
-    uint32_t a[KD_ITEMS], b[KD_ITEMS];
-    int32_t ax[KD_ITEMS], ay[KD_ITEMS], az[KD_ITEMS], bx[KD_ITEMS], by[KD_ITEMS], bz[KD_ITEMS];
-    uint32_t ai[KD_ITEMS], bi[KD_ITEMS];
+                                                             uint32_t* __restrict__ rid,
+                                                             uint32_t ntiles) {
+    // tiles in strides of the grid (capped beside a query: see kd_grid)
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t s = tile_seg[t];
+        const KdSeg sg = segs[s];
+        const uint32_t m = PASS == 1 ? sp[s].m : sp[s].m2;
+        const uint32_t l0 = (t - tile_first[s]) * KD_TILE + threadIdx.x;
+        if (l0 >= m) continue;
+        uint32_t a[KD_ITEMS], b[KD_ITEMS];
+        int32_t ax[KD_ITEMS], ay[KD_ITEMS], az[KD_ITEMS], bx[KD_ITEMS], by[KD_ITEMS], bz[KD_ITEMS];
+        uint32_t ai[KD_ITEMS], bi[KD_ITEMS];
 #pragma unroll
-    for (int k = 0; k < KD_ITEMS; ++k) {
-        const uint32_t li = l0 + k * KD_THREADS;
-        if (li < m) {
-            a[k] = mlpos[sg.begin + li];
-            b[k] = mrpos[sg.begin + li];
+        for (int k = 0; k < KD_ITEMS; ++k) {
+            const uint32_t li = l0 + k * KD_THREADS;
+            if (li < m) {
+                a[k] = mlpos[sg.begin + li];
+                b[k] = mrpos[sg.begin + li];
+            }
         }
-    }
 #pragma unroll
-    for (int k = 0; k < KD_ITEMS; ++k) {
-        if (l0 + k * KD_THREADS < m) {
-            ax[k] = rx[a[k]];
-            ay[k] = ry[a[k]];
-            az[k] = rz[a[k]];
-            ai[k] = rid[a[k]];
-            bx[k] = rx[b[k]];
-            by[k] = ry[b[k]];
-            bz[k] = rz[b[k]];
-            bi[k] = rid[b[k]];
+        for (int k = 0; k < KD_ITEMS; ++k) {
+            if (l0 + k * KD_THREADS < m) {
+                ax[k] = rx[a[k]];
+                ay[k] = ry[a[k]];
+                az[k] = rz[a[k]];
+                ai[k] = rid[a[k]];
+                bx[k] = rx[b[k]];
+                by[k] = ry[b[k]];
+                bz[k] = rz[b[k]];
+                bi[k] = rid[b[k]];
+            }
         }
-    }
 #pragma unroll
-    for (int k = 0; k < KD_ITEMS; ++k) {
-        if (l0 + k * KD_THREADS < m) {
-            rx[a[k]] = bx[k];
-            ry[a[k]] = by[k];
-            rz[a[k]] = bz[k];
-            rid[a[k]] = bi[k];
-            rx[b[k]] = ax[k];
-            ry[b[k]] = ay[k];
-            rz[b[k]] = az[k];
-            rid[b[k]] = ai[k];
+        for (int k = 0; k < KD_ITEMS; ++k) {
+            if (l0 + k * KD_THREADS < m) {
+                rx[a[k]] = bx[k];
+                ry[a[k]] = by[k];
+                rz[a[k]] = bz[k];
+                rid[a[k]] = bi[k];
+                rx[b[k]] = ax[k];
+                ry[b[k]] = ay[k];
+                rz[b[k]] = az[k];
+                rid[b[k]] = ai[k];
+            }
         }
     }
 }
@@ -673,73 +700,74 @@ __global__ void __launch_bounds__(32 * KD_WARPS) kd_warp_build_kernel(
     const Transform* tfs, int32_t* ntree) {
     __shared__ KdSeg stk[KD_WARPS][KD_WSTACK];
     const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t w = blockIdx.x * KD_WARPS + wl;
-    if (w >= nsmall) return;
     KdSeg* st = stk[wl];
-    if (lane == 0) st[0] = small[w];
-    int top = 1;
-    __syncwarp();
-    while (top > 0) {
-        const KdSeg sg = st[top - 1];
-        --top;
+    // segments in strides of the grid's warps (capped beside a query)
+    for (uint32_t w = blockIdx.x * KD_WARPS + wl; w < nsmall; w += gridDim.x * KD_WARPS) {
+        if (lane == 0) st[0] = small[w];
+        int top = 1;
         __syncwarp();
-        const uint32_t b = sg.begin, e = sg.end, count = e - b;
-        const int node = sg.node;
-        int32_t mn[3], mx[3];
-        kd_warp_minmax(rx, ry, rz, b, e, lane, mn, mx);
-        if (lane < 3) {
-            bmin[3 * node + lane] = mn[lane];
-            bmax[3 * node + lane] = mx[lane];
-        }
-        if (count <= (uint32_t)KD_LEAF) continue;
-        const Transform tf = tfs[sg.pad];
-        int f;
-        double cut;
-        kd_choose_cut(sg.lo, sg.hi, mn, mx, tf, f, cut);
-        uint32_t eq = 0;
-        const uint32_t L = kd_warp_pass<1>(rx, ry, rz, rid, mlpos, mrpos, b, e, f, cut, tf, lane, &eq);
-        // pass 2 (<= cut on [b+L, e), which pass 1 left holding the elements
-        // >= cut) moves only elements equal to the cut value: with none, its
-        // count is 0 and it swaps nothing
-        const uint32_t L2 =
-            eq ? kd_warp_pass<2>(rx, ry, rz, rid, mlpos, mrpos, b + L, e, f, cut, tf, lane) : 0u;
-        const uint32_t lim1 = L, lim2 = L + L2;
-        uint32_t index;
-        if (lim1 > count / 2) index = lim1;
-        else if (lim2 < count / 2) index = lim2;
-        else index = count / 2;
-        uint32_t cid = 0;
-        if (lane == 0) cid = atomicAdd(&counters[1], 2u);
-        cid = __shfl_sync(0xffffffffu, cid, 0);
-        if (cid + 2 > node_cap || top + 2 > KD_WSTACK) {
-            if (lane == 0) atomicAdd(&counters[2], 1u);
-            return;
-        }
-        if (lane == 0) {
-            c1[node] = (int32_t)cid;
-            c2[node] = (int32_t)(cid + 1);
-            feat[node] = f;
-            for (int side = 1; side >= 0; --side) {
-                KdSeg ch = sg;
-                if (side == 0) {
-                    ch.end = b + index;
-                    ch.hi[f] = cut;
-                } else {
-                    ch.begin = b + index;
-                    ch.lo[f] = cut;
-                }
-                ch.node = (int32_t)(cid + side);
-                nb[cid + side] = ch.begin;
-                ne[cid + side] = ch.end;
-                c1[cid + side] = -1;
-                c2[cid + side] = -1;
-                feat[cid + side] = 0;
-                ntree[cid + side] = sg.pad;
-                st[top + (1 - side)] = ch;
+        while (top > 0) {
+            const KdSeg sg = st[top - 1];
+            --top;
+            __syncwarp();
+            const uint32_t b = sg.begin, e = sg.end, count = e - b;
+            const int node = sg.node;
+            int32_t mn[3], mx[3];
+            kd_warp_minmax(rx, ry, rz, b, e, lane, mn, mx);
+            if (lane < 3) {
+                bmin[3 * node + lane] = mn[lane];
+                bmax[3 * node + lane] = mx[lane];
             }
+            if (count <= (uint32_t)KD_LEAF) continue;
+            const Transform tf = tfs[sg.pad];
+            int f;
+            double cut;
+            kd_choose_cut(sg.lo, sg.hi, mn, mx, tf, f, cut);
+            uint32_t eq = 0;
+            const uint32_t L = kd_warp_pass<1>(rx, ry, rz, rid, mlpos, mrpos, b, e, f, cut, tf, lane, &eq);
+            // pass 2 (<= cut on [b+L, e), which pass 1 left holding the elements
+            // >= cut) moves only elements equal to the cut value: with none, its
+            // count is 0 and it swaps nothing
+            const uint32_t L2 =
+                eq ? kd_warp_pass<2>(rx, ry, rz, rid, mlpos, mrpos, b + L, e, f, cut, tf, lane) : 0u;
+            const uint32_t lim1 = L, lim2 = L + L2;
+            uint32_t index;
+            if (lim1 > count / 2) index = lim1;
+            else if (lim2 < count / 2) index = lim2;
+            else index = count / 2;
+            uint32_t cid = 0;
+            if (lane == 0) cid = atomicAdd(&counters[1], 2u);
+            cid = __shfl_sync(0xffffffffu, cid, 0);
+            if (cid + 2 > node_cap || top + 2 > KD_WSTACK) {
+                if (lane == 0) atomicAdd(&counters[2], 1u);
+                return;
+            }
+            if (lane == 0) {
+                c1[node] = (int32_t)cid;
+                c2[node] = (int32_t)(cid + 1);
+                feat[node] = f;
+                for (int side = 1; side >= 0; --side) {
+                    KdSeg ch = sg;
+                    if (side == 0) {
+                        ch.end = b + index;
+                        ch.hi[f] = cut;
+                    } else {
+                        ch.begin = b + index;
+                        ch.lo[f] = cut;
+                    }
+                    ch.node = (int32_t)(cid + side);
+                    nb[cid + side] = ch.begin;
+                    ne[cid + side] = ch.end;
+                    c1[cid + side] = -1;
+                    c2[cid + side] = -1;
+                    feat[cid + side] = 0;
+                    ntree[cid + side] = sg.pad;
+                    st[top + (1 - side)] = ch;
+                }
+            }
+            top += 2;
+            __syncwarp();
         }
-        top += 2;
-        __syncwarp();
     }
 }
 
@@ -1109,6 +1137,12 @@ static int kd_tiles(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, u
     return NBG_OK;
 }
 
+// Blocks of a level-pass launch over `ntiles` tiles: one per tile, or at most
+// the forest's cap when the build shares the SMs with a query.
+static unsigned kd_grid(const KdForest* kd, uint32_t ntiles) {
+    return kd->grid_cap ? std::min(ntiles, kd->grid_cap) : ntiles;
+}
+
 // known_tiles: the tile count when the tile map of `segs` is already built
 // (~0u: build it).
 template <int PASS>
@@ -1120,8 +1154,8 @@ static int kd_pass(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, Kd
         if (rc) return rc;
     }
     if (ntiles) {
-        kd_count_kernel<PASS><<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg, sp, kd->rx,
-                                                             kd->ry, kd->rz, kd->tfs, kd->tile_cnt);
+        kd_count_kernel<PASS><<<kd_grid(kd, ntiles), KD_THREADS, 0, st>>>(
+            segs, kd->nt, kd->tile_seg, sp, kd->rx, kd->ry, kd->rz, kd->tfs, kd->tile_cnt, ntiles);
     }
     cudaMemsetAsync(kd->tile_cnt + ntiles, 0, 8, st);
     size_t tb = kd->scan_bytes;
@@ -1130,13 +1164,11 @@ static int kd_pass(Context* ctx, KdForest* kd, const KdSeg* segs, uint32_t S, Kd
                                                                     sp, kd->rx, kd->ry, kd->rz,
                                                                     kd->tfs);
     if (ntiles) {
-        kd_classify_kernel<PASS><<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg,
-                                                                kd->tile_cnt, sp, kd->rx, kd->ry,
-                                                                kd->rz, kd->tfs, kd->mlpos,
-                                                                kd->mrpos);
-        kd_swap_kernel<PASS><<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg, sp,
-                                                            kd->mlpos, kd->mrpos, kd->rx, kd->ry,
-                                                            kd->rz, kd->rid);
+        kd_classify_kernel<PASS><<<kd_grid(kd, ntiles), KD_THREADS, 0, st>>>(
+            segs, kd->nt, kd->tile_seg, kd->tile_cnt, sp, kd->rx, kd->ry, kd->rz, kd->tfs, kd->mlpos,
+            kd->mrpos, ntiles);
+        kd_swap_kernel<PASS><<<kd_grid(kd, ntiles), KD_THREADS, 0, st>>>(
+            segs, kd->nt, kd->tile_seg, sp, kd->mlpos, kd->mrpos, kd->rx, kd->ry, kd->rz, kd->rid, ntiles);
     }
     NBG_LAUNCHED(3 + (ntiles ? 3 : 0));
     return cudaGetLastError() == cudaSuccess ? NBG_OK : NBG_ERR_CUDA;
@@ -1239,8 +1271,8 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
         rc = kd_tiles(ctx, kd, segs, S, &ntiles, st);
         if (rc) return rc;
         if (ntiles)
-            kd_minmax_kernel<<<ntiles, KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->rx, kd->ry,
-                                                            kd->rz, kd->split);
+            kd_minmax_kernel<<<kd_grid(kd, ntiles), KD_THREADS, 0, st>>>(segs, kd->nt, kd->tile_seg, kd->rx,
+                                                                         kd->ry, kd->rz, kd->split, ntiles);
         kd_split_kernel<<<(S + 127) / 128, 128, 0, st>>>(segs, S, kd->split, kd->tfs, kd->bmin, kd->bmax);
         NBG_LAUNCHED(2 + (ntiles ? 1 : 0));
         // pass 1 runs on the same segments: their tile map is already built
@@ -1293,7 +1325,8 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
     if (nsmall) {
         rc = kd_grow_nodes(ctx, kd, std::max<uint32_t>(kd->node_cap, node_count + (uint32_t)(n / 8) + 1024), st);
         if (rc) return rc;
-        kd_warp_build_kernel<<<(nsmall + KD_WARPS - 1) / KD_WARPS, 32 * KD_WARPS, 0, st>>>(
+        const uint32_t wblocks = (nsmall + KD_WARPS - 1) / KD_WARPS;
+        kd_warp_build_kernel<<<kd->wgrid_cap ? std::min(wblocks, kd->wgrid_cap) : wblocks, 32 * KD_WARPS, 0, st>>>(
             kd->small, nsmall, kd->rx, kd->ry, kd->rz, kd->rid, kd->mlpos, kd->mrpos, kd->c1, kd->c2,
             kd->feat, kd->nb, kd->ne, kd->bmin, kd->bmax, kd->counters, kd->node_cap, kd->tfs,
             kd->ntree);
@@ -1341,7 +1374,7 @@ static int kd_build(Context* ctx, KdForest* kd, Tile* const* tiles, uint32_t sma
 }
 
 // Builds one forest holding the replicas of every listed tile that has none.
-int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t st) {
+int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t st, bool beside_query) {
     NBG_RANGE("nbg kd replica build");
     std::vector<Tile*> todo;
     for (int i = 0; i < count; ++i)
@@ -1363,6 +1396,10 @@ int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t st)
         return NBG_ERR_UNSUPPORTED;
     }
     kd->n = n;
+    if (beside_query && n >= kKdBesideMinPoints) {
+        kd->grid_cap = (uint32_t)(kKdBesideBlocksPerSm * ctx->sm_count);
+        kd->wgrid_cap = (uint32_t)(kKdBesideWarpBlocksPerSm * ctx->sm_count);
+    }
     kd->rootbox.assign(6 * (size_t)kd->ntrees, 0.0);
     const int T = kd->ntrees;
     int rc = kd_alloc(ctx, (void**)&kd->rx, n * 4, kd);
@@ -1421,9 +1458,9 @@ int kd_ensure_many(Context* ctx, Tile* const* tiles, int count, cudaStream_t st)
     return NBG_OK;
 }
 
-int kd_ensure(Context* ctx, Tile* t, cudaStream_t st) {
+int kd_ensure(Context* ctx, Tile* t, cudaStream_t st, bool beside_query) {
     Tile* one[1] = {t};
-    return kd_ensure_many(ctx, one, 1, st);
+    return kd_ensure_many(ctx, one, 1, st, beside_query);
 }
 
 bool kd_built(const Tile* t) { return t->kd && t->kd->built; }
