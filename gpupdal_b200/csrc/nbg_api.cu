@@ -928,6 +928,12 @@ extern "C" int nbg_run(nbg_context* h, nbg_tile* th, const nbg_stage_opts* stage
     char* packed_dev_c = nullptr;
     size_t packed_bytes_c = 0;
     auto cleanup = [&]() {
+        // The blocks go back to the context's cache, where the next call may
+        // take them: on an error return the fork stream (handed-back rows, tie
+        // order) or the side stream (KD replica) can still be writing them.
+        cudaStreamSynchronize(stream);
+        cudaStreamSynchronize(ctx->fork);
+        cudaStreamSynchronize(ctx->side);
         if (packed_dev_c) dev_free(ctx, packed_dev_c, packed_bytes_c);
         for (auto& o : hout)
             if (o.dev) dev_free(ctx, o.dev, o.bytes);
