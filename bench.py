@@ -426,7 +426,7 @@ def extras_leg(ctx, args, cpu=None):
         las.write_las(path, x, y, z, version=(1, 4), point_format=7)
         f = las.LasFile(path)
         rec = np.ascontiguousarray(f.records)
-        drec = torch.from_numpy(rec).to(dev)
+        drec = torch.from_numpy(rec.copy()).to(dev)  # the mapped records are read-only
         nbytes = rec.nbytes
 
         def up_host():
